@@ -1,0 +1,139 @@
+"""Python access to the parity oracles.  TEST INFRASTRUCTURE ONLY.
+
+* ``OracleLib`` -- ctypes binding of the C restatement ``rmhd2d_oracle.c``
+  (built into ``oracle/liborc.so`` by ``build()``).
+* ``run_reference`` -- runs the reference's own step built by
+  ``oracle/build_ref.py`` (``oracle/_ref/ref_{cpu,gpu}_{periodic,symmetric}``)
+  on a state and returns the final state, the per-step dt and the timing.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline and
+reference legs may import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liborc.so"
+REF_DIR = HERE / "_ref"
+
+BC = {"periodic": 0, "symmetric": 1}
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("cfl", ctypes.c_double), ("eps", ctypes.c_double),
+        ("eta", ctypes.c_double), ("eta_table", ctypes.POINTER(ctypes.c_double)),
+        ("bc", ctypes.c_int),
+    ]
+
+
+def build(verbose: bool = False) -> Path:
+    """Compile the C restatement (no FMA contraction) into oracle/liborc.so."""
+    src = HERE / "rmhd2d_oracle.c"
+    if LIB.exists() and LIB.stat().st_mtime >= max(src.stat().st_mtime, (HERE / "rmhd2d_oracle.h").stat().st_mtime):
+        return LIB
+    cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
+           "-Wall", "-o", str(LIB), str(src), "-lm"]
+    subprocess.run(cmd, check=True, capture_output=not verbose)
+    return LIB
+
+
+class OracleLib:
+    def __init__(self):
+        build()
+        self.lib = ctypes.CDLL(str(LIB))
+        P = ctypes.POINTER(_Params)
+        D = ctypes.POINTER(ctypes.c_double)
+        self.lib.orc_calc_dt.argtypes = [P, D]
+        self.lib.orc_calc_dt.restype = ctypes.c_double
+        self.lib.orc_is_crashed.argtypes = [P, D]
+        self.lib.orc_boundary.argtypes = [P, D]
+        self.lib.orc_run.argtypes = [P, D, ctypes.c_int, D]
+        self.lib.orc_run.restype = ctypes.c_int
+
+    @staticmethod
+    def _params(setup, eta_keep):
+        tab = None
+        if setup.eta_table is not None:
+            tab = np.ascontiguousarray(setup.eta_table, dtype=np.float64)
+            eta_keep.append(tab)
+        p = _Params(setup.nx, setup.ny, setup.dx, setup.dy, setup.gamma, setup.cfl, setup.eps,
+                    setup.eta, tab.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if tab is not None else None,
+                    BC[setup.bc])
+        return p
+
+    def boundary(self, setup, state: np.ndarray) -> np.ndarray:
+        keep = []
+        p = self._params(setup, keep)
+        out = np.ascontiguousarray(state, dtype=np.float64).copy()
+        self.lib.orc_boundary(ctypes.byref(p), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
+    def calc_dt(self, setup, state: np.ndarray) -> float:
+        keep = []
+        p = self._params(setup, keep)
+        s = np.ascontiguousarray(state, dtype=np.float64)
+        return self.lib.orc_calc_dt(ctypes.byref(p), s.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+
+    def run(self, setup, state: np.ndarray, nsteps: int, apply_boundary: bool = True):
+        """Returns (final_state, dts, crashed_at) after nsteps RK2 steps."""
+        keep = []
+        p = self._params(setup, keep)
+        s = np.ascontiguousarray(state, dtype=np.float64).copy()
+        dp = s.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        if apply_boundary:
+            self.lib.orc_boundary(ctypes.byref(p), dp)
+        dts = np.zeros(max(nsteps, 1), dtype=np.float64)
+        rc = self.lib.orc_run(ctypes.byref(p), dp, nsteps, dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if rc < 0:
+            raise MemoryError("oracle work allocation failed")
+        crashed_at = rc - 1 if rc > 0 else -1
+        return s, dts[:nsteps], crashed_at
+
+
+def reference_binary(kind: str, bc: str) -> Path:
+    return REF_DIR / f"ref_{kind}_{bc}"
+
+
+def run_reference(setup, state: np.ndarray, n_timed: int, n_warmup: int = 0, kind: str = "cpu",
+                  threads: int | None = None, timeout: float = 1800.0):
+    """Run the reference's own step (built by build_ref.py) from ``state``
+    (boundary applied inside, as the reference's initializeU does).
+    Returns (final_state, dts, info_dict)."""
+    exe = reference_binary(kind, setup.bc)
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} not built (oracle/build_ref.py)")
+    env = dict(os.environ)
+    env.update({
+        "REF_NX": str(setup.nx), "REF_NY": str(setup.ny), "REF_DX": repr(setup.dx), "REF_DY": repr(setup.dy),
+        "REF_GAMMA": repr(setup.gamma), "REF_CFL": repr(setup.cfl), "REF_EPS": repr(setup.eps),
+        "REF_ETA": repr(setup.eta),
+    })
+    if threads is not None:
+        env["OMP_NUM_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory(dir=os.environ.get("RMHD_TMPDIR")) as td:
+        td = Path(td)
+        np.ascontiguousarray(state, dtype=np.float64).tofile(td / "in.bin")
+        if setup.eta_table is not None:
+            np.ascontiguousarray(setup.eta_table, dtype=np.float64).tofile(td / "eta.bin")
+            env["REF_ETA_TABLE"] = str(td / "eta.bin")
+        else:
+            env["REF_ETA_TABLE"] = ""
+        r = subprocess.run([str(exe), str(td / "in.bin"), str(td / "out.bin"), str(n_warmup), str(n_timed),
+                            str(td / "dts.bin")], env=env, capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"{exe.name} failed ({r.returncode}): {r.stderr[-2000:]}")
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        out = np.fromfile(td / "out.bin", dtype=np.float64).reshape(setup.nx, setup.ny, 8)
+        dts = np.fromfile(td / "dts.bin", dtype=np.float64)
+    return out, dts, info

@@ -1,0 +1,669 @@
+/*
+ * rmhd2d_oracle.c -- CPU restatement of one RK2 step of the 2D resistive-MHD
+ * solver in keita-akutagawa/ResistiveMHD_GPU (single-GPU Thrust library).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity checker for the CUDA
+ * path in resistivemhd_gpu_b200/.  Only tests/, __graft_entry__.smoke() and
+ * the cpu_baseline / reference legs of bench.py may load it.  The product
+ * never links or calls it.
+ *
+ * It restates, operation by operation and in the same evaluation order, the
+ * arithmetic of these reference files (paths inside the reference project):
+ *
+ *   ResistiveMHD_singleGPU_thrust/lib_ResistiveMHD_2D_GPU_periodicXY/
+ *     resistiveMHD_2D.cu:133-195   oneStepRK2 (stage order, CT reuse)
+ *     resistiveMHD_2D.cu:53-130    oneStepFirst/SecondFunctor (update)
+ *     resistiveMHD_2D.cu:247-291   calculateDtFunctor / calculateDt
+ *     resistiveMHD_2D.cu:294-309   IsNan / checkCalculationIsCrashed
+ *     resistiveMHD_2D.cu:313-426   shift/back B to centre for CT
+ *     calculate_half_Q.cu:4-67     GetBasicParamterFunctor (primitives)
+ *     muscl.cu:6-126, minmod.hpp   MUSCL-minmod interface states
+ *     hlld.cu:26-131, 134-233      Sign, CalculateFluxFunctor, y-sweep shuffles
+ *     hlld.cu:256-444              calculateHLLDParameterFunctor
+ *     hlld.cu:448-565              getOneFlux / setFluxFunctor
+ *     ct.cu:22-85                  getEZVector_kernel, CT_kernel
+ *     boundary.cu:4-141            periodicBoundaryX2nd / Y2nd
+ *   .../lib_ResistiveMHD_2D_GPU_symmetricXY/boundary.cu:4-206
+ *                                  symmetricBoundaryX2nd(+BX) / Y2nd(+BY)
+ *   ResistiveMHD_singleGPU_thrust/examples2D/plasmoid/main_plasmoid.cu:175-290
+ *                                  addResistiveTermToFluxF/G (driver hook)
+ *
+ * State layout is the reference's: an array of nx*ny cells, cell k = j + i*ny
+ * (y fastest), each cell 8 doubles {rho, rhoU, rhoV, rhoW, bX, bY, bZ, e}.
+ * nx, ny include 3 ghost layers per side.  bX of cell (i,j) is the x-face
+ * value at x_{i+1/2}; bY is the y-face value at y_{j+1/2}.
+ *
+ * Build with -ffp-contract=off (no fused multiply-add) so every operation is
+ * one IEEE-754 binary64 operation, exactly as the reference's host build on
+ * x86-64 (SSE2) evaluates it.
+ *
+ * Where the reference reads buffer entries that the current call did not
+ * write (e.g. dQCenter at i = nx-1 in the x sweep, flat-index wrap in the y
+ * sweep), this restatement writes NaN instead.  Those entries only feed
+ * ghost cells that the boundary pass overwrites, so a finite final state
+ * is a check that no such value reaches the result.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "rmhd2d_oracle.h"
+
+enum { RHO = 0, MX = 1, MY = 2, MZ = 3, BXF = 4, BYF = 5, BZF = 6, EN = 7, NV = 8 };
+
+/* BasicParameter field order: rho, u, v, w, bX, bY, bZ, p
+   (basic_parameter_struct.hpp:5-27). */
+enum { QR = 0, QU = 1, QV = 2, QW = 3, QBX = 4, QBY = 5, QBZ = 6, QP = 7 };
+
+/* thrust::min / thrust::max semantics: min(a,b) = (b < a) ? b : a. */
+static inline double tmin(double a, double b) { return (b < a) ? b : a; }
+static inline double tmax(double a, double b) { return (a < b) ? b : a; }
+
+/* hlld.cu:26-32 Sign: (x > 0) - (x < 0) as double. */
+static inline double sgn(double x) { return (double)((x > 0.0) - (x < 0.0)); }
+
+/* minmod.hpp:6-16: sign_x * max(min(|x|, sign_x*y), EPS), sign_x an int. */
+static inline double minmod(double x, double y, double eps)
+{
+    int s = (x > 0) - (x < 0);
+    double ax = fabs(x);
+    return (double)s * tmax(tmin(ax, (double)s * y), eps);
+}
+
+/* calculate_half_Q.cu:4-38 GetBasicParamterFunctor on a cell c and its
+   neighbour cp along the sweep.  c points at 8 doubles in sweep order
+   (rho, rhoU, rhoV, rhoW, bX, bY, bZ, e). */
+static void basic_param(const double *c, const double *cp, double gm, double *q)
+{
+    double rho = c[0];
+    double u = c[1] / rho;
+    double v = c[2] / rho;
+    double w = c[3] / rho;
+    double bX = c[4], bY = c[5], bZ = c[6], e = c[7];
+    double p = (gm - 1.0)
+             * (e - 0.5 * (rho * (u * u + v * v + w * w))
+             - 0.5 * (bX * bX + bY * bY + bZ * bZ));
+    double bXPlus1 = cp[4];
+    q[QR] = rho; q[QU] = u; q[QV] = v; q[QW] = w;
+    q[QBX] = 0.5 * (bX + bXPlus1);
+    q[QBY] = bY; q[QBZ] = bZ; q[QP] = p;
+}
+
+/* muscl.cu:6-30 LeftParameterFunctor. */
+static void muscl_left(const double *qm, const double *q, const double *qp, double eps, double *out)
+{
+    static const int comps[7] = {QR, QU, QV, QW, QBY, QBZ, QP};
+    for (int n = 0; n < 7; ++n) {
+        int c = comps[n];
+        out[c] = q[c] + 0.5 * minmod(q[c] - qm[c], qp[c] - q[c], eps);
+    }
+    out[QBX] = q[QBX];
+}
+
+/* muscl.cu:66-90 RightParameterFunctor (q at k, qp at k+off, qpp at k+2off). */
+static void muscl_right(const double *q, const double *qp, const double *qpp, double eps, double *out)
+{
+    static const int comps[7] = {QR, QU, QV, QW, QBY, QBZ, QP};
+    for (int n = 0; n < 7; ++n) {
+        int c = comps[n];
+        out[c] = qp[c] - 0.5 * minmod(qp[c] - q[c], qpp[c] - qp[c], eps);
+    }
+    out[QBX] = q[QBX];
+}
+
+/* hlld.cu:448-467 getOneFlux. */
+static void one_flux(double rho, double u, double v, double w, double bX, double bY,
+                     double bZ, double e, double pT, double *f)
+{
+    f[0] = rho * u;
+    f[1] = rho * u * u + pT - bX * bX;
+    f[2] = rho * u * v - bX * bY;
+    f[3] = rho * u * w - bX * bZ;
+    f[4] = 0.0;
+    f[5] = u * bY - v * bX;
+    f[6] = u * bZ - w * bX;
+    f[7] = (e + pT) * u - bX * (bX * u + bY * v + bZ * w);
+}
+
+/* hlld.cu:256-432 calculateHLLDParameterFunctor, hlld.cu:469-549
+   setFluxFunctor and hlld.cu:35-107 CalculateFluxFunctor, fused: all six
+   candidate fluxes are formed and summed with the reference's indicator
+   weights, so non-finite candidates propagate as they do there. */
+static void hlld_flux(const double *L, const double *R, double gm, double EPS, double *flux)
+{
+    double rhoL = L[QR], uL = L[QU], vL = L[QV], wL = L[QW];
+    double bXL = L[QBX], bYL = L[QBY], bZL = L[QBZ], pL = L[QP];
+    double eL = pL / (gm - 1.0)
+              + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL)
+              + 0.5 * (bXL * bXL + bYL * bYL + bZL * bZL);
+    double pTL = pL + 0.5 * (bXL * bXL + bYL * bYL + bZL * bZL);
+
+    double rhoR = R[QR], uR = R[QU], vR = R[QV], wR = R[QW];
+    double bXR = R[QBX], bYR = R[QBY], bZR = R[QBZ], pR = R[QP];
+    double eR = pR / (gm - 1.0)
+              + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR)
+              + 0.5 * (bXR * bXR + bYR * bYR + bZR * bZR);
+    double pTR = pR + 0.5 * (bXR * bXR + bYR * bYR + bZR * bZR);
+
+    double csL = sqrt(gm * pL / rhoL);
+    double caL = sqrt((bXL * bXL + bYL * bYL + bZL * bZL) / rhoL);
+    double vaL = sqrt(bXL * bXL / rhoL);
+    double cfL = sqrt(0.5 * (csL * csL + caL * caL
+               + sqrt((csL * csL + caL * caL) * (csL * csL + caL * caL)
+               - 4.0 * csL * csL * vaL * vaL)));
+
+    double csR = sqrt(gm * pR / rhoR);
+    double caR = sqrt((bXR * bXR + bYR * bYR + bZR * bZR) / rhoR);
+    double vaR = sqrt(bXR * bXR / rhoR);
+    double cfR = sqrt(0.5 * (csR * csR + caR * caR
+               + sqrt((csR * csR + caR * caR) * (csR * csR + caR * caR)
+               - 4.0 * csR * csR * vaR * vaR)));
+
+    double SL = tmin(uL, uR) - tmax(cfL, cfR);
+    double SR = tmax(uL, uR) + tmax(cfL, cfR);
+    SL = tmin(SL, 0.0);
+    SR = tmax(SR, 0.0);
+
+    double SM = ((SR - uR) * rhoR * uR - (SL - uL) * rhoL * uL - pTR + pTL)
+              / ((SR - uR) * rhoR - (SL - uL) * rhoL + EPS);
+    double pT1 = ((SR - uR) * rhoR * pTL - (SL - uL) * rhoL * pTR
+               + rhoL * rhoR * (SR - uR) * (SL - uL) * (uR - uL))
+               / ((SR - uR) * rhoR - (SL - uL) * rhoL + EPS);
+    double pT1L = pT1, pT1R = pT1;
+
+    double rho1L = rhoL * (SL - uL) / (SL - SM + EPS);
+    double u1L = SM;
+    double v1L = vL - bXL * bYL * (SM - uL) / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    double w1L = wL - bXL * bZL * (SM - uL) / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    double bX1L = bXL;
+    double bY1L = bYL * (rhoL * (SL - uL) * (SL - uL) - bXL * bXL)
+                / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    double bZ1L = bZL * (rhoL * (SL - uL) * (SL - uL) - bXL * bXL)
+                / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    double e1L = ((SL - uL) * eL - pTL * uL + pT1 * SM
+               + bXL * ((uL * bXL + vL * bYL + wL * bZL) - (u1L * bX1L + v1L * bY1L + w1L * bZ1L)))
+               / (SL - SM + EPS);
+
+    double rho1R = rhoR * (SR - uR) / (SR - SM + EPS);
+    double u1R = SM;
+    double v1R = vR - bXR * bYR * (SM - uR) / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    double w1R = wR - bXR * bZR * (SM - uR) / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    double bX1R = bXR;
+    double bY1R = bYR * (rhoR * (SR - uR) * (SR - uR) - bXR * bXR)
+                / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    double bZ1R = bZR * (rhoR * (SR - uR) * (SR - uR) - bXR * bXR)
+                / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    double e1R = ((SR - uR) * eR - pTR * uR + pT1 * SM
+               + bXR * ((uR * bXR + vR * bYR + wR * bZR) - (u1R * bX1R + v1R * bY1R + w1R * bZ1R)))
+               / (SR - SM + EPS);
+
+    double S1L = SM - sqrt(bX1L * bX1L / rho1L);
+    double S1R = SM + sqrt(bX1R * bX1R / rho1R);
+
+    double rho2L = rho1L, rho2R = rho1R, u2 = SM;
+    double v2 = (sqrt(rho1L) * v1L + sqrt(rho1R) * v1R + (bY1R - bY1L) * sgn(bX1L))
+              / (sqrt(rho1L) + sqrt(rho1R) + EPS);
+    double w2 = (sqrt(rho1L) * w1L + sqrt(rho1R) * w1R + (bZ1R - bZ1L) * sgn(bX1L))
+              / (sqrt(rho1L) + sqrt(rho1R) + EPS);
+    double bY2 = (sqrt(rho1L) * bY1R + sqrt(rho1R) * bY1L + sqrt(rho1L * rho1R) * (v1R - v1L) * sgn(bX1L))
+               / (sqrt(rho1L) + sqrt(rho1R) + EPS);
+    double bZ2 = (sqrt(rho1L) * bZ1R + sqrt(rho1R) * bZ1L + sqrt(rho1L * rho1R) * (w1R - w1L) * sgn(bX1L))
+               / (sqrt(rho1L) + sqrt(rho1R) + EPS);
+    double e2L = e1L - sqrt(rho1L)
+               * ((u1L * bX1L + v1L * bY1L + w1L * bZ1L) - (u2 * bXL + v2 * bY2 + w2 * bZ2))
+               * sgn(bXL);
+    double e2R = e1R + sqrt(rho1R)
+               * ((u1R * bX1R + v1R * bY1R + w1R * bZ1R) - (u2 * bXR + v2 * bY2 + w2 * bZ2))
+               * sgn(bXR);
+    double pT2L = pT1L, pT2R = pT1R;
+
+    double fOL[8], fML[8], fIL[8], fOR[8], fMR[8], fIR[8];
+    one_flux(rhoL, uL, vL, wL, bXL, bYL, bZL, eL, pTL, fOL);
+    one_flux(rho1L, u1L, v1L, w1L, bXL, bY1L, bZ1L, e1L, pT1L, fML);
+    one_flux(rho2L, u2, v2, w2, bXL, bY2, bZ2, e2L, pT2L, fIL);
+    one_flux(rhoR, uR, vR, wR, bXR, bYR, bZR, eR, pTR, fOR);
+    one_flux(rho1R, u1R, v1R, w1R, bXR, bY1R, bZ1R, e1R, pT1R, fMR);
+    one_flux(rho2R, u2, v2, w2, bXR, bY2, bZ2, e2R, pT2R, fIR);
+
+    double iOL = (double)(SL > 0.0);
+    double iML = (double)((SL <= 0.0) && (0.0 < S1L));
+    double iIL = (double)((S1L <= 0.0) && (0.0 < SM));
+    double iOR = (double)(SR <= 0.0);
+    double iMR = (double)((S1R <= 0.0) && (0.0 < SR));
+    double iIR = (double)((SM <= 0.0) && (0.0 < S1R));
+    for (int n = 0; n < 8; ++n) {
+        flux[n] = fOL[n] * iOL + fML[n] * iML + fIL[n] * iIL
+                + fOR[n] * iOR + fMR[n] * iMR + fIR[n] * iIR;
+    }
+}
+
+/* eta at cell (i,j): the driver's getEta.  A table (cell-centred, k = j +
+   i*ny) when given, else the uniform value. */
+static inline double eta_at(const orc_params *p, int i, int j)
+{
+    return p->eta_table ? p->eta_table[j + i * p->ny] : p->eta;
+}
+
+/* x-direction flux F at interface i+1/2 of every cell (HLLD::calculateFluxF,
+   hlld.cu:110-131, + resistive hook main_plasmoid.cu:175-215).  Uc is the
+   state with cell-centred B. */
+static void flux_x(const orc_params *p, const double *Uc, double *F, double *dQ,
+                   double *dQL, double *dQR)
+{
+    const int nx = p->nx, ny = p->ny, N = nx * ny;
+    const double gm = p->gamma, EPS = p->eps;
+    const double qnan = NAN;
+
+    /* setPhysicalParameterX: k in [0, N - ny); entries at i = nx-1 stale. */
+    for (int k = 0; k < N; ++k) {
+        if (k < N - ny) basic_param(&Uc[k * NV], &Uc[(k + ny) * NV], gm, &dQ[k * 8]);
+        else for (int c = 0; c < 8; ++c) dQ[k * 8 + c] = qnan;
+    }
+    /* getLeftQX: k in [ny, N - ny). getRightQX: k in [0, N - 2ny). */
+    #pragma omp parallel for schedule(static)
+    for (int k = 0; k < N; ++k) {
+        if (k >= ny && k < N - ny)
+            muscl_left(&dQ[(k - ny) * 8], &dQ[k * 8], &dQ[(k + ny) * 8], EPS, &dQL[k * 8]);
+        else for (int c = 0; c < 8; ++c) dQL[k * 8 + c] = qnan;
+        if (k < N - 2 * ny)
+            muscl_right(&dQ[k * 8], &dQ[(k + ny) * 8], &dQ[(k + 2 * ny) * 8], EPS, &dQR[k * 8]);
+        else for (int c = 0; c < 8; ++c) dQR[k * 8 + c] = qnan;
+    }
+    #pragma omp parallel for schedule(static)
+    for (int k = 0; k < N; ++k) hlld_flux(&dQL[k * 8], &dQR[k * 8], gm, EPS, &F[k * 8]);
+
+    /* addResistiveTermToFluxF: 0 < i < nx-2, 0 < j < ny-2, U = Uc. */
+    const double dx = p->dx, dy = p->dy;
+    #pragma omp parallel for schedule(static)
+    for (int i = 1; i < nx - 2; ++i) {
+        for (int j = 1; j < ny - 2; ++j) {
+            const double *U = Uc;
+            double jY, jZ, eta;
+            double etaJY, etaJYPlus1, etaJZ, etaJZPlus1;
+            double etaJYBZ, etaJYBZPlus1, etaJZBY, etaJZBYPlus1;
+            jY = -(U[(j + (i + 1) * ny) * NV + BZF] - U[(j + (i - 1) * ny) * NV + BZF]) / (2.0 * dx);
+            jZ = (U[(j + (i + 1) * ny) * NV + BYF] - U[(j + (i - 1) * ny) * NV + BYF]) / (2.0 * dx)
+               - (U[(j + 1 + i * ny) * NV + BXF] - U[(j - 1 + i * ny) * NV + BXF]) / (2.0 * dy);
+            eta = eta_at(p, i, j);
+            etaJY = eta * jY;
+            etaJZ = eta * jZ;
+            etaJYBZ = etaJY * U[(j + i * ny) * NV + BZF];
+            etaJZBY = etaJZ * U[(j + i * ny) * NV + BYF];
+
+            jY = -(U[(j + (i + 2) * ny) * NV + BZF] - U[(j + i * ny) * NV + BZF]) / (2.0 * dx);
+            jZ = (U[(j + (i + 2) * ny) * NV + BYF] - U[(j + i * ny) * NV + BYF]) / (2.0 * dx)
+               - (U[(j + 1 + (i + 1) * ny) * NV + BXF] - U[(j - 1 + (i + 1) * ny) * NV + BXF]) / (2.0 * dy);
+            eta = eta_at(p, i + 1, j);
+            etaJYPlus1 = eta * jY;
+            etaJZPlus1 = eta * jZ;
+            etaJYBZPlus1 = etaJYPlus1 * U[(j + (i + 1) * ny) * NV + BZF];
+            etaJZBYPlus1 = etaJZPlus1 * U[(j + (i + 1) * ny) * NV + BYF];
+
+            double *f = &F[(j + i * ny) * 8];
+            f[5] -= 0.5 * (etaJZ + etaJZPlus1);
+            f[6] += 0.5 * (etaJY + etaJYPlus1);
+            f[7] += 0.5 * (etaJYBZ + etaJYBZPlus1) - 0.5 * (etaJZBY + etaJZBYPlus1);
+        }
+    }
+}
+
+/* y-direction flux G at interface j+1/2 (HLLD::calculateFluxG,
+   hlld.cu:134-233, + resistive hook main_plasmoid.cu:234-274).  The y sweep
+   runs the x-sweep arithmetic on the permuted cell
+   (rho, rhoV, rhoW, rhoU, bY, bZ, bX, e) and un-permutes the flux. */
+static void flux_y(const orc_params *p, const double *Uc, double *G, double *T,
+                   double *dQ, double *dQL, double *dQR)
+{
+    const int nx = p->nx, ny = p->ny, N = nx * ny;
+    const double gm = p->gamma, EPS = p->eps;
+    const double qnan = NAN;
+
+    /* shuffleForTmpUForFluxG_kernel */
+    for (int k = 0; k < N; ++k) {
+        const double *u = &Uc[k * NV];
+        double *t = &T[k * NV];
+        t[0] = u[RHO]; t[1] = u[MY]; t[2] = u[MZ]; t[3] = u[MX];
+        t[4] = u[BYF]; t[5] = u[BZF]; t[6] = u[BXF]; t[7] = u[EN];
+    }
+    /* setPhysicalParameterY: k in [0, N-1). */
+    for (int k = 0; k < N; ++k) {
+        if (k < N - 1) basic_param(&T[k * NV], &T[(k + 1) * NV], gm, &dQ[k * 8]);
+        else for (int c = 0; c < 8; ++c) dQ[k * 8 + c] = qnan;
+    }
+    /* getLeftQY: k in [1, N-1).  getRightQY: k in [0, N-2).  Entries that
+       wrap across a column (j = 0 or j >= ny-2) mix neighbouring columns in
+       the reference; they are poisoned here. */
+    #pragma omp parallel for schedule(static)
+    for (int k = 0; k < N; ++k) {
+        int j = k % ny;
+        if (k >= 1 && k < N - 1 && j >= 1 && j <= ny - 2)
+            muscl_left(&dQ[(k - 1) * 8], &dQ[k * 8], &dQ[(k + 1) * 8], EPS, &dQL[k * 8]);
+        else for (int c = 0; c < 8; ++c) dQL[k * 8 + c] = qnan;
+        if (k < N - 2 && j <= ny - 3)
+            muscl_right(&dQ[k * 8], &dQ[(k + 1) * 8], &dQ[(k + 2) * 8], EPS, &dQR[k * 8]);
+        else for (int c = 0; c < 8; ++c) dQR[k * 8 + c] = qnan;
+    }
+    #pragma omp parallel for schedule(static)
+    for (int k = 0; k < N; ++k) {
+        double f[8];
+        hlld_flux(&dQL[k * 8], &dQR[k * 8], gm, EPS, f);
+        /* shuffleForFluxG_kernel: f1<-f3, f2<-f1, f3<-f2, f4<-f6, f5<-f4, f6<-f5 */
+        double *g = &G[k * 8];
+        g[0] = f[0]; g[1] = f[3]; g[2] = f[1]; g[3] = f[2];
+        g[4] = f[6]; g[5] = f[4]; g[6] = f[5]; g[7] = f[7];
+    }
+
+    const double dx = p->dx, dy = p->dy;
+    #pragma omp parallel for schedule(static)
+    for (int i = 1; i < nx - 2; ++i) {
+        for (int j = 1; j < ny - 2; ++j) {
+            const double *U = Uc;
+            double jX, jZ, eta;
+            double etaJX, etaJXPlus1, etaJZ, etaJZPlus1;
+            double etaJZBX, etaJZBXPlus1, etaJXBZ, etaJXBZPlus1;
+            jX = (U[(j + 1 + i * ny) * NV + BZF] - U[(j - 1 + i * ny) * NV + BZF]) / (2.0 * dy);
+            jZ = (U[(j + (i + 1) * ny) * NV + BYF] - U[(j + (i - 1) * ny) * NV + BYF]) / (2.0 * dx)
+               - (U[(j + 1 + i * ny) * NV + BXF] - U[(j - 1 + i * ny) * NV + BXF]) / (2.0 * dy);
+            eta = eta_at(p, i, j);
+            etaJX = eta * jX;
+            etaJZ = eta * jZ;
+            etaJXBZ = etaJX * U[(j + i * ny) * NV + BZF];
+            etaJZBX = etaJZ * U[(j + i * ny) * NV + BXF];
+
+            jX = (U[(j + 2 + i * ny) * NV + BZF] - U[(j + i * ny) * NV + BZF]) / (2.0 * dy);
+            jZ = (U[(j + 1 + (i + 1) * ny) * NV + BYF] - U[(j + 1 + (i - 1) * ny) * NV + BYF]) / (2.0 * dx)
+               - (U[(j + 2 + i * ny) * NV + BXF] - U[(j + i * ny) * NV + BXF]) / (2.0 * dy);
+            eta = eta_at(p, i, j + 1);
+            etaJXPlus1 = eta * jX;
+            etaJZPlus1 = eta * jZ;
+            etaJXBZPlus1 = etaJXPlus1 * U[(j + 1 + i * ny) * NV + BZF];
+            etaJZBXPlus1 = etaJZPlus1 * U[(j + 1 + i * ny) * NV + BXF];
+
+            double *g = &G[(j + i * ny) * 8];
+            g[4] += 0.5 * (etaJZ + etaJZPlus1);
+            g[6] -= 0.5 * (etaJX + etaJXPlus1);
+            g[7] += 0.5 * (etaJZBX + etaJZBXPlus1) - 0.5 * (etaJXBZ + etaJXBZPlus1);
+        }
+    }
+}
+
+/* resistiveMHD_2D.cu:313-368 shiftUToCenterForCT, in place. */
+static void shift_to_center(const orc_params *p, double *U, double *tmp)
+{
+    const int nx = p->nx, ny = p->ny, N = nx * ny;
+    for (int k = 0; k < N; ++k) tmp[k] = U[k * NV + BXF];
+    for (int i = 1; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            U[(j + i * ny) * NV + BXF] = 0.5 * (tmp[j + i * ny] + tmp[j + (i - 1) * ny]);
+    for (int k = 0; k < N; ++k) tmp[k] = U[k * NV + BYF];
+    for (int i = 0; i < nx; ++i)
+        for (int j = 1; j < ny; ++j)
+            U[(j + i * ny) * NV + BYF] = 0.5 * (tmp[j + i * ny] + tmp[j - 1 + i * ny]);
+}
+
+/* resistiveMHD_2D.cu:371-426 backUToCenterHalfForCT, in place. */
+static void back_to_face(const orc_params *p, double *U, double *tmp)
+{
+    const int nx = p->nx, ny = p->ny, N = nx * ny;
+    for (int k = 0; k < N; ++k) tmp[k] = U[k * NV + BXF];
+    for (int i = 0; i < nx - 1; ++i)
+        for (int j = 0; j < ny; ++j)
+            U[(j + i * ny) * NV + BXF] = 0.5 * (tmp[j + i * ny] + tmp[j + (i + 1) * ny]);
+    for (int k = 0; k < N; ++k) tmp[k] = U[k * NV + BYF];
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny - 1; ++j)
+            U[(j + i * ny) * NV + BYF] = 0.5 * (tmp[j + i * ny] + tmp[j + 1 + i * ny]);
+}
+
+/* ct.cu:22-41 getEZVector_kernel: corner Ez for i < nx-1, j < ny-1; the
+   reference never writes the last row/column of eZVector (zero-initialised
+   there), which only reaches ghost faces. */
+static void corner_ez(const orc_params *p, const double *F, const double *G, double *Ez)
+{
+    const int nx = p->nx, ny = p->ny;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            if (i < nx - 1 && j < ny - 1) {
+                double eZG1 = G[(j + i * ny) * 8 + 4];
+                double eZG2 = G[(j + (i + 1) * ny) * 8 + 4];
+                double eZF1 = -1.0 * F[(j + i * ny) * 8 + 5];
+                double eZF2 = -1.0 * F[(j + 1 + i * ny) * 8 + 5];
+                Ez[j + i * ny] = 0.25 * (eZG1 + eZG2 + eZF1 + eZF2);
+            } else {
+                Ez[j + i * ny] = NAN;
+            }
+        }
+}
+
+/* ct.cu:44-59 CT_kernel. */
+static void ct_update(const orc_params *p, const double *bXOld, const double *bYOld,
+                      const double *Ez, double dt, double *U)
+{
+    const int nx = p->nx, ny = p->ny;
+    for (int i = 1; i < nx; ++i)
+        for (int j = 1; j < ny; ++j) {
+            U[(j + i * ny) * NV + BXF] = bXOld[j + i * ny]
+                - dt / p->dy * (Ez[j + i * ny] - Ez[j - 1 + i * ny]);
+            U[(j + i * ny) * NV + BYF] = bYOld[j + i * ny]
+                + dt / p->dx * (Ez[j + i * ny] - Ez[j + (i - 1) * ny]);
+        }
+}
+
+/* resistiveMHD_2D.cu:247-291: CFL dt over every cell (ghosts included),
+   using the stored face B as if it were cell-centred, then the diffusive
+   limit with the scalar eta. */
+double orc_calc_dt(const orc_params *p, const double *U)
+{
+    const int N = p->nx * p->ny;
+    const double gm = p->gamma;
+    double dtMin = 0.0;
+    for (int k = 0; k < N; ++k) {
+        const double *c = &U[k * NV];
+        double rho = c[RHO];
+        double u = c[MX] / rho, v = c[MY] / rho, w = c[MZ] / rho;
+        double bX = c[BXF], bY = c[BYF], bZ = c[BZF], e = c[EN];
+        double pr = (gm - 1.0)
+                  * (e - 0.5 * rho * (u * u + v * v + w * w)
+                  - 0.5 * (bX * bX + bY * bY + bZ * bZ));
+        double cs = sqrt(gm * pr / rho);
+        double ca = sqrt((bX * bX + bY * bY + bZ * bZ) / rho);
+        double sx = fabs(u) + sqrt(cs * cs + ca * ca);
+        double sy = fabs(v) + sqrt(cs * cs + ca * ca);
+        double r = 1.0 / (sx / p->dx + sy / p->dy + p->eps);
+        /* thrust::min_element keeps the first minimum: replace only on '<'. */
+        if (k == 0 || r < dtMin) dtMin = r;
+    }
+    double a = p->dx * p->dx / p->eta, b = p->dy * p->dy / p->eta;
+    return fmin(dtMin, fmin(a, b)) * p->cfl;
+}
+
+/* resistiveMHD_2D.cu:294-309. */
+int orc_is_crashed(const orc_params *p, const double *U)
+{
+    const int N = p->nx * p->ny;
+    for (int k = 0; k < N; ++k) if (isnan(U[k * NV + EN])) return 1;
+    return 0;
+}
+
+/* boundary.cu:4-57 periodicBoundaryX2nd_kernel + :59-110 Y2nd. */
+static void periodic_boundary(const orc_params *p, double *U)
+{
+    const int nx = p->nx, ny = p->ny;
+    for (int j = 0; j < ny; ++j)
+        for (int g = 0; g < 3; ++g) {
+            memcpy(&U[(j + g * ny) * NV], &U[(j + (nx - 6 + g) * ny) * NV], NV * sizeof(double));
+            memcpy(&U[(j + (nx - 3 + g) * ny) * NV], &U[(j + (3 + g) * ny) * NV], NV * sizeof(double));
+        }
+    for (int i = 0; i < nx; ++i)
+        for (int g = 0; g < 3; ++g) {
+            memcpy(&U[(g + i * ny) * NV], &U[(ny - 6 + g + i * ny) * NV], NV * sizeof(double));
+            memcpy(&U[(ny - 3 + g + i * ny) * NV], &U[(3 + g + i * ny) * NV], NV * sizeof(double));
+        }
+}
+
+static void copy_except(double *dst, const double *src, int skip)
+{
+    for (int f = 0; f < NV; ++f) if (f != skip) dst[f] = src[f];
+}
+
+/* symmetricXY/boundary.cu:4-104 symmetricBoundaryX2nd (+BX) and :107-205
+   symmetricBoundaryY2nd (+BY): mirror copies of every field except the
+   normal B, whose ghosts are integrated from the discrete div B = 0. */
+static void symmetric_boundary(const orc_params *p, double *U)
+{
+    const int nx = p->nx, ny = p->ny;
+    const double dx = p->dx, dy = p->dy;
+#define C(i, j) (&U[((j) + (i) * ny) * NV])
+    for (int j = 0; j < ny; ++j) {
+        copy_except(C(0, j), C(5, j), BXF);
+        copy_except(C(1, j), C(4, j), BXF);
+        copy_except(C(2, j), C(3, j), BXF);
+        copy_except(C(nx - 1, j), C(nx - 6, j), BXF);
+        copy_except(C(nx - 2, j), C(nx - 5, j), BXF);
+        copy_except(C(nx - 3, j), C(nx - 4, j), BXF);
+    }
+    for (int j = 0; j < ny; ++j) {
+        if (0 < j) {
+            C(2, j)[BXF] = C(3, j)[BXF] + (C(3, j)[BYF] - C(3, j - 1)[BYF]) / dy * dx;
+            C(1, j)[BXF] = C(2, j)[BXF] + (C(2, j)[BYF] - C(2, j - 1)[BYF]) / dy * dx;
+            C(0, j)[BXF] = C(1, j)[BXF] + (C(1, j)[BYF] - C(1, j - 1)[BYF]) / dy * dx;
+            C(nx - 3, j)[BXF] = C(nx - 4, j)[BXF] - (C(nx - 3, j)[BYF] - C(nx - 3, j - 1)[BYF]) / dy * dx;
+            C(nx - 2, j)[BXF] = C(nx - 3, j)[BXF] - (C(nx - 2, j)[BYF] - C(nx - 2, j - 1)[BYF]) / dy * dx;
+            C(nx - 1, j)[BXF] = C(nx - 2, j)[BXF] - (C(nx - 1, j)[BYF] - C(nx - 1, j - 1)[BYF]) / dy * dx;
+        }
+        if (j == 0) {
+            C(2, j)[BXF] = C(3, j)[BXF];
+            C(1, j)[BXF] = C(2, j)[BXF];
+            C(0, j)[BXF] = C(1, j)[BXF];
+            C(nx - 3, j)[BXF] = C(nx - 4, j)[BXF];
+            C(nx - 2, j)[BXF] = C(nx - 3, j)[BXF];
+            C(nx - 1, j)[BXF] = C(nx - 2, j)[BXF];
+        }
+    }
+    for (int i = 0; i < nx; ++i) {
+        copy_except(C(i, 0), C(i, 5), BYF);
+        copy_except(C(i, 1), C(i, 4), BYF);
+        copy_except(C(i, 2), C(i, 3), BYF);
+        copy_except(C(i, ny - 1), C(i, ny - 6), BYF);
+        copy_except(C(i, ny - 2), C(i, ny - 5), BYF);
+        copy_except(C(i, ny - 3), C(i, ny - 4), BYF);
+    }
+    for (int i = 0; i < nx; ++i) {
+        if (0 < i) {
+            C(i, 2)[BYF] = C(i, 3)[BYF] + (C(i, 3)[BXF] - C(i - 1, 3)[BXF]) / dx * dy;
+            C(i, 1)[BYF] = C(i, 2)[BYF] + (C(i, 2)[BXF] - C(i - 1, 2)[BXF]) / dx * dy;
+            C(i, 0)[BYF] = C(i, 1)[BYF] + (C(i, 1)[BXF] - C(i - 1, 1)[BXF]) / dx * dy;
+            C(i, ny - 3)[BYF] = C(i, ny - 4)[BYF] - (C(i, ny - 3)[BXF] - C(i - 1, ny - 3)[BXF]) / dx * dy;
+            C(i, ny - 2)[BYF] = C(i, ny - 3)[BYF] - (C(i, ny - 2)[BXF] - C(i - 1, ny - 2)[BXF]) / dx * dy;
+            C(i, ny - 1)[BYF] = C(i, ny - 2)[BYF] - (C(i, ny - 1)[BXF] - C(i - 1, ny - 1)[BXF]) / dx * dy;
+        }
+        if (i == 0) {
+            C(i, 2)[BYF] = C(i, 3)[BYF];
+            C(i, 1)[BYF] = C(i, 2)[BYF];
+            C(i, 0)[BYF] = C(i, 1)[BYF];
+            C(i, ny - 3)[BYF] = C(i, ny - 4)[BYF];
+            C(i, ny - 2)[BYF] = C(i, ny - 3)[BYF];
+            C(i, ny - 1)[BYF] = C(i, ny - 2)[BYF];
+        }
+    }
+#undef C
+}
+
+void orc_boundary(const orc_params *p, double *U)
+{
+    if (p->bc == ORC_BC_SYMMETRIC) symmetric_boundary(p, U);
+    else periodic_boundary(p, U);
+}
+
+size_t orc_work_doubles(int nx, int ny)
+{
+    size_t N = (size_t)nx * ny;
+    /* UBar, T, F, G, dQ, dQL, dQR (8 each) + bXOld, bYOld, tmp, Ez */
+    return N * (7 * 8 + 4);
+}
+
+/* resistiveMHD_2D.cu:133-195 oneStepRK2.  U is updated in place; work must
+   hold orc_work_doubles(nx, ny) doubles.  Returns the dt used. */
+double orc_step(const orc_params *p, double *U, double *work)
+{
+    const int nx = p->nx, ny = p->ny, N = nx * ny;
+    double *UBar = work;
+    double *T = UBar + (size_t)N * 8;
+    double *F = T + (size_t)N * 8;
+    double *G = F + (size_t)N * 8;
+    double *dQ = G + (size_t)N * 8;
+    double *dQL = dQ + (size_t)N * 8;
+    double *dQR = dQL + (size_t)N * 8;
+    double *bXOld = dQR + (size_t)N * 8;
+    double *bYOld = bXOld + N;
+    double *tmp = bYOld + N;
+    double *Ez = tmp + N;
+
+    for (int k = 0; k < N; ++k) { bXOld[k] = U[k * NV + BXF]; bYOld[k] = U[k * NV + BYF]; }
+    memcpy(UBar, U, (size_t)N * NV * sizeof(double));
+
+    const double dt = orc_calc_dt(p, U);
+    const double dx = p->dx, dy = p->dy;
+
+    shift_to_center(p, U, tmp);
+    flux_x(p, U, F, dQ, dQL, dQR);
+    flux_y(p, U, G, T, dQ, dQL, dQR);
+    back_to_face(p, U, tmp);
+
+    /* oneStepFirstFunctor over k in [ny, N). */
+    #pragma omp parallel for schedule(static)
+    for (int k = ny; k < N; ++k) {
+        const double *u = &U[k * NV];
+        const double *f = &F[k * 8], *fm = &F[(k - ny) * 8];
+        const double *g = &G[k * 8], *gm = &G[(k - 1) * 8];
+        double *ub = &UBar[k * NV];
+        for (int c = 0; c < 8; ++c)
+            ub[c] = u[c] - dt / dx * (f[c] - fm[c]) - dt / dy * (g[c] - gm[c]);
+    }
+
+    corner_ez(p, F, G, Ez);
+    ct_update(p, bXOld, bYOld, Ez, dt, UBar);
+    orc_boundary(p, UBar);
+
+    shift_to_center(p, UBar, tmp);
+    flux_x(p, UBar, F, dQ, dQL, dQR);
+    flux_y(p, UBar, G, T, dQ, dQL, dQR);
+    back_to_face(p, UBar, tmp);
+
+    /* oneStepSecondFunctor over k in [ny, N). */
+    #pragma omp parallel for schedule(static)
+    for (int k = ny; k < N; ++k) {
+        double *u = &U[k * NV];
+        const double *ub = &UBar[k * NV];
+        const double *f = &F[k * 8], *fm = &F[(k - ny) * 8];
+        const double *g = &G[k * 8], *gm = &G[(k - 1) * 8];
+        for (int c = 0; c < 8; ++c)
+            u[c] = 0.5 * (u[c] + ub[c]
+                 - dt / dx * (f[c] - fm[c])
+                 - dt / dy * (g[c] - gm[c]));
+    }
+
+    /* CT again with the stage-1 corner EMF (setOldFlux2D is not called for
+       stage 2). */
+    ct_update(p, bXOld, bYOld, Ez, dt, U);
+    orc_boundary(p, U);
+    return dt;
+}
+
+/* Runs nsteps steps; dts (may be NULL) receives each step's dt.  Returns 0,
+   or 1 + the step index at which the crash check (NaN energy) fired, after
+   which no further step is taken, as the reference drivers do. */
+int orc_run(const orc_params *p, double *U, int nsteps, double *dts)
+{
+    size_t nw = orc_work_doubles(p->nx, p->ny);
+    double *work = (double *)malloc(nw * sizeof(double));
+    if (!work) return -1;
+    int rc = 0;
+    for (int s = 0; s < nsteps; ++s) {
+        double dt = orc_step(p, U, work);
+        if (dts) dts[s] = dt;
+        if (orc_is_crashed(p, U)) { rc = 1 + s; break; }
+    }
+    free(work);
+    return rc;
+}

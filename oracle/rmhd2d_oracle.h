@@ -1,0 +1,39 @@
+/*
+ * rmhd2d_oracle.h -- CPU restatement of the reference's 2D resistive-MHD RK2
+ * step.  TEST INFRASTRUCTURE ONLY: the parity checker for the CUDA path,
+ * never linked into the product.  See rmhd2d_oracle.c for the reference
+ * file:line each function restates.
+ */
+#ifndef RMHD2D_ORACLE_H
+#define RMHD2D_ORACLE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_BC_PERIODIC = 0, ORC_BC_SYMMETRIC = 1 };
+
+typedef struct {
+    int nx, ny;               /* cells per direction, 3 ghost layers per side included */
+    double dx, dy;
+    double gamma;             /* gamma_mhd */
+    double cfl;               /* CFL */
+    double eps;               /* EPS regulariser */
+    double eta;               /* scalar eta: resistive term when eta_table is NULL, and dt limit */
+    const double *eta_table;  /* optional cell-centred eta, k = j + i*ny */
+    int bc;                   /* ORC_BC_PERIODIC or ORC_BC_SYMMETRIC (both directions) */
+} orc_params;
+
+double orc_calc_dt(const orc_params *p, const double *U);
+int orc_is_crashed(const orc_params *p, const double *U);
+void orc_boundary(const orc_params *p, double *U);
+size_t orc_work_doubles(int nx, int ny);
+double orc_step(const orc_params *p, double *U, double *work);
+int orc_run(const orc_params *p, double *U, int nsteps, double *dts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

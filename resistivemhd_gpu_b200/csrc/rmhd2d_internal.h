@@ -1,0 +1,46 @@
+// rmhd2d_internal.h -- shared between the C-ABI host code and the CUDA
+// kernels of librmhd2d.  Not part of the public interface (include/rmhd2d.h).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace rmhd2d {
+
+// Field order of a cell, identical to the reference's ConservationParameter
+// (lib_ResistiveMHD_2D_GPU_periodicXY/conservation_parameter_struct.hpp:5-27).
+enum Field { RHO = 0, MX = 1, MY = 2, MZ = 3, BXF = 4, BYF = 5, BZF = 6, EN = 7, NFIELD = 8 };
+
+enum Bc { BC_PERIODIC = 0, BC_SYMMETRIC = 1 };
+
+// Geometry and physics constants passed by value to every kernel.
+struct Grid {
+    int nx, ny;          // cells incl. 3 ghost layers per side
+    int pitch;           // doubles between consecutive i rows of a plane (>= ny, multiple of 32)
+    long long plane;     // doubles per field plane = nx * pitch
+    double dx, dy;
+    double gamma, cfl, eps, eta;
+    int bc;
+};
+
+// Device-side control block (one per solver), zero-initialised at create.
+struct Control {
+    unsigned long long amax[2];  // max over cells of |u|/dx + ... as raw bits, per step parity
+    double dt;                   // dt of the most recent step (reference's global dt)
+    double total_time;           // sum of dt over the steps taken
+    int crashed;                 // NaN energy seen in the newest state
+    int error;                   // kernel-side error code (bounded wait expired, ...)
+    int pad[2];
+};
+
+enum KernelError { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };
+
+// Tile of the fused stage kernel: TI cells along x (i) by TJ along y (j).
+constexpr int TI = 8;
+constexpr int TJ = 32;
+constexpr int HALO = 3;
+constexpr int UI = TI + 2 * HALO;  // staged rows
+constexpr int UJ = TJ + 2 * HALO;  // staged columns (TMA inner box: UJ * 8 bytes, multiple of 16)
+constexpr int STAGE_THREADS = TI * TJ;
+
+}  // namespace rmhd2d
