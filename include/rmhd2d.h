@@ -1,0 +1,163 @@
+/*
+ * rmhd2d.h -- C ABI of librmhd2d, a B200-native (sm_100a) 2D resistive-MHD
+ * RK2 step that drops in for the single-GPU Thrust library of
+ * keita-akutagawa/ResistiveMHD_GPU
+ * (ResistiveMHD_singleGPU_thrust/lib_ResistiveMHD_2D_GPU_periodicXY and
+ *  .../lib_ResistiveMHD_2D_GPU_symmetricXY).
+ *
+ * Plain C types only: pointers, sizes, ints and doubles.  Every function
+ * returns an rmhd2d_status (0 = success).  The reference library performs no
+ * error checks at all; here a failure leaves the solver unchanged where
+ * possible and rmhd2d_last_error() describes it.
+ *
+ * State layout at the boundary is the reference's: an array of nx*ny cells,
+ * cell k = j + i*ny (y fastest), each cell 8 doubles in the order of the
+ * reference's ConservationParameter (conservation_parameter_struct.hpp:5-27):
+ *   rho, rhoU, rhoV, rhoW, bX, bY, bZ, e
+ * nx and ny include 3 ghost layers per side (the periodic period is nx-6);
+ * bX of cell (i,j) lives on the x-face i+1/2 and bY on the y-face j+1/2.
+ *
+ * Threading: a solver is used from one host thread at a time.  Work is
+ * enqueued on the solver's CUDA stream; functions that return host values
+ * (rmhd2d_get_dt, rmhd2d_check_crashed, rmhd2d_get_state, ...) synchronise
+ * that stream.  Several solvers may coexist in one process (the reference
+ * allows one, through process-global __constant__ state).
+ */
+#ifndef RMHD2D_H
+#define RMHD2D_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RMHD2D_ABI_VERSION 1
+#define RMHD2D_GHOST 3
+
+typedef enum {
+    RMHD2D_OK = 0,
+    RMHD2D_ERR_INVALID = 1,     /* bad argument or configuration */
+    RMHD2D_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    RMHD2D_ERR_NO_DEVICE = 3,   /* no usable sm_100 device */
+    RMHD2D_ERR_STATE = 4,       /* call not valid in the solver's current state */
+    RMHD2D_ERR_IO = 5,          /* file could not be written or read */
+    RMHD2D_ERR_KERNEL = 6       /* a kernel reported an internal error (bounded wait expired) */
+} rmhd2d_status;
+
+typedef enum {
+    RMHD2D_BC_PERIODIC = 0,     /* Boundary::periodicBoundaryX2nd/Y2nd (TP boundary.cu:4-141) */
+    RMHD2D_BC_SYMMETRIC = 1     /* Boundary::symmetricBoundaryX2nd/Y2nd (TS boundary.cu:4-206) */
+} rmhd2d_bc;
+
+typedef enum {
+    /* FP64, bit-identical to the reference evaluated in IEEE binary64 without
+       fused multiply-add (the reference's own host build). */
+    RMHD2D_FP64_EXACT = 0,
+    /* FP64 with fused multiply-add and only the selected HLLD candidate
+       fluxes; differs from EXACT by rounding only. */
+    RMHD2D_FP64_FAST = 1
+} rmhd2d_precision;
+
+typedef struct {
+    int nx, ny;                 /* cells per direction incl. 3 ghost layers per side; both >= 12 */
+    double dx, dy;              /* cell sizes (reference const.hpp:7,12) */
+    double gamma_mhd;           /* ratio of specific heats (const.hpp:18) */
+    double cfl;                 /* CFL number (const.hpp:17) */
+    double eps;                 /* EPS regulariser of the reference (const.hpp:4) */
+    double eta;                 /* scalar eta: the resistive term when no eta table is set,
+                                   and always the diffusive dt limit dx^2/eta (resistiveMHD_2D.cu:288) */
+    int bc;                     /* rmhd2d_bc, applied in x and y */
+    int precision;              /* rmhd2d_precision */
+    int device;                 /* CUDA device ordinal */
+    void *stream;               /* cudaStream_t to enqueue on, or NULL for a solver-owned stream */
+} rmhd2d_config;
+
+typedef struct rmhd2d_solver rmhd2d_solver;
+
+/* Fills cfg with defaults (gamma 5/3, cfl 0.4, eps 1e-20, periodic, FP64 exact). */
+void rmhd2d_config_default(rmhd2d_config *cfg);
+
+/* Replaces the constructor ResistiveMHD2D::ResistiveMHD2D()
+   (TP resistiveMHD_2D.cu:11-22) together with the link-time globals of
+   const.hpp:4-25 and initializeDeviceConstants() (const.cu:4-24). */
+int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out);
+int rmhd2d_destroy(rmhd2d_solver *s);
+
+/* Replaces the body of the user's ResistiveMHD2D::initializeU()
+   (e.g. examples2D/plasmoid/main_plasmoid.cu:132-156): uploads a full state
+   (ghosts included) from host memory in the layout above.  With
+   apply_boundary != 0 the boundary of the configured kind is applied
+   afterwards, as the reference drivers do at the end of initializeU. */
+int rmhd2d_set_state(rmhd2d_solver *s, const double *host_state, int apply_boundary);
+
+/* Same as rmhd2d_set_state from device memory (any CUDA-visible pointer). */
+int rmhd2d_set_state_device(rmhd2d_solver *s, const double *device_state, int apply_boundary);
+
+/* Replaces ResistiveMHD2D::getU() (TP resistiveMHD_2D.cu:431-434): copies
+   the full state into host memory (nx*ny*8 doubles). */
+int rmhd2d_get_state(rmhd2d_solver *s, double *host_state);
+
+/* Sets a cell-centred resistivity table (nx*ny doubles, k = j + i*ny) used
+   by the resistive flux instead of the uniform eta; NULL returns to uniform
+   eta.  Replaces the driver's getEta() (main_plasmoid.cu:159-172) sampled at
+   cell centres, as the driver's addResistiveTermToFluxF/G kernels sample it. */
+int rmhd2d_set_eta_table(rmhd2d_solver *s, const double *host_eta);
+
+/* Replaces Boundary::periodicBoundaryX2nd + Y2nd (TP boundary.cu:4-141) or
+   symmetricBoundaryX2nd + Y2nd (TS boundary.cu:4-206) applied to U. */
+int rmhd2d_apply_boundary(rmhd2d_solver *s);
+
+/* Replaces ResistiveMHD2D::calculateDt() (TP resistiveMHD_2D.cu:277-291):
+   returns the dt the next step will use, CFL * min(min_cells 1/(|u|/dx + ...),
+   dx^2/eta, dy^2/eta). */
+int rmhd2d_calculate_dt(rmhd2d_solver *s, double *dt);
+
+/* Replaces ResistiveMHD2D::oneStepRK2() (TP resistiveMHD_2D.cu:133-195,
+   TS resistiveMHD_2D.cu:133-195): one Heun RK2 step with constrained
+   transport.  Enqueued asynchronously. */
+int rmhd2d_step_rk2(rmhd2d_solver *s);
+
+/* nsteps calls of rmhd2d_step_rk2, replayed from a captured CUDA graph. */
+int rmhd2d_run(rmhd2d_solver *s, int nsteps);
+
+/* dt of the most recent step: the reference's global `dt` after
+   oneStepRK2 (const.hpp:20). */
+int rmhd2d_get_dt(rmhd2d_solver *s, double *dt);
+
+/* Sum of the dt of all steps taken: the drivers' `totalTime += dt`
+   (main_plasmoid.cu:325). */
+int rmhd2d_get_total_time(rmhd2d_solver *s, double *t);
+
+/* Replaces ResistiveMHD2D::checkCalculationIsCrashed()
+   (TP resistiveMHD_2D.cu:294-309): *crashed = 1 if any cell of the current
+   state has a NaN energy. */
+int rmhd2d_check_crashed(rmhd2d_solver *s, int *crashed);
+
+/* Replaces ResistiveMHD2D::save(dir, name, step) (TP resistiveMHD_2D.cu:198-244):
+   writes dir/name_step.bin, nx*ny cells of 8 little-endian doubles in the
+   field order above, i-major, byte-identical to the reference. */
+int rmhd2d_save(rmhd2d_solver *s, const char *directory, const char *name_without_step, int step);
+
+/* Reads a file written by rmhd2d_save (or the reference's save()) back into
+   the solver state.  No counterpart in the reference (it cannot resume). */
+int rmhd2d_load(rmhd2d_solver *s, const char *path);
+
+/* Writes a host state in the save() format; no GPU needed.  Used by the
+   save/load round trip and by host tools. */
+int rmhd2d_write_snapshot(const char *path, const double *host_state, int nx, int ny);
+
+/* Text of the last error of this solver (or of the last failed create when
+   s is NULL); never NULL. */
+const char *rmhd2d_last_error(const rmhd2d_solver *s);
+
+/* Name of a status code. */
+const char *rmhd2d_status_string(int status);
+
+/* ABI version (RMHD2D_ABI_VERSION of the library). */
+int rmhd2d_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,498 @@
+// api.cu -- host implementation of the C ABI declared in include/rmhd2d.h.
+//
+// A solver owns two pitched SoA states (A: the current state U^n, B: the
+// stage-1 state U*), an optional eta plane, the symmetric-wall row of CT'd
+// bY, and a device control block (CFL maxima, dt, total time, crash and
+// error flags).  One RK2 step is four launches on the solver's stream:
+//
+//   stage 1 (A -> B) ; boundary(B) ; stage 2 (B, A -> A) ; boundary(A) + CFL/NaN
+//
+// and the dt of step n+1 is reduced while step n finishes, so no host
+// synchronisation happens inside a step (the reference synchronises on
+// every boundary call and on the dt minimum, resistiveMHD_2D.cu:286-290).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rmhd2d.h"
+#include "aux_kernels.h"
+#include "rmhd2d_internal.h"
+#include "stage.cuh"
+
+using namespace rmhd2d;
+
+struct rmhd2d_solver {
+    rmhd2d_config cfg{};
+    Grid g{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    double *A = nullptr;         // current state, 8 planes
+    double *B = nullptr;         // stage-1 state / staging, 8 planes
+    double *eta = nullptr;       // eta plane or nullptr
+    double *row2 = nullptr;      // nx doubles
+    Control *ctl = nullptr;      // device control block
+    Control *ctl_host = nullptr; // pinned mirror for readback
+    CUtensorMap mapA{}, mapB{};
+    int parity = 0;
+    bool has_state = false;
+    long long steps = 0;
+    cudaGraphExec_t graph2[2] = {nullptr, nullptr};
+    std::string err;
+};
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_create_err = "";
+
+int fail(rmhd2d_solver *s, int code, const std::string &msg)
+{
+    if (s) {
+        s->err = msg;
+    } else {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_create_err = msg;
+    }
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(s, RMHD2D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+    } while (0)
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 3-D tensor map over one state: (j: ny, i: nx, field: 8), box (UJ, UI, 8).
+bool encode_state_map(CUtensorMap *map, const Grid &g, double *base)
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)g.ny, (cuuint64_t)g.nx, (cuuint64_t)NFIELD};
+    cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.plane * 8};
+    cuuint32_t box[3] = {(cuuint32_t)UJ, (cuuint32_t)UI, (cuuint32_t)NFIELD};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+int sync_and_check(rmhd2d_solver *s)
+{
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(s->ctl_host, s->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+    if (s->ctl_host->error != KERR_NONE)
+        return fail(s, RMHD2D_ERR_KERNEL, "a stage kernel's bounded wait for its staged tile expired");
+    return RMHD2D_OK;
+}
+
+// Re-reduces the CFL rate and crash flag of the current state into slot
+// `parity` (after a state change outside a step).
+int refresh_rate(rmhd2d_solver *s)
+{
+    CK(cudaMemsetAsync(&s->ctl->amax[s->parity], 0, sizeof(unsigned long long), s->stream));
+    CK(cudaMemsetAsync(&s->ctl->crashed, 0, sizeof(int), s->stream));
+    launch_rate(s->g, s->A, s->ctl, s->parity, 1, s->stream);
+    CK(cudaGetLastError());
+    return RMHD2D_OK;
+}
+
+int do_boundary(rmhd2d_solver *s)
+{
+    if (s->g.bc == BC_SYMMETRIC) launch_snapshot_row2(s->g, s->A, s->row2, s->stream);
+    launch_boundary(s->g, s->A, s->row2, nullptr, 0, s->stream);
+    CK(cudaGetLastError());
+    return RMHD2D_OK;
+}
+
+void enqueue_step(rmhd2d_solver *s, int parity)
+{
+    StageArgs a{};
+    a.g = s->g;
+    a.eta = s->eta;
+    a.row2 = s->g.bc == BC_SYMMETRIC ? s->row2 : nullptr;
+    a.ctl = s->ctl;
+    a.parity = parity;
+    auto launch = s->cfg.precision == RMHD2D_FP64_FAST ? fast::launch_stage : exact::launch_stage;
+    // stage 1: U^n (A) -> U* (B)
+    a.src = s->A;
+    a.un = s->A;
+    a.dst = s->B;
+    launch(1, &s->mapA, a, s->stream);
+    launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
+    // stage 2: (U*, U^n) -> U^{n+1} in A
+    a.src = s->B;
+    a.un = s->A;
+    a.dst = s->A;
+    launch(2, &s->mapB, a, s->stream);
+    launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
+}
+
+int upload_from_device_aos(rmhd2d_solver *s, const double *aos_dev, int apply_boundary)
+{
+    launch_aos_to_planes(s->g, aos_dev, s->A, s->stream);
+    CK(cudaGetLastError());
+    s->has_state = true;
+    if (apply_boundary) {
+        int rc = do_boundary(s);
+        if (rc) return rc;
+    }
+    return refresh_rate(s);
+}
+
+void destroy_graphs(rmhd2d_solver *s)
+{
+    for (auto &gx : s->graph2) {
+        if (gx) cudaGraphExecDestroy(gx);
+        gx = nullptr;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void rmhd2d_config_default(rmhd2d_config *c)
+{
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->nx = c->ny = 0;
+    c->dx = c->dy = 1.0;
+    c->gamma_mhd = 5.0 / 3.0;
+    c->cfl = 0.4;
+    c->eps = 1e-20;
+    c->eta = 0.0;
+    c->bc = RMHD2D_BC_PERIODIC;
+    c->precision = RMHD2D_FP64_EXACT;
+    c->device = 0;
+    c->stream = nullptr;
+}
+
+int rmhd2d_abi_version(void) { return RMHD2D_ABI_VERSION; }
+
+const char *rmhd2d_status_string(int st)
+{
+    switch (st) {
+    case RMHD2D_OK: return "ok";
+    case RMHD2D_ERR_INVALID: return "invalid argument";
+    case RMHD2D_ERR_CUDA: return "CUDA error";
+    case RMHD2D_ERR_NO_DEVICE: return "no sm_100 device";
+    case RMHD2D_ERR_STATE: return "invalid solver state";
+    case RMHD2D_ERR_IO: return "I/O error";
+    case RMHD2D_ERR_KERNEL: return "kernel error";
+    default: return "unknown status";
+    }
+}
+
+const char *rmhd2d_last_error(const rmhd2d_solver *s)
+{
+    if (s) return s->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_create_err.c_str();
+}
+
+int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
+{
+    rmhd2d_solver *s = nullptr;
+    if (!cfg || !out) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (cfg->nx < 12 || cfg->ny < 12) return fail(s, RMHD2D_ERR_INVALID, "nx and ny must be >= 12 (3 ghosts per side)");
+    if ((long long)cfg->nx * cfg->ny > (1LL << 31)) return fail(s, RMHD2D_ERR_INVALID, "grid too large");
+    if (!(cfg->dx > 0) || !(cfg->dy > 0)) return fail(s, RMHD2D_ERR_INVALID, "dx and dy must be positive");
+    if (!(cfg->gamma_mhd > 1.0)) return fail(s, RMHD2D_ERR_INVALID, "gamma_mhd must be > 1");
+    if (!(cfg->eta >= 0.0)) return fail(s, RMHD2D_ERR_INVALID, "eta must be >= 0");
+    if (cfg->bc != RMHD2D_BC_PERIODIC && cfg->bc != RMHD2D_BC_SYMMETRIC)
+        return fail(s, RMHD2D_ERR_INVALID, "unknown boundary kind");
+    if (cfg->precision != RMHD2D_FP64_EXACT && cfg->precision != RMHD2D_FP64_FAST)
+        return fail(s, RMHD2D_ERR_INVALID, "unknown precision");
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
+        return fail(s, RMHD2D_ERR_NO_DEVICE, "no CUDA device with that ordinal");
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major != 10 || prop.minor != 0)
+        return fail(s, RMHD2D_ERR_NO_DEVICE, "librmhd2d is built for sm_100a (B200) only");
+
+    s = new rmhd2d_solver();
+    s->cfg = *cfg;
+    s->device = cfg->device;
+    Grid &g = s->g;
+    g.nx = cfg->nx;
+    g.ny = cfg->ny;
+    g.pitch = (cfg->ny + 31) / 32 * 32;
+    g.plane = (long long)g.nx * g.pitch;
+    g.dx = cfg->dx;
+    g.dy = cfg->dy;
+    g.gamma = cfg->gamma_mhd;
+    g.cfl = cfg->cfl;
+    g.eps = cfg->eps;
+    g.eta = cfg->eta;
+    g.bc = cfg->bc;
+
+    auto bail = [&](int code, const std::string &msg) {
+        {
+            std::lock_guard<std::mutex> lk(g_err_mu);
+            g_create_err = msg;
+        }
+        rmhd2d_destroy(s);
+        return code;
+    };
+    if (cudaSetDevice(s->device) != cudaSuccess) return bail(RMHD2D_ERR_CUDA, "cudaSetDevice failed");
+    if (cfg->stream) {
+        s->stream = (cudaStream_t)cfg->stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(RMHD2D_ERR_CUDA, "cudaStreamCreate failed");
+        s->own_stream = true;
+    }
+    const size_t state_bytes = (size_t)g.plane * NFIELD * sizeof(double);
+    if (cudaMalloc(&s->A, state_bytes) != cudaSuccess || cudaMalloc(&s->B, state_bytes) != cudaSuccess ||
+        cudaMalloc(&s->row2, (size_t)g.nx * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&s->ctl, sizeof(Control)) != cudaSuccess ||
+        cudaMallocHost(&s->ctl_host, sizeof(Control)) != cudaSuccess)
+        return bail(RMHD2D_ERR_CUDA, "device allocation failed");
+    // Zero the planes so padding columns hold finite values.
+    if (cudaMemset(s->A, 0, state_bytes) != cudaSuccess || cudaMemset(s->B, 0, state_bytes) != cudaSuccess ||
+        cudaMemset(s->row2, 0, (size_t)g.nx * sizeof(double)) != cudaSuccess ||
+        cudaMemset(s->ctl, 0, sizeof(Control)) != cudaSuccess)
+        return bail(RMHD2D_ERR_CUDA, "device memset failed");
+    if (!encode_state_map(&s->mapA, g, s->A) || !encode_state_map(&s->mapB, g, s->B))
+        return bail(RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    *out = s;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_destroy(rmhd2d_solver *s)
+{
+    if (!s) return RMHD2D_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    destroy_graphs(s);
+    cudaFree(s->A);
+    cudaFree(s->B);
+    cudaFree(s->eta);
+    cudaFree(s->row2);
+    cudaFree(s->ctl);
+    if (s->ctl_host) cudaFreeHost(s->ctl_host);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_set_state(rmhd2d_solver *s, const double *host, int apply_boundary)
+{
+    if (!s || !host) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->g.nx * s->g.ny * NFIELD;
+    // B doubles as the AoS staging buffer (it holds no live data between steps).
+    CK(cudaMemcpyAsync(s->B, host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    return upload_from_device_aos(s, s->B, apply_boundary);
+}
+
+int rmhd2d_set_state_device(rmhd2d_solver *s, const double *dev, int apply_boundary)
+{
+    if (!s || !dev) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->g.nx * s->g.ny * NFIELD;
+    CK(cudaMemcpyAsync(s->B, dev, n * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    return upload_from_device_aos(s, s->B, apply_boundary);
+}
+
+int rmhd2d_get_state(rmhd2d_solver *s, double *host)
+{
+    if (!s || !host) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->g.nx * s->g.ny * NFIELD;
+    launch_planes_to_aos(s->g, s->A, s->B, s->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(host, s->B, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    return sync_and_check(s);
+}
+
+int rmhd2d_set_eta_table(rmhd2d_solver *s, const double *host_eta)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    destroy_graphs(s);
+    if (!host_eta) {
+        cudaFree(s->eta);
+        s->eta = nullptr;
+        return RMHD2D_OK;
+    }
+    if (!s->eta) {
+        CK(cudaMalloc(&s->eta, (size_t)s->g.plane * sizeof(double)));
+        CK(cudaMemsetAsync(s->eta, 0, (size_t)s->g.plane * sizeof(double), s->stream));
+    }
+    CK(cudaMemcpy2DAsync(s->eta, (size_t)s->g.pitch * sizeof(double), host_eta, (size_t)s->g.ny * sizeof(double),
+                         (size_t)s->g.ny * sizeof(double), (size_t)s->g.nx, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return RMHD2D_OK;
+}
+
+int rmhd2d_apply_boundary(rmhd2d_solver *s)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    int rc = do_boundary(s);
+    if (rc) return rc;
+    return refresh_rate(s);
+}
+
+int rmhd2d_calculate_dt(rmhd2d_solver *s, double *dt)
+{
+    if (!s || !dt) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    int rc = sync_and_check(s);
+    if (rc) return rc;
+    double amax;
+    std::memcpy(&amax, &s->ctl_host->amax[s->parity], sizeof(double));
+    const Grid &g = s->g;
+    const double dtMin = 1.0 / (amax + g.eps);
+    *dt = std::fmin(dtMin, std::fmin(g.dx * g.dx / g.eta, g.dy * g.dy / g.eta)) * g.cfl;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_step_rk2(rmhd2d_solver *s)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    enqueue_step(s, s->parity);
+    CK(cudaGetLastError());
+    s->parity ^= 1;
+    s->steps += 1;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_run(rmhd2d_solver *s, int nsteps)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (nsteps < 0) return fail(s, RMHD2D_ERR_INVALID, "nsteps < 0");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    while (nsteps >= 2) {
+        cudaGraphExec_t &ge = s->graph2[s->parity];
+        if (!ge) {
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_step(s, s->parity);
+            enqueue_step(s, s->parity ^ 1);
+            cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+            if (e != cudaSuccess) return fail(s, RMHD2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&ge, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                ge = nullptr;
+                return fail(s, RMHD2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            }
+        }
+        CK(cudaGraphLaunch(ge, s->stream));
+        s->steps += 2;
+        nsteps -= 2;
+    }
+    if (nsteps == 1) return rmhd2d_step_rk2(s);
+    return RMHD2D_OK;
+}
+
+int rmhd2d_get_dt(rmhd2d_solver *s, double *dt)
+{
+    if (!s || !dt) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(s->device));
+    int rc = sync_and_check(s);
+    if (rc) return rc;
+    *dt = s->ctl_host->dt;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_get_total_time(rmhd2d_solver *s, double *t)
+{
+    if (!s || !t) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(s->device));
+    int rc = sync_and_check(s);
+    if (rc) return rc;
+    *t = s->ctl_host->total_time;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_check_crashed(rmhd2d_solver *s, int *crashed)
+{
+    if (!s || !crashed) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    int rc = sync_and_check(s);
+    if (rc) return rc;
+    *crashed = s->ctl_host->crashed ? 1 : 0;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_write_snapshot(const char *path, const double *host_state, int nx, int ny)
+{
+    rmhd2d_solver *s = nullptr;
+    if (!path || !host_state || nx <= 0 || ny <= 0) return fail(s, RMHD2D_ERR_INVALID, "bad snapshot arguments");
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(s, RMHD2D_ERR_IO, std::string("cannot open ") + path);
+    // The reference's save() loops (resistiveMHD_2D.cu:214-243) emit every
+    // cell k = 0 .. nx*ny-1 in order, 8 raw doubles each.
+    const size_t n = (size_t)nx * ny * NFIELD;
+    const size_t w = std::fwrite(host_state, sizeof(double), n, f);
+    const int closed = std::fclose(f);
+    if (w != n || closed != 0) return fail(s, RMHD2D_ERR_IO, std::string("short write to ") + path);
+    return RMHD2D_OK;
+}
+
+int rmhd2d_save(rmhd2d_solver *s, const char *dir, const char *name, int step)
+{
+    if (!s || !dir || !name) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    std::vector<double> h((size_t)s->g.nx * s->g.ny * NFIELD);
+    int rc = rmhd2d_get_state(s, h.data());
+    if (rc) return rc;
+    const std::string path = std::string(dir) + "/" + name + "_" + std::to_string(step) + ".bin";
+    rc = rmhd2d_write_snapshot(path.c_str(), h.data(), s->g.nx, s->g.ny);
+    if (rc) return fail(s, rc, std::string("cannot write ") + path);
+    return RMHD2D_OK;
+}
+
+int rmhd2d_load(rmhd2d_solver *s, const char *path)
+{
+    if (!s || !path) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    const size_t n = (size_t)s->g.nx * s->g.ny * NFIELD;
+    std::vector<double> h(n);
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(s, RMHD2D_ERR_IO, std::string("cannot open ") + path);
+    const size_t r = std::fread(h.data(), sizeof(double), n, f);
+    const int extra = std::fgetc(f);
+    std::fclose(f);
+    if (r != n || extra != EOF) return fail(s, RMHD2D_ERR_IO, std::string("size mismatch reading ") + path);
+    int rc = rmhd2d_set_state(s, h.data(), 0);
+    if (rc) return rc;
+    return sync_and_check(s);
+}
+
+}  // extern "C"

@@ -1,0 +1,280 @@
+// aux_kernels.cu -- boundary fill, CFL reduction and layout conversion for
+// librmhd2d.  Compiled with -fmad=false: the symmetric boundary's div-B
+// integration and the CFL rate must round exactly as the reference does.
+#include <cuda_runtime.h>
+
+#include "aux_kernels.h"
+#include "physics.cuh"
+
+namespace rmhd2d {
+
+namespace {
+
+__device__ __forceinline__ long long at(const Grid &g, int i, int j) { return (long long)i * g.pitch + j; }
+
+// Mirror index of the symmetric boundary (TS boundary.cu:9-52): ghost 0,1,2
+// take cells 5,4,3 and ghost n-1,n-2,n-3 take n-6,n-5,n-4.
+__device__ __forceinline__ int mirror(int c, int n)
+{
+    if (c < 3) return 5 - c;
+    if (c >= n - 3) return 2 * n - 7 - c;
+    return c;
+}
+
+// Periodic wrap (boundary.cu:9-57, period n-6).
+__device__ __forceinline__ int wrap(int c, int n)
+{
+    if (c < 3) return c + n - 6;
+    if (c >= n - 3) return c - (n - 6);
+    return c;
+}
+
+// bY seen by the x-wall integration at interior column c and row r: the
+// lower-wall face row (r = 2) holds the stage's constrained-transport value
+// (row2), which the symmetric y pass replaces only afterwards.
+__device__ __forceinline__ double bY_prewall(const Grid &g, const double *bY, const double *row2, int c, int r)
+{
+    return r == 2 ? row2[c] : bY[at(g, c, r)];
+}
+
+// x-wall ghost bX at ghost column c, interior row r
+// (TS boundary.cu:56-88 symmetricBoundaryX2ndBX_kernel, 0 < j branch).
+__device__ double bX_xghost(const Grid &g, const double *bX, const double *bY, const double *row2, int c, int r)
+{
+    const double dx = g.dx, dy = g.dy;
+    const int nx = g.nx;
+    if (c < 3) {
+        const double d3 = (bY_prewall(g, bY, row2, 3, r) - bY_prewall(g, bY, row2, 3, r - 1)) / dy * dx;
+        double b = bX[at(g, 3, r)] + d3;          // column 2
+        if (c == 2) return b;
+        b = b + (bY_prewall(g, bY, row2, 3, r) - bY_prewall(g, bY, row2, 3, r - 1)) / dy * dx;  // column 1 (bY copied from 3)
+        if (c == 1) return b;
+        return b + (bY_prewall(g, bY, row2, 4, r) - bY_prewall(g, bY, row2, 4, r - 1)) / dy * dx;  // column 0 (bY from 4)
+    }
+    double b = bX[at(g, nx - 4, r)]
+             - (bY_prewall(g, bY, row2, nx - 4, r) - bY_prewall(g, bY, row2, nx - 4, r - 1)) / dy * dx;  // nx-3
+    if (c == nx - 3) return b;
+    b = b - (bY_prewall(g, bY, row2, nx - 5, r) - bY_prewall(g, bY, row2, nx - 5, r - 1)) / dy * dx;       // nx-2
+    if (c == nx - 2) return b;
+    return b - (bY_prewall(g, bY, row2, nx - 6, r) - bY_prewall(g, bY, row2, nx - 6, r - 1)) / dy * dx;    // nx-1
+}
+
+// bX after the x pass at column c (any) and interior row r.
+__device__ __forceinline__ double bX_afterx(const Grid &g, const double *bX, const double *bY, const double *row2,
+                                            int c, int r)
+{
+    return (c >= 3 && c < g.nx - 3) ? bX[at(g, c, r)] : bX_xghost(g, bX, bY, row2, c, r);
+}
+
+// y-wall ghost bY at column i, ghost row j
+// (TS boundary.cu:159-188 symmetricBoundaryY2ndBY_kernel).
+__device__ double bY_yghost(const Grid &g, const double *bX, const double *bY, const double *row2, int i, int j)
+{
+    const double dx = g.dx, dy = g.dy;
+    const int ny = g.ny;
+    const int mi = mirror(i, g.nx);
+    if (j < 3) {
+        double b = bY[at(g, mi, 3)];
+        if (i == 0) return b;
+        const double s3 = (bX_afterx(g, bX, bY, row2, i, 3) - bX_afterx(g, bX, bY, row2, i - 1, 3)) / dx * dy;
+        b = b + s3;                                   // row 2
+        if (j == 2) return b;
+        b = b + (bX_afterx(g, bX, bY, row2, i, 3) - bX_afterx(g, bX, bY, row2, i - 1, 3)) / dx * dy;  // row 1
+        if (j == 1) return b;
+        return b + (bX_afterx(g, bX, bY, row2, i, 4) - bX_afterx(g, bX, bY, row2, i - 1, 4)) / dx * dy;  // row 0
+    }
+    double b = bY[at(g, mi, ny - 4)];
+    if (i == 0) return b;
+    b = b - (bX_afterx(g, bX, bY, row2, i, ny - 4) - bX_afterx(g, bX, bY, row2, i - 1, ny - 4)) / dx * dy;  // ny-3
+    if (j == ny - 3) return b;
+    b = b - (bX_afterx(g, bX, bY, row2, i, ny - 5) - bX_afterx(g, bX, bY, row2, i - 1, ny - 5)) / dx * dy;  // ny-2
+    if (j == ny - 2) return b;
+    return b - (bX_afterx(g, bX, bY, row2, i, ny - 6) - bX_afterx(g, bX, bY, row2, i - 1, ny - 6)) / dx * dy;  // ny-1
+}
+
+// Maps a linear ghost-cell index to (i, j): first the 6 ghost columns
+// (all rows, j contiguous), then the 6 ghost rows of the interior columns.
+__device__ __forceinline__ void ghost_cell(const Grid &g, long long t, int &i, int &j)
+{
+    const long long ncol = 6LL * g.ny;
+    if (t < ncol) {
+        const int c = (int)(t / g.ny);
+        j = (int)(t - (long long)c * g.ny);
+        i = c < 3 ? c : g.nx - 6 + c;
+    } else {
+        const long long u = t - ncol;
+        const int w = g.nx - 6;
+        const int r = (int)(u / w);
+        i = 3 + (int)(u - (long long)r * w);
+        j = r < 3 ? r : g.ny - 6 + r;
+    }
+}
+
+// Fills every ghost cell of `s` from its interior (and, for symmetric walls,
+// the CT'd lower-wall bY row), with the exact results of the reference's two
+// boundary passes (periodic: boundary.cu:4-141; symmetric: TS boundary.cu:4-206).
+// With `ctl` set it also folds the ghost cells' CFL rate and NaN-energy test
+// into the reductions of the stage-2 kernel.
+__global__ void boundary_kernel(Grid g, double *s, const double *row2, Control *ctl, int slot)
+{
+    const long long nghost = 6LL * g.ny + 6LL * (g.nx - 6);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long bits = 0ull;
+    int nan_e = 0;
+    if (t < nghost) {
+        int i, j;
+        ghost_cell(g, t, i, j);
+        const long long P = g.plane;
+        const long long k = at(g, i, j);
+        double v[8];
+        if (g.bc == BC_PERIODIC) {
+            const long long src = at(g, wrap(i, g.nx), wrap(j, g.ny));
+#pragma unroll
+            for (int f = 0; f < 8; ++f) v[f] = s[f * P + src];
+        } else {
+            const int mi = mirror(i, g.nx), mj = mirror(j, g.ny);
+            const long long src = at(g, mi, mj);
+            const int hydro[6] = {RHO, MX, MY, MZ, BZF, EN};
+#pragma unroll
+            for (int n = 0; n < 6; ++n) v[hydro[n]] = s[hydro[n] * P + src];
+            const double *bX = s + BXF * P, *bY = s + BYF * P;
+            v[BXF] = bX_afterx(g, bX, bY, row2, i, mj);
+            v[BYF] = (j >= 3 && j < g.ny - 3) ? bY[at(g, mi, j)] : bY_yghost(g, bX, bY, row2, i, j);
+        }
+        // all reads of this thread precede its writes; a ghost cell is never
+        // read by the boundary fill, so the in-place update is race free.
+#pragma unroll
+        for (int f = 0; f < 8; ++f) s[f * P + k] = v[f];
+        if (ctl) {
+            bits = rate_bits(cfl_rate(v[RHO], v[MX], v[MY], v[MZ], v[BXF], v[BYF], v[BZF], v[EN], g.gamma, g.dx, g.dy));
+            nan_e = v[EN] != v[EN];
+        }
+    }
+    if (ctl) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
+            bits = o > bits ? o : bits;
+        }
+        const int any_nan = __any_sync(0xffffffffu, nan_e);
+        if ((threadIdx.x & 31) == 0) {
+            if (bits) atomicMax(&ctl->amax[slot], bits);
+            if (any_nan) atomicExch(&ctl->crashed, 1);
+        }
+    }
+}
+
+// Copies the lower-wall face row bY(i, 2) into row2 (used when the boundary
+// is applied to a state that did not come from a stage, e.g. after set_state).
+__global__ void snapshot_row2_kernel(Grid g, const double *s, double *row2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < g.nx) row2[i] = s[BYF * g.plane + at(g, i, 2)];
+}
+
+// CFL rate over every cell (resistiveMHD_2D.cu:247-291) and the NaN-energy
+// test (resistiveMHD_2D.cu:294-309).
+__global__ void rate_kernel(Grid g, const double *s, Control *ctl, int slot, int set_crash)
+{
+    const long long n = (long long)g.nx * g.ny;
+    unsigned long long bits = 0ull;
+    int nan_e = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
+        const long long k = at(g, i, j);
+        const long long P = g.plane;
+        const double e = s[EN * P + k];
+        const unsigned long long b = rate_bits(cfl_rate(s[RHO * P + k], s[MX * P + k], s[MY * P + k], s[MZ * P + k],
+                                                        s[BXF * P + k], s[BYF * P + k], s[BZF * P + k], e,
+                                                        g.gamma, g.dx, g.dy));
+        bits = b > bits ? b : bits;
+        nan_e |= (e != e);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
+        bits = o > bits ? o : bits;
+    }
+    const int any_nan = __any_sync(0xffffffffu, nan_e);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&ctl->amax[slot], bits);
+        if (set_crash && any_nan) atomicExch(&ctl->crashed, 1);
+    }
+}
+
+// AoS (reference layout, cell k = j + i*ny, 8 doubles) <-> SoA planes.
+__global__ void aos_to_planes_kernel(Grid g, const double *aos, double *s)
+{
+    const long long n = (long long)g.nx * g.ny;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n * 8; t += (long long)gridDim.x * blockDim.x) {
+        const long long cell = t >> 3;
+        const int f = (int)(t & 7);
+        const int i = (int)(cell / g.ny), j = (int)(cell - (long long)i * g.ny);
+        s[f * g.plane + at(g, i, j)] = aos[t];
+    }
+}
+
+__global__ void planes_to_aos_kernel(Grid g, const double *s, double *aos)
+{
+    const long long n = (long long)g.nx * g.ny;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n * 8; t += (long long)gridDim.x * blockDim.x) {
+        const long long cell = t >> 3;
+        const int f = (int)(t & 7);
+        const int i = (int)(cell / g.ny), j = (int)(cell - (long long)i * g.ny);
+        aos[t] = s[f * g.plane + at(g, i, j)];
+    }
+}
+
+// Dense (nx, ny) table -> pitched plane.
+__global__ void table_to_plane_kernel(Grid g, const double *tab, double *plane)
+{
+    const long long n = (long long)g.nx * g.ny;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
+        plane[at(g, i, j)] = tab[t];
+    }
+}
+
+int grid_for(long long n, int threads)
+{
+    long long b = (n + threads - 1) / threads;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+void launch_boundary(const Grid &g, double *s, const double *row2, Control *ctl, int slot, cudaStream_t st)
+{
+    const long long nghost = 6LL * g.ny + 6LL * (g.nx - 6);
+    const int threads = 256;
+    const int blocks = (int)((nghost + threads - 1) / threads);
+    boundary_kernel<<<blocks, threads, 0, st>>>(g, s, row2, ctl, slot);
+}
+
+void launch_snapshot_row2(const Grid &g, const double *s, double *row2, cudaStream_t st)
+{
+    snapshot_row2_kernel<<<(g.nx + 255) / 256, 256, 0, st>>>(g, s, row2);
+}
+
+void launch_rate(const Grid &g, const double *s, Control *ctl, int slot, int set_crash, cudaStream_t st)
+{
+    rate_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, st>>>(g, s, ctl, slot, set_crash);
+}
+
+void launch_aos_to_planes(const Grid &g, const double *aos, double *s, cudaStream_t st)
+{
+    aos_to_planes_kernel<<<grid_for((long long)g.nx * g.ny * 8, 256), 256, 0, st>>>(g, aos, s);
+}
+
+void launch_planes_to_aos(const Grid &g, const double *s, double *aos, cudaStream_t st)
+{
+    planes_to_aos_kernel<<<grid_for((long long)g.nx * g.ny * 8, 256), 256, 0, st>>>(g, s, aos);
+}
+
+void launch_table_to_plane(const Grid &g, const double *tab, double *plane, cudaStream_t st)
+{
+    table_to_plane_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, st>>>(g, tab, plane);
+}
+
+}  // namespace rmhd2d

@@ -1,0 +1,207 @@
+// physics.cuh -- per-cell and per-interface arithmetic of the 2D resistive-MHD
+// step, written for the fused sm_100a stage kernel.  Every expression keeps
+// the operation order of the reference's functors so that, compiled without
+// FMA contraction (-fmad=false), results are bit-identical to the reference
+// evaluated in IEEE binary64 (reference files under
+// ResistiveMHD_singleGPU_thrust/lib_ResistiveMHD_2D_GPU_periodicXY/).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace rmhd2d {
+
+// thrust::min / thrust::max semantics ((b < a) ? b : a).
+__device__ __forceinline__ double tmin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double tmax(double a, double b) { return (a < b) ? b : a; }
+
+// hlld.cu:26-32 Sign.
+__device__ __forceinline__ double sgn(double x) { return (double)((x > 0.0) - (x < 0.0)); }
+
+// minmod.hpp:6-16: sign_x * max(min(|x|, sign_x * y), EPS) with an int sign.
+__device__ __forceinline__ double minmod(double x, double y, double eps)
+{
+    const int s = (x > 0.0) - (x < 0.0);
+    const double ds = (double)s;
+    return ds * tmax(tmin(fabs(x), ds * y), eps);
+}
+
+// Interface state fed to HLLD: BasicParameter (basic_parameter_struct.hpp:5-27).
+struct Prim {
+    double rho, u, v, w, bX, bY, bZ, p;
+};
+
+// hlld.cu:448-467 getOneFlux, accumulated into f (f4 is identically 0 and
+// is not produced).
+__device__ __forceinline__ void add_one_flux(double rho, double u, double v, double w, double bX,
+                                             double bY, double bZ, double e, double pT, double f[8])
+{
+    f[0] += rho * u;
+    f[1] += rho * u * u + pT - bX * bX;
+    f[2] += rho * u * v - bX * bY;
+    f[3] += rho * u * w - bX * bZ;
+    f[5] += u * bY - v * bX;
+    f[6] += u * bZ - w * bX;
+    f[7] += (e + pT) * u - bX * (bX * u + bY * v + bZ * w);
+}
+
+// Weighted candidate: f += F(state) * ind (all six candidates are formed,
+// so non-finite values propagate exactly as in the reference's
+// CalculateFluxFunctor, hlld.cu:35-107).
+__device__ __forceinline__ void add_weighted_flux(double rho, double u, double v, double w, double bX,
+                                                  double bY, double bZ, double e, double pT,
+                                                  double ind, double f[8])
+{
+    f[0] += (rho * u) * ind;
+    f[1] += (rho * u * u + pT - bX * bX) * ind;
+    f[2] += (rho * u * v - bX * bY) * ind;
+    f[3] += (rho * u * w - bX * bZ) * ind;
+    f[4] += 0.0 * ind;
+    f[5] += (u * bY - v * bX) * ind;
+    f[6] += (u * bZ - w * bX) * ind;
+    f[7] += ((e + pT) * u - bX * (bX * u + bY * v + bZ * w)) * ind;
+}
+
+// HLLD flux through one interface: hlld.cu:256-432
+// (calculateHLLDParameterFunctor), hlld.cu:469-549 (setFluxFunctor) and
+// hlld.cu:35-107 (CalculateFluxFunctor).
+//
+// ALL_CANDIDATES = true forms all six candidate fluxes and sums them with the
+// reference's 0/1 indicator weights (bit-identical to the reference for every
+// input, including non-finite ones).  ALL_CANDIDATES = false forms only the
+// candidates whose indicator is 1 and adds them in the reference's order,
+// which gives the same bits whenever all six candidates are finite.
+template <bool ALL_CANDIDATES>
+__device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double gm, double EPS,
+                                          double f[8])
+{
+    const double rhoL = L.rho, uL = L.u, vL = L.v, wL = L.w, bXL = L.bX, bYL = L.bY, bZL = L.bZ, pL = L.p;
+    const double rhoR = R.rho, uR = R.u, vR = R.v, wR = R.w, bXR = R.bX, bYR = R.bY, bZR = R.bZ, pR = R.p;
+
+    const double eL = pL / (gm - 1.0)
+                    + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL)
+                    + 0.5 * (bXL * bXL + bYL * bYL + bZL * bZL);
+    const double pTL = pL + 0.5 * (bXL * bXL + bYL * bYL + bZL * bZL);
+    const double eR = pR / (gm - 1.0)
+                    + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR)
+                    + 0.5 * (bXR * bXR + bYR * bYR + bZR * bZR);
+    const double pTR = pR + 0.5 * (bXR * bXR + bYR * bYR + bZR * bZR);
+
+    const double csL = sqrt(gm * pL / rhoL);
+    const double caL = sqrt((bXL * bXL + bYL * bYL + bZL * bZL) / rhoL);
+    const double vaL = sqrt(bXL * bXL / rhoL);
+    const double cfL = sqrt(0.5 * (csL * csL + caL * caL
+                     + sqrt((csL * csL + caL * caL) * (csL * csL + caL * caL)
+                     - 4.0 * csL * csL * vaL * vaL)));
+    const double csR = sqrt(gm * pR / rhoR);
+    const double caR = sqrt((bXR * bXR + bYR * bYR + bZR * bZR) / rhoR);
+    const double vaR = sqrt(bXR * bXR / rhoR);
+    const double cfR = sqrt(0.5 * (csR * csR + caR * caR
+                     + sqrt((csR * csR + caR * caR) * (csR * csR + caR * caR)
+                     - 4.0 * csR * csR * vaR * vaR)));
+
+    double SL = tmin(uL, uR) - tmax(cfL, cfR);
+    double SR = tmax(uL, uR) + tmax(cfL, cfR);
+    SL = tmin(SL, 0.0);
+    SR = tmax(SR, 0.0);
+
+    const double SM = ((SR - uR) * rhoR * uR - (SL - uL) * rhoL * uL - pTR + pTL)
+                    / ((SR - uR) * rhoR - (SL - uL) * rhoL + EPS);
+    const double pT1 = ((SR - uR) * rhoR * pTL - (SL - uL) * rhoL * pTR
+                     + rhoL * rhoR * (SR - uR) * (SL - uL) * (uR - uL))
+                     / ((SR - uR) * rhoR - (SL - uL) * rhoL + EPS);
+
+    const double rho1L = rhoL * (SL - uL) / (SL - SM + EPS);
+    const double u1L = SM;
+    const double v1L = vL - bXL * bYL * (SM - uL) / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    const double w1L = wL - bXL * bZL * (SM - uL) / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    const double bX1L = bXL;
+    const double bY1L = bYL * (rhoL * (SL - uL) * (SL - uL) - bXL * bXL)
+                      / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    const double bZ1L = bZL * (rhoL * (SL - uL) * (SL - uL) - bXL * bXL)
+                      / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    const double e1L = ((SL - uL) * eL - pTL * uL + pT1 * SM
+                     + bXL * ((uL * bXL + vL * bYL + wL * bZL) - (u1L * bX1L + v1L * bY1L + w1L * bZ1L)))
+                     / (SL - SM + EPS);
+
+    const double rho1R = rhoR * (SR - uR) / (SR - SM + EPS);
+    const double u1R = SM;
+    const double v1R = vR - bXR * bYR * (SM - uR) / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    const double w1R = wR - bXR * bZR * (SM - uR) / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    const double bX1R = bXR;
+    const double bY1R = bYR * (rhoR * (SR - uR) * (SR - uR) - bXR * bXR)
+                      / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    const double bZ1R = bZR * (rhoR * (SR - uR) * (SR - uR) - bXR * bXR)
+                      / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    const double e1R = ((SR - uR) * eR - pTR * uR + pT1 * SM
+                     + bXR * ((uR * bXR + vR * bYR + wR * bZR) - (u1R * bX1R + v1R * bY1R + w1R * bZ1R)))
+                     / (SR - SM + EPS);
+
+    const double S1L = SM - sqrt(bX1L * bX1L / rho1L);
+    const double S1R = SM + sqrt(bX1R * bX1R / rho1R);
+
+    const double sqL = sqrt(rho1L), sqR = sqrt(rho1R), sqLR = sqrt(rho1L * rho1R);
+    const double sbX = sgn(bX1L);
+    const double u2 = SM;
+    const double v2 = (sqL * v1L + sqR * v1R + (bY1R - bY1L) * sbX) / (sqL + sqR + EPS);
+    const double w2 = (sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sbX) / (sqL + sqR + EPS);
+    const double bY2 = (sqL * bY1R + sqR * bY1L + sqLR * (v1R - v1L) * sbX) / (sqL + sqR + EPS);
+    const double bZ2 = (sqL * bZ1R + sqR * bZ1L + sqLR * (w1R - w1L) * sbX) / (sqL + sqR + EPS);
+    const double e2L = e1L - sqL * ((u1L * bX1L + v1L * bY1L + w1L * bZ1L) - (u2 * bXL + v2 * bY2 + w2 * bZ2))
+                     * sgn(bXL);
+    const double e2R = e1R + sqR * ((u1R * bX1R + v1R * bY1R + w1R * bZ1R) - (u2 * bXR + v2 * bY2 + w2 * bZ2))
+                     * sgn(bXR);
+
+    const bool bOL = SL > 0.0;
+    const bool bML = (SL <= 0.0) && (0.0 < S1L);
+    const bool bIL = (S1L <= 0.0) && (0.0 < SM);
+    const bool bOR = SR <= 0.0;
+    const bool bMR = (S1R <= 0.0) && (0.0 < SR);
+    const bool bIR = (SM <= 0.0) && (0.0 < S1R);
+
+#pragma unroll
+    for (int n = 0; n < 8; ++n) f[n] = 0.0;
+    if (ALL_CANDIDATES) {
+        // rho2L = rho1L, rho2R = rho1R, pT2 = pT1 (hlld.cu:360-378).
+        add_weighted_flux(rhoL, uL, vL, wL, bXL, bYL, bZL, eL, pTL, (double)bOL, f);
+        add_weighted_flux(rho1L, u1L, v1L, w1L, bXL, bY1L, bZ1L, e1L, pT1, (double)bML, f);
+        add_weighted_flux(rho1L, u2, v2, w2, bXL, bY2, bZ2, e2L, pT1, (double)bIL, f);
+        add_weighted_flux(rhoR, uR, vR, wR, bXR, bYR, bZR, eR, pTR, (double)bOR, f);
+        add_weighted_flux(rho1R, u1R, v1R, w1R, bXR, bY1R, bZ1R, e1R, pT1, (double)bMR, f);
+        add_weighted_flux(rho1R, u2, v2, w2, bXR, bY2, bZ2, e2R, pT1, (double)bIR, f);
+    } else {
+        if (bOL) add_one_flux(rhoL, uL, vL, wL, bXL, bYL, bZL, eL, pTL, f);
+        if (bML) add_one_flux(rho1L, u1L, v1L, w1L, bXL, bY1L, bZ1L, e1L, pT1, f);
+        if (bIL) add_one_flux(rho1L, u2, v2, w2, bXL, bY2, bZ2, e2L, pT1, f);
+        if (bOR) add_one_flux(rhoR, uR, vR, wR, bXR, bYR, bZR, eR, pTR, f);
+        if (bMR) add_one_flux(rho1R, u1R, v1R, w1R, bXR, bY1R, bZ1R, e1R, pT1, f);
+        if (bIR) add_one_flux(rho1R, u2, v2, w2, bXR, bY2, bZ2, e2R, pT1, f);
+    }
+}
+
+// resistiveMHD_2D.cu:247-274 calculateDtFunctor, returning the denominator
+// term a = maxSpeedX/dx + maxSpeedY/dy; the cell's dt candidate is
+// 1/(a + EPS), so the minimum over cells is 1/(max a + EPS).
+__device__ __forceinline__ double cfl_rate(double rho, double mx, double my, double mz, double bX,
+                                           double bY, double bZ, double e, double gm, double dx,
+                                           double dy)
+{
+    const double u = mx / rho, v = my / rho, w = mz / rho;
+    const double p = (gm - 1.0)
+                   * (e - 0.5 * rho * (u * u + v * v + w * w)
+                   - 0.5 * (bX * bX + bY * bY + bZ * bZ));
+    const double cs = sqrt(gm * p / rho);
+    const double ca = sqrt((bX * bX + bY * bY + bZ * bZ) / rho);
+    const double sx = fabs(u) + sqrt(cs * cs + ca * ca);
+    const double sy = fabs(v) + sqrt(cs * cs + ca * ca);
+    return sx / dx + sy / dy;
+}
+
+// Order-preserving encoding of a non-negative rate for atomicMax; NaN maps
+// above every finite value so a NaN rate yields a NaN dt.
+__device__ __forceinline__ unsigned long long rate_bits(double a)
+{
+    if (a != a) return 0x7FF8000000000000ull;
+    return (unsigned long long)__double_as_longlong(a);
+}
+
+}  // namespace rmhd2d

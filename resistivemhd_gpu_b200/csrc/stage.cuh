@@ -1,0 +1,55 @@
+// stage.cuh -- the fused RK2 stage kernel for sm_100a.
+//
+// One launch performs one stage of the reference's ResistiveMHD2D::oneStepRK2
+// (lib_ResistiveMHD_2D_GPU_periodicXY/resistiveMHD_2D.cu:133-195) on the
+// interior cells: face -> centre B, primitive recovery, MUSCL-minmod, HLLD
+// fluxes in x and y, the resistive eta*J flux terms, the flux-difference
+// update, and (stage 1) the corner EMF plus constrained transport of the
+// face B.  The stage-2 launch also reduces the CFL rate of the new state for
+// the next step's dt and raises the crash flag on a NaN energy.
+//
+// Data layout: 8 field planes of nx x pitch doubles (index i*pitch + j,
+// y contiguous), one allocation per state.  Each CTA owns TI x TJ interior
+// cells and stages them with a 3-cell halo on every side by one 3-D TMA load
+// (box TJ+6 x TI+6 x 8 fields) into shared memory; everything after that
+// load reads shared memory only.
+//
+// This header is compiled twice: into an "exact" variant (-fmad=false, all
+// six HLLD candidate fluxes formed), bit-identical to the reference
+// evaluated in IEEE binary64, and a "fast" variant (FMA contraction, only
+// the selected HLLD candidates).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "physics.cuh"
+#include "rmhd2d_internal.h"
+
+namespace rmhd2d {
+
+struct StageArgs {
+    Grid g;
+    const double *src;   // state this stage reads (TMA source); stage 2: U*
+    const double *un;    // stage 2: U^n (hydro fields read at own cells)
+    double *dst;         // planes written (stage 1: U*; stage 2: U^n in place)
+    const double *eta;   // cell-centred eta plane or nullptr (uniform g.eta)
+    double *row2;        // symmetric boundaries: CT'd bY at j = 2, indexed by i
+    Control *ctl;
+    int parity;          // step parity: dt from ctl->amax[parity]
+};
+
+// One launcher per variant (stage_exact.cu, stage_fast.cu).
+namespace exact {
+void launch_stage(int stage, const CUtensorMap *tmap, const StageArgs &args, cudaStream_t stream);
+size_t stage_smem_bytes();
+int stage_regs(int stage);
+}  // namespace exact
+namespace fast {
+void launch_stage(int stage, const CUtensorMap *tmap, const StageArgs &args, cudaStream_t stream);
+size_t stage_smem_bytes();
+int stage_regs(int stage);
+}  // namespace fast
+
+}  // namespace rmhd2d

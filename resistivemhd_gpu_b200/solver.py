@@ -1,0 +1,225 @@
+"""Python host interface of the B200 resistive-MHD step.
+
+``Solver`` wraps one ``rmhd2d_solver`` of the C ABI.  ``ResistiveMHD2D``
+mirrors the reference's class of the same name
+(ResistiveMHD_singleGPU_thrust/lib_ResistiveMHD_2D_GPU_periodicXY/
+resistiveMHD_2D.hpp:9-52): ``initializeU`` (overridden by the user, as the
+reference's drivers do), ``oneStepRK2``, ``calculateDt``, ``save``, ``getU``
+and ``checkCalculationIsCrashed``, plus the reference's globals ``dt`` and
+``totalTime`` as attributes.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+def _as_f64(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Solver:
+    """One solver instance on one CUDA device.
+
+    ``nx``, ``ny`` include 3 ghost layers per side.  ``bc`` is "periodic" or
+    "symmetric" (both directions).  ``precision`` is "fp64_exact" (bit-for-bit
+    the reference's IEEE binary64 arithmetic) or "fp64_fast" (FMA contraction).
+    ``stream`` may be a CUDA stream handle (int) to enqueue on."""
+
+    def __init__(self, nx: int, ny: int, dx: float, dy: float, *, gamma: float = 5.0 / 3.0, cfl: float = 0.4,
+                 eps: float = 1e-20, eta: float = 0.0, bc: str = "periodic", precision: str = "fp64_exact",
+                 device: int = 0, stream: int | None = None):
+        lib = _lib.load()
+        cfg = _lib.Config()
+        lib.rmhd2d_config_default(ctypes.byref(cfg))
+        cfg.nx, cfg.ny, cfg.dx, cfg.dy = int(nx), int(ny), float(dx), float(dy)
+        cfg.gamma_mhd, cfg.cfl, cfg.eps, cfg.eta = float(gamma), float(cfl), float(eps), float(eta)
+        if bc not in _lib.BC:
+            raise ValueError(f"unknown boundary kind {bc!r}")
+        if precision not in _lib.PRECISION:
+            raise ValueError(f"unknown precision {precision!r}")
+        cfg.bc = _lib.BC[bc]
+        cfg.precision = _lib.PRECISION[precision]
+        cfg.device = int(device)
+        cfg.stream = stream
+        h = ctypes.c_void_p()
+        _lib.check(lib.rmhd2d_create(ctypes.byref(cfg), ctypes.byref(h)), None)
+        self._lib = lib
+        self._h = h
+        self.nx, self.ny = int(nx), int(ny)
+        self.bc, self.precision = bc, precision
+
+    @classmethod
+    def from_setup(cls, setup, precision: str = "fp64_exact", device: int = 0, apply_boundary: bool = True,
+                   stream: int | None = None) -> "Solver":
+        s = cls(setup.nx, setup.ny, setup.dx, setup.dy, gamma=setup.gamma, cfl=setup.cfl, eps=setup.eps,
+                eta=setup.eta, bc=setup.bc, precision=precision, device=device, stream=stream)
+        if setup.eta_table is not None:
+            s.set_eta_table(setup.eta_table)
+        s.set_state(setup.state, apply_boundary=apply_boundary)
+        return s
+
+    # -- lifetime --
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.rmhd2d_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _ck(self, st: int) -> None:
+        _lib.check(st, self._h)
+
+    # -- state --
+    def set_state(self, state: np.ndarray, apply_boundary: bool = True) -> None:
+        a = _as_f64(state)
+        if a.size != self.nx * self.ny * 8:
+            raise ValueError(f"state must hold {self.nx}x{self.ny}x8 doubles, got shape {a.shape}")
+        self._ck(self._lib.rmhd2d_set_state(self._h, a.ctypes.data_as(_DP), int(bool(apply_boundary))))
+
+    def set_state_device(self, device_ptr: int, apply_boundary: bool = True) -> None:
+        self._ck(self._lib.rmhd2d_set_state_device(self._h, ctypes.c_void_p(device_ptr), int(bool(apply_boundary))))
+
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.nx, self.ny, 8), dtype=np.float64)
+        if not (out.flags.c_contiguous and out.dtype == np.float64 and out.size == self.nx * self.ny * 8):
+            raise ValueError("out must be a C-contiguous float64 array of nx*ny*8 elements")
+        self._ck(self._lib.rmhd2d_get_state(self._h, out.ctypes.data_as(_DP)))
+        return out
+
+    def set_eta_table(self, eta: np.ndarray | None) -> None:
+        if eta is None:
+            self._ck(self._lib.rmhd2d_set_eta_table(self._h, None))
+            return
+        a = _as_f64(eta)
+        if a.size != self.nx * self.ny:
+            raise ValueError("eta table must hold nx*ny doubles")
+        self._ck(self._lib.rmhd2d_set_eta_table(self._h, a.ctypes.data_as(_DP)))
+
+    def apply_boundary(self) -> None:
+        self._ck(self._lib.rmhd2d_apply_boundary(self._h))
+
+    # -- stepping --
+    def calculate_dt(self) -> float:
+        d = ctypes.c_double()
+        self._ck(self._lib.rmhd2d_calculate_dt(self._h, ctypes.byref(d)))
+        return d.value
+
+    def step(self) -> None:
+        self._ck(self._lib.rmhd2d_step_rk2(self._h))
+
+    def run(self, nsteps: int) -> None:
+        self._ck(self._lib.rmhd2d_run(self._h, int(nsteps)))
+
+    @property
+    def dt(self) -> float:
+        d = ctypes.c_double()
+        self._ck(self._lib.rmhd2d_get_dt(self._h, ctypes.byref(d)))
+        return d.value
+
+    @property
+    def total_time(self) -> float:
+        d = ctypes.c_double()
+        self._ck(self._lib.rmhd2d_get_total_time(self._h, ctypes.byref(d)))
+        return d.value
+
+    def check_crashed(self) -> bool:
+        c = ctypes.c_int()
+        self._ck(self._lib.rmhd2d_check_crashed(self._h, ctypes.byref(c)))
+        return bool(c.value)
+
+    # -- snapshots --
+    def save(self, directory: str, name_without_step: str, step: int) -> str:
+        self._ck(self._lib.rmhd2d_save(self._h, os.fsencode(directory), os.fsencode(name_without_step), int(step)))
+        return os.path.join(directory, f"{name_without_step}_{step}.bin")
+
+    def load(self, path: str) -> None:
+        self._ck(self._lib.rmhd2d_load(self._h, os.fsencode(path)))
+
+
+def write_snapshot(path: str, state: np.ndarray) -> None:
+    """Write a host state in the reference save() format (no GPU needed)."""
+    lib = _lib.load()
+    a = _as_f64(state)
+    if a.ndim != 3 or a.shape[2] != 8:
+        raise ValueError("state must have shape (nx, ny, 8)")
+    _lib.check(lib.rmhd2d_write_snapshot(os.fsencode(path), a.ctypes.data_as(_DP), a.shape[0], a.shape[1]), None)
+
+
+def read_snapshot(path: str, nx: int, ny: int) -> np.ndarray:
+    """Read a save() file (the reference's or this library's)."""
+    a = np.fromfile(path, dtype="<f8")
+    if a.size != nx * ny * 8:
+        raise ValueError(f"{path}: expected {nx * ny * 8} doubles, found {a.size}")
+    return a.reshape(nx, ny, 8)
+
+
+class ResistiveMHD2D:
+    """Drop-in mirror of the reference's ``ResistiveMHD2D`` class.
+
+    Subclass and override ``initializeU`` to fill ``self.U`` (an (nx, ny, 8)
+    array, ghosts included) exactly as the reference's drivers implement
+    ``ResistiveMHD2D::initializeU`` -- the boundary is applied afterwards,
+    as those drivers do.  ``dt`` and ``totalTime`` mirror the reference's
+    globals (const.hpp:20-23)."""
+
+    def __init__(self, nx: int, ny: int, dx: float, dy: float, *, gamma_mhd: float = 5.0 / 3.0, CFL: float = 0.4,
+                 EPS: float = 1e-20, eta: float = 0.0, boundary: str = "periodic", eta_table=None,
+                 precision: str = "fp64_exact", device: int = 0):
+        self._s = Solver(nx, ny, dx, dy, gamma=gamma_mhd, cfl=CFL, eps=EPS, eta=eta, bc=boundary,
+                         precision=precision, device=device)
+        if eta_table is not None:
+            self._s.set_eta_table(eta_table)
+        self.nx, self.ny = nx, ny
+        self.U = np.zeros((nx, ny, 8), dtype=np.float64)
+        self.dt = 0.0
+        self.totalTime = 0.0
+
+    @property
+    def solver(self) -> Solver:
+        return self._s
+
+    def initializeU(self) -> None:
+        """Override: fill self.U.  The default uploads self.U as it is."""
+
+    def _upload(self) -> None:
+        self._s.set_state(self.U, apply_boundary=True)
+
+    def initialize(self) -> None:
+        self.initializeU()
+        self._upload()
+
+    def oneStepRK2(self) -> None:
+        self._s.step()
+        self.dt = self._s.dt
+        self.totalTime = self._s.total_time
+
+    def calculateDt(self) -> float:
+        self.dt = self._s.calculate_dt()
+        return self.dt
+
+    def checkCalculationIsCrashed(self) -> bool:
+        return self._s.check_crashed()
+
+    def getU(self) -> np.ndarray:
+        return self._s.get_state()
+
+    def save(self, directoryname: str, filenameWithoutStep: str, step: int) -> str:
+        return self._s.save(directoryname, filenameWithoutStep, step)

@@ -1,0 +1,56 @@
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100) GPU and librmhd2d.so")
+
+
+def load_golden(name: str):
+    """Returns (setup, initial_state, final_state, dts, total_time) of a fixture."""
+    from resistivemhd_gpu_b200.setups import Setup
+
+    z = np.load(GOLDEN / f"{name}.npz")
+    dx, dy, gamma, cfl, eps, eta = (float(v) for v in z["params"])
+    tab = z["eta_table"]
+    s = Setup(name, z["initial"].copy(), dx, dy, gamma, cfl, eps, eta,
+              tab.copy() if tab.size else None, str(z["bc"]))
+    return s, z["initial"], z["final"], z["dts"], float(z["total_time"])
+
+
+GOLDEN_CASES = sorted(p.stem for p in GOLDEN.glob("*.npz"))
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle.oracle import OracleLib
+
+    return OracleLib()
+
+
+@pytest.fixture(scope="session")
+def gpu():
+    """Skips nothing: a GPU test run without a usable B200 is a failure."""
+    import ctypes
+
+    from resistivemhd_gpu_b200 import _lib
+
+    lib = _lib.load()
+    cudart_ok = True
+    try:
+        import torch
+
+        cudart_ok = torch.cuda.is_available()
+    except Exception:
+        pass
+    assert cudart_ok, "GPU tests need a CUDA device"
+    return lib

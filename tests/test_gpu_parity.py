@@ -1,0 +1,212 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the
+reference's golden outputs.
+
+* FP64 exact variant: bit-identical to the oracle / reference (np.array_equal).
+* FP64 fast variant (FMA contraction): relative L1 error per variable
+  <= 1e-12 after the stated number of steps, the bar the step must meet
+  against the reference.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, load_golden
+
+pytestmark = pytest.mark.gpu
+
+FAST_REL_L1 = 1e-12
+
+
+def run_cuda(setup, nsteps, precision="fp64_exact", initial=None, use_run=False):
+    from resistivemhd_gpu_b200 import Solver
+
+    with Solver.from_setup(setup, precision=precision, apply_boundary=False) as s:
+        s.set_state(setup.state if initial is None else initial, apply_boundary=True)
+        dts = []
+        if use_run:
+            s.run(nsteps)
+            dts = None
+        else:
+            for _ in range(nsteps):
+                s.step()
+                dts.append(s.dt)
+        out = s.get_state()
+        total = s.total_time
+        crashed = s.check_crashed()
+    return out, (np.array(dts) if dts is not None else None), total, crashed
+
+
+def rel_l1(a, b):
+    num = np.abs(a - b).sum(axis=(0, 1))
+    den = np.abs(b).sum(axis=(0, 1))
+    return num / np.where(den > 0, den, 1.0)
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_exact_matches_reference_golden(gpu, name):
+    s, init, final, dts, total = load_golden(name)
+    out, cdts, ctotal, crashed = run_cuda(s, len(dts), initial=init)
+    assert not crashed
+    assert np.array_equal(cdts, dts)
+    assert np.array_equal(out, final)
+    assert ctotal == pytest.approx(total, rel=1e-15)
+
+
+CASES = [
+    ("periodic", False, (33, 70)),   # partial tiles in both directions
+    ("periodic", True, (8, 9)),
+    ("symmetric", False, (70, 33)),
+    ("symmetric", True, (41, 95)),
+    ("periodic", False, (6, 6)),     # smallest legal grid
+    ("symmetric", False, (6, 31)),
+]
+
+
+@pytest.mark.parametrize("bc,table,shape", CASES)
+def test_exact_bitwise_vs_oracle(gpu, oracle, bc, table, shape):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(*shape, seed=5, bc=bc, with_table=table)
+    ref, rdts, _ = oracle.run(s, s.state, 7)
+    out, cdts, _, crashed = run_cuda(s, 7)
+    assert not crashed
+    assert np.array_equal(cdts, rdts)
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("bc,table,shape", CASES[:4])
+def test_fast_within_tolerance(gpu, oracle, bc, table, shape):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(*shape, seed=6, bc=bc, with_table=table)
+    ref, _, _ = oracle.run(s, s.state, 10)
+    out, _, _, crashed = run_cuda(s, 10, precision="fp64_fast")
+    assert not crashed
+    assert rel_l1(out, ref).max() <= FAST_REL_L1
+
+
+def test_run_graph_equals_step_loop(gpu):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(40, 36, seed=9, bc="symmetric", with_table=True)
+    a, _, ta, _ = run_cuda(s, 7)
+    b, _, tb, _ = run_cuda(s, 7, use_run=True)
+    assert np.array_equal(a, b)
+    assert ta == tb
+
+
+def test_calculate_dt_matches_oracle(gpu, oracle):
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    for bc in ("periodic", "symmetric"):
+        s = setups.random_smooth_state(30, 20, seed=3, bc=bc)
+        st = oracle.boundary(s, s.state)
+        with Solver.from_setup(s, apply_boundary=True) as sol:
+            assert sol.calculate_dt() == oracle.calc_dt(s, st)
+
+
+def test_orszag_tang_256_100_steps(gpu, oracle):
+    """The reference's CPU-runnable config: OT 256^2, 100 steps."""
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.orszag_tang(256)
+    ref, rdts, _ = oracle.run(s, s.state, 100)
+    out, cdts, _, _ = run_cuda(s, 100)
+    assert np.array_equal(cdts, rdts)
+    assert np.array_equal(out, ref)
+    fast, _, _, _ = run_cuda(s, 100, precision="fp64_fast")
+    assert rel_l1(fast, ref).max() <= FAST_REL_L1
+    bx, by = out[..., 4], out[..., 5]
+    div = (bx[3:-3, 3:-3] - bx[2:-4, 3:-3]) / s.dx + (by[3:-3, 3:-3] - by[3:-3, 2:-4]) / s.dy
+    assert np.abs(div).max() < 1e-10
+
+
+def test_harris_symmetric_eta_table(gpu, oracle):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.harris_sheet(256, 128)
+    ref, rdts, _ = oracle.run(s, s.state, 20)
+    out, cdts, _, _ = run_cuda(s, 20)
+    assert np.array_equal(cdts, rdts)
+    assert np.array_equal(out, ref)
+
+
+def test_save_load_resume(gpu, tmp_path):
+    from resistivemhd_gpu_b200 import Solver, read_snapshot, setups
+
+    s = setups.random_smooth_state(30, 26, seed=4, bc="symmetric")
+    with Solver.from_setup(s) as a:
+        a.run(4)
+        path = a.save(str(tmp_path), "snap", 4)
+        snap = read_snapshot(path, s.nx, s.ny)
+        assert np.array_equal(snap, a.get_state())
+        a.run(3)
+        ref = a.get_state()
+    with Solver.from_setup(s) as b:
+        b.load(path)
+        b.run(3)
+        assert np.array_equal(b.get_state(), ref)
+
+
+def test_crash_flag_on_host_injected_nan(gpu):
+    """A NaN energy injected into the host state before upload is reported by
+    check_crashed after the next step (no GPU fault involved)."""
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.random_smooth_state(20, 20, seed=2)
+    st = s.state.copy()
+    st[10, 10, 7] = np.nan
+    with Solver.from_setup(s, apply_boundary=False) as sol:
+        sol.set_state(st, apply_boundary=True)
+        assert sol.check_crashed()
+        sol.step()
+        assert sol.check_crashed()
+    with Solver.from_setup(s) as sol:
+        sol.step()
+        assert not sol.check_crashed()
+
+
+def test_reference_class_mirror(gpu, oracle):
+    from resistivemhd_gpu_b200 import ResistiveMHD2D, setups
+
+    s = setups.orszag_tang(40)
+
+    class OT(ResistiveMHD2D):
+        def initializeU(self):
+            self.U[...] = s.state
+
+    sim = OT(s.nx, s.ny, s.dx, s.dy, gamma_mhd=s.gamma, CFL=s.cfl, EPS=s.eps, eta=s.eta)
+    sim.initialize()
+    total = 0.0
+    for _ in range(5):
+        sim.oneStepRK2()
+        assert not sim.checkCalculationIsCrashed()
+        total += sim.dt
+    ref, rdts, _ = oracle.run(s, s.state, 5)
+    assert np.array_equal(sim.getU(), ref)
+    assert sim.totalTime == total
+
+
+@pytest.mark.skipif(os.environ.get("RMHD_SKIP_LARGE") == "1", reason="large-grid property test disabled")
+def test_full_size_properties(gpu):
+    """Harris 2048x1024 (the benchmark size): no crash, div B at round-off;
+    periodic 1024^2 OT: interior sums of rho and e conserved to round-off."""
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.harris_sheet(2048, 1024)
+    with Solver.from_setup(s, precision="fp64_fast") as sol:
+        sol.run(20)
+        assert not sol.check_crashed()
+        u = sol.get_state()
+    bx, by = u[..., 4], u[..., 5]
+    div = (bx[3:-3, 3:-3] - bx[2:-4, 3:-3]) / s.dx + (by[3:-3, 3:-3] - by[3:-3, 2:-4]) / s.dy
+    assert np.abs(div).max() < 1e-9
+    o = setups.orszag_tang(1024)
+    with Solver.from_setup(o, precision="fp64_fast") as sol:
+        u0 = sol.get_state()
+        sol.run(20)
+        u1 = sol.get_state()
+    for f in (0, 7):
+        a0, a1 = u0[3:-3, 3:-3, f].sum(), u1[3:-3, 3:-3, f].sum()
+        assert abs(a1 - a0) <= 1e-11 * abs(a0)
