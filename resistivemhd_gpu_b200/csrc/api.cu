@@ -23,6 +23,7 @@
 
 #include "../../include/rmhd2d.h"
 #include "aux_kernels.h"
+#include "physics.cuh"
 #include "rmhd2d_internal.h"
 #include "stage.cuh"
 
@@ -114,6 +115,7 @@ int sync_and_check(rmhd2d_solver *s)
 int refresh_rate(rmhd2d_solver *s)
 {
     CK(cudaMemsetAsync(&s->ctl->amax[s->parity], 0, sizeof(unsigned long long), s->stream));
+    CK(cudaMemsetAsync(&s->ctl->first_nan[s->parity], 0, sizeof(int), s->stream));
     CK(cudaMemsetAsync(&s->ctl->crashed, 0, sizeof(int), s->stream));
     launch_rate(s->g, s->A, s->ctl, s->parity, 1, s->stream);
     CK(cudaGetLastError());
@@ -371,11 +373,8 @@ int rmhd2d_calculate_dt(rmhd2d_solver *s, double *dt)
     CK(cudaSetDevice(s->device));
     int rc = sync_and_check(s);
     if (rc) return rc;
-    double amax;
-    std::memcpy(&amax, &s->ctl_host->amax[s->parity], sizeof(double));
     const Grid &g = s->g;
-    const double dtMin = 1.0 / (amax + g.eps);
-    *dt = std::fmin(dtMin, std::fmin(g.dx * g.dx / g.eta, g.dy * g.dy / g.eta)) * g.cfl;
+    *dt = step_dt(s->ctl_host->amax[s->parity], s->ctl_host->first_nan[s->parity], g.dx, g.dy, g.eps, g.eta, g.cfl);
     return RMHD2D_OK;
 }
 

@@ -146,8 +146,10 @@ __global__ void boundary_kernel(Grid g, double *s, const double *row2, Control *
 #pragma unroll
         for (int f = 0; f < 8; ++f) s[f * P + k] = v[f];
         if (ctl) {
-            bits = rate_bits(cfl_rate(v[RHO], v[MX], v[MY], v[MZ], v[BXF], v[BYF], v[BZF], v[EN], g.gamma, g.dx, g.dy));
+            const double r = cfl_rate(v[RHO], v[MX], v[MY], v[MZ], v[BXF], v[BYF], v[BZF], v[EN], g.gamma, g.dx, g.dy);
+            bits = rate_bits(r);
             nan_e = v[EN] != v[EN];
+            if (i == 0 && j == 0 && r != r) ctl->first_nan[slot] = 1;
         }
     }
     if (ctl) {
@@ -184,10 +186,11 @@ __global__ void rate_kernel(Grid g, const double *s, Control *ctl, int slot, int
         const long long k = at(g, i, j);
         const long long P = g.plane;
         const double e = s[EN * P + k];
-        const unsigned long long b = rate_bits(cfl_rate(s[RHO * P + k], s[MX * P + k], s[MY * P + k], s[MZ * P + k],
-                                                        s[BXF * P + k], s[BYF * P + k], s[BZF * P + k], e,
-                                                        g.gamma, g.dx, g.dy));
+        const double r = cfl_rate(s[RHO * P + k], s[MX * P + k], s[MY * P + k], s[MZ * P + k],
+                                  s[BXF * P + k], s[BYF * P + k], s[BZF * P + k], e, g.gamma, g.dx, g.dy);
+        const unsigned long long b = rate_bits(r);
         bits = b > bits ? b : bits;
+        if (t == 0 && r != r) ctl->first_nan[slot] = 1;
         nan_e |= (e != e);
     }
 #pragma unroll

@@ -8,6 +8,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 namespace rmhd2d {
 
 // thrust::min / thrust::max semantics ((b < a) ? b : a).
@@ -196,12 +198,36 @@ __device__ __forceinline__ double cfl_rate(double rho, double mx, double my, dou
     return sx / dx + sy / dy;
 }
 
-// Order-preserving encoding of a non-negative rate for atomicMax; NaN maps
-// above every finite value so a NaN rate yields a NaN dt.
+// Order-preserving encoding of a non-negative rate for atomicMax.  A NaN
+// rate encodes as 0: the reference's thrust::min_element over the cells'
+// dt candidates 1/(a + EPS) (resistiveMHD_2D.cu:286) compares with '<', so
+// a NaN candidate never becomes the minimum -- unless it sits in cell k = 0,
+// the initial minimum, which the reductions flag separately (first_nan).
 __device__ __forceinline__ unsigned long long rate_bits(double a)
 {
-    if (a != a) return 0x7FF8000000000000ull;
+    if (a != a) return 0ull;
     return (unsigned long long)__double_as_longlong(a);
+}
+
+__host__ __device__ __forceinline__ double bits_to_double(unsigned long long b)
+{
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)b);
+#else
+    double d;
+    memcpy(&d, &b, sizeof(d));
+    return d;
+#endif
+}
+
+// dt of a step from the reduced rates (resistiveMHD_2D.cu:286-288):
+// dtMin = 1/(max a + EPS), or NaN when cell 0's candidate is NaN;
+// dt = CFL * min(dtMin, dx^2/eta, dy^2/eta) with the host min() (fmin).
+__host__ __device__ __forceinline__ double step_dt(unsigned long long amax_bits, int first_nan, double dx,
+                                                  double dy, double eps, double eta, double cfl)
+{
+    const double dtMin = first_nan ? bits_to_double(0x7FF8000000000000ull) : 1.0 / (bits_to_double(amax_bits) + eps);
+    return fmin(dtMin, fmin(dx * dx / eta, dy * dy / eta)) * cfl;
 }
 
 }  // namespace rmhd2d

@@ -25,12 +25,12 @@ struct Grid {
 
 // Device-side control block (one per solver), zero-initialised at create.
 struct Control {
-    unsigned long long amax[2];  // max over cells of |u|/dx + ... as raw bits, per step parity
+    unsigned long long amax[2];  // max over cells of |u|/dx + |v|/dy terms (raw bits, NaN skipped), per step parity
+    int first_nan[2];            // cell k = 0 had a NaN dt candidate, per step parity
     double dt;                   // dt of the most recent step (reference's global dt)
     double total_time;           // sum of dt over the steps taken
     int crashed;                 // NaN energy seen in the newest state
     int error;                   // kernel-side error code (bounded wait expired, ...)
-    int pad[2];
 };
 
 enum KernelError { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };

@@ -103,13 +103,12 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageArgs a)
 
     // dt of this step from the CFL reduction of the previous state
     // (resistiveMHD_2D.cu:277-291), identical in every thread.
-    const double amax = __longlong_as_double((long long)a.ctl->amax[a.parity]);
-    const double dtMin = 1.0 / (amax + g.eps);
-    const double dt = fmin(dtMin, fmin(g.dx * g.dx / g.eta, g.dy * g.dy / g.eta)) * g.cfl;
+    const double dt = step_dt(a.ctl->amax[a.parity], a.ctl->first_nan[a.parity], g.dx, g.dy, g.eps, g.eta, g.cfl);
     if (STAGE == 1 && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
         a.ctl->dt = dt;
         a.ctl->total_time = a.ctl->total_time + dt;
         a.ctl->amax[a.parity ^ 1] = 0ull;
+        a.ctl->first_nan[a.parity ^ 1] = 0;
         a.ctl->crashed = 0;
     }
 
