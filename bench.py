@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 resistive-MHD RK2 step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64_fast|fp64_exact] [--workload harris|orszag_tang]
+
+Workload (default): the Harris current sheet, 2048 x 1024 interior cells,
+symmetric walls, uniform eta 1e-3 plus a Gaussian eta bump (cell-centred
+table), FP64 -- the configuration the headline metric is quoted on.  A
+"step" is one full RK2 step (two fused stage kernels, two boundary fills,
+the CFL reduction for the next dt).  The state (2 x 135 MB) is larger than
+the 126 MB L2, so no L2 flush is needed between steps.
+
+Metric: interior cell-updates per second (higher is better).
+
+--impl reference times the reference's own step (the unmodified library of
+keita-akutagawa/ResistiveMHD_GPU built for the host with Thrust's OpenMP
+backend by oracle/build_ref.py) on all host cores, on the same workload.
+
+For --gpus N > 1 (launched with torch.distributed.run) each rank runs an
+independent replica of the workload on its own GPU ("replicas only": the
+single-domain step has no exchange), value = all ranks' cell-updates / the
+slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s"
+MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+B200_FP64_TFLOPS_NOMINAL = 37.0
+
+
+def workload(name: str):
+    from resistivemhd_gpu_b200 import setups
+
+    if name == "harris":
+        return setups.harris_sheet(2048, 1024), "harris_2048x1024_fp64"
+    if name == "orszag_tang":
+        return setups.orszag_tang(256), "orszag_tang_256x256_fp64"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def algorithmic_bytes(setup) -> dict:
+    """Minimum HBM bytes per launch of each stage kernel.
+    stage 1 reads U^n (8 doubles/cell) [+ eta], writes U* (8);
+    stage 2 reads U* (8) and the hydro part of U^n (6) [+ eta], writes U^{n+1} (8)."""
+    cells = setup.interior_cells
+    eta = 8 if setup.eta_table is not None else 0
+    return {"stage1": cells * (64 + 64 + eta), "stage2": cells * (64 + 48 + 64 + eta), "per_cell_update":
+            (64 + 64 + eta) + (64 + 48 + 64 + eta)}
+
+
+def hbm_peak():
+    try:
+        d = json.loads(MEASURED_PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_from_profile(label: str):
+    """dram bytes per launch of the stage kernels from the committed ncu
+    summary (profiles/stage_kernel_<label>.md, line 'traffic_bytes_per_launch:')."""
+    p = ROOT / "profiles" / f"stage_kernel_{label}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            vals = dict(kv.split("=") for kv in line.split(":", 1)[1].split())
+            return {k: float(v) for k, v in vals.items()}
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile(prefix="clk", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        try:
+            rows = [r.split(",") for r in Path(self.tmp.name).read_text().strip().splitlines() if r.strip()]
+            os.unlink(self.tmp.name)
+        except Exception:
+            rows = []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], None, set()
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                continue
+        loaded = [v for v in sm if mx and v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_reference_binary(kind: str, setup, warmup: int, steps: int, threads: int | None):
+    from oracle.oracle import run_reference
+
+    _, _, info = run_reference(setup, setup.state, steps, n_warmup=warmup, kind=kind, threads=threads,
+                               timeout=3600)
+    return info
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    setup, label = workload(args.workload)
+    threads = os.cpu_count() or 1
+    info = run_reference_binary("cpu", setup, args.warmup, args.steps, threads)
+    secs = info["seconds"]
+    value = setup.interior_cells * args.steps / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": label, "cells": setup.interior_cells, "bc": setup.bc, "eta": "uniform + gaussian bump table"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+                         "sample": f"{label}: {args.warmup} warm-up + {args.steps} timed steps of the reference "
+                                   f"library built for the host (Thrust OMP backend) on {threads} threads, "
+                                   f"{cpu_model()}"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
+    import numpy as np
+    import torch
+
+    from resistivemhd_gpu_b200 import Solver
+
+    torch.cuda.set_device(local_rank)
+    setup, label = workload(args.workload)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+
+    sol = Solver.from_setup(setup, precision=args.precision, device=local_rank)
+    sol.run(args.warmup)
+    sol.dt  # synchronise
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed region: exactly K steps ----
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        ms = sol.run_timed(args.steps)
+    barrier()
+    crashed = sol.check_crashed()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    cells = setup.interior_cells
+    value = world * cells * args.steps / (ms_max * 1e-3)
+
+    # ---- per-kernel breakdown for the roofline (same stream, CUDA events) ----
+    prof = [sol.profile_step() for _ in range(max(3, min(args.steps, 20)))]
+    st1 = statistics.median(p[0] for p in prof)
+    bn1 = statistics.median(p[1] for p in prof)
+    st2 = statistics.median(p[2] for p in prof)
+    bn2 = statistics.median(p[3] for p in prof)
+    ab = algorithmic_bytes(setup)
+    peak, peak_kind = hbm_peak()
+    achieved = (ab["stage1"] + ab["stage2"]) / ((st1 + st2) * 1e-3) / 1e9
+    traffic = traffic_from_profile(label)
+    roofline = {
+        "kernel": "stage_kernel (stage 1 + stage 2 per step)", "bound": "hbm", "achieved": achieved,
+        "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+        "traffic": (traffic["stage1"] + traffic["stage2"]) / 2 if traffic else None,
+        "algorithmic_bytes_per_launch": (ab["stage1"] + ab["stage2"]) / 2,
+        "launch_ms": {"stage1": st1, "boundary1": bn1, "stage2": st2, "boundary2_cfl": bn2},
+        "note": "FP64-issue bound: see fp64 and DESIGN.md",
+    }
+
+    # ---- end-to-end through the public API with pinned host buffers ----
+    e2e = None
+    if args.e2e:
+        host = torch.empty(setup.state.shape, dtype=torch.float64, pin_memory=True).numpy()
+        host[...] = setup.state
+        out = torch.empty(setup.state.shape, dtype=torch.float64, pin_memory=True).numpy()
+        e2e_sol = Solver(setup.nx, setup.ny, setup.dx, setup.dy, gamma=setup.gamma, cfl=setup.cfl, eps=setup.eps,
+                         eta=setup.eta, bc=setup.bc, precision=args.precision, device=local_rank)
+        if setup.eta_table is not None:
+            e2e_sol.set_eta_table(setup.eta_table)
+        e2e_sol.set_state(host, apply_boundary=True)
+        e2e_sol.run(args.warmup)
+        e2e_sol.dt
+        barrier()
+        t0 = time.perf_counter()
+        e2e_sol.set_state(host, apply_boundary=True)          # H2D of the initial state
+        total = 0.0
+        for _ in range(args.steps):
+            e2e_sol.step()                                     # oneStepRK2
+            if e2e_sol.check_crashed():                        # checkCalculationIsCrashed (D2H)
+                break
+            total += e2e_sol.dt                                # totalTime += dt (D2H)
+        e2e_sol.get_state(out)                                 # getU (D2H of the result)
+        t1 = time.perf_counter()
+        el = torch.tensor([t1 - t0], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(el, op=dist.ReduceOp.MAX)
+        state_bytes = setup.state.nbytes
+        ctl_bytes = 48  # control block read back by each synchronising query
+        e2e = {"value": world * cells * args.steps / float(el.item()), "unit": METRIC,
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps + 2 * ctl_bytes,
+               "note": "set_state(pinned) + K x (step_rk2 + check_crashed + get_dt) + get_state(pinned), wall clock"}
+        e2e_sol.close()
+
+    line = None
+    if rank == 0:
+        clocks = clk.summary()
+        gpu_launches = 4 * args.steps
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": label, "cells": cells, "nx": setup.nx, "ny": setup.ny, "bc": setup.bc,
+                       "eta": "uniform 1e-3 + gaussian bump (cell-centred table)" if setup.eta_table is not None
+                       else f"uniform {setup.eta}",
+                       "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (2 x state = %.0f MB)" % (2 * setup.state.nbytes / 1e6)},
+            "roofline": roofline,
+            "clocks": clocks,
+            "gpu_launches": gpu_launches,
+            "crashed": crashed,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        # FP64 issue bound: executed FP64 instruction rate is in the ncu summary.
+        line["fp64"] = {"peak_nominal_tflops": B200_FP64_TFLOPS_NOMINAL,
+                        "see": f"profiles/stage_kernel_{label}.md"}
+    sol.close()
+
+    if rank == 0 and world == 1 and args.baselines:
+        # reference's own CUDA build on the same GPU (bounded sample)
+        try:
+            info = run_reference_binary("gpu", setup, 2, min(args.steps, 10), None)
+            rv = cells * info["steps"] / info["seconds"]
+            line["ref_gpu"] = {"value": rv, "unit": METRIC, "speedup": value / rv,
+                               "sample": f"{label}: 2 warm-up + {info['steps']} steps of the reference library "
+                                         "built for sm_100a (oneStepRK2 + checkCalculationIsCrashed), wall clock"}
+        except Exception as e:  # reported, never fatal
+            line["ref_gpu"] = {"unavailable": str(e)[:200]}
+        # reference's own CPU build on the host cores (bounded sample)
+        try:
+            threads = os.cpu_count() or 1
+            k = 6
+            info = run_reference_binary("cpu", setup, 1, k, threads)
+            cv = cells * k / info["seconds"]
+            line["cpu_baseline"] = {"value": cv, "unit": METRIC, "cores": threads, "kind": "reference",
+                                    "sample": f"{label}: 1 warm-up + {k} timed steps of the reference library built "
+                                              f"for the host (Thrust OMP backend), {threads} threads, {cpu_model()}"}
+        except Exception as e:
+            line["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64_fast", "fp64_exact"], default="fp64_fast")
+    ap.add_argument("--workload", choices=["harris", "orszag_tang"], default="harris")
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-baselines", dest="baselines", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        ours_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -121,6 +121,15 @@ int rmhd2d_step_rk2(rmhd2d_solver *s);
 /* nsteps calls of rmhd2d_step_rk2, replayed from a captured CUDA graph. */
 int rmhd2d_run(rmhd2d_solver *s, int nsteps);
 
+/* Measurement hooks (the reference has no timers).
+   rmhd2d_run_timed: rmhd2d_run(nsteps) bracketed by CUDA events on the
+   solver's stream; waits and returns the elapsed device time in *ms.
+   rmhd2d_profile_step: one step with CUDA events around each of its four
+   launches (stage 1, boundary, stage 2, boundary + CFL reduction); waits and
+   returns their device durations in ms[0..3]. */
+int rmhd2d_run_timed(rmhd2d_solver *s, int nsteps, float *ms);
+int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4);
+
 /* dt of the most recent step: the reference's global `dt` after
    oneStepRK2 (const.hpp:20). */
 int rmhd2d_get_dt(rmhd2d_solver *s, double *dt);

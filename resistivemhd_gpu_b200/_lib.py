@@ -48,6 +48,8 @@ SIGNATURES = [
     ("rmhd2d_calculate_dt", ctypes.c_int, [_S, _D]),
     ("rmhd2d_step_rk2", ctypes.c_int, [_S]),
     ("rmhd2d_run", ctypes.c_int, [_S, ctypes.c_int]),
+    ("rmhd2d_run_timed", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    ("rmhd2d_profile_step", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_float)]),
     ("rmhd2d_get_dt", ctypes.c_int, [_S, _D]),
     ("rmhd2d_get_total_time", ctypes.c_int, [_S, _D]),
     ("rmhd2d_check_crashed", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_int)]),

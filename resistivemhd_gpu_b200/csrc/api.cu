@@ -420,6 +420,60 @@ int rmhd2d_run(rmhd2d_solver *s, int nsteps)
     return RMHD2D_OK;
 }
 
+int rmhd2d_run_timed(rmhd2d_solver *s, int nsteps, float *ms)
+{
+    if (!s || !ms) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s->stream));
+    int rc = rmhd2d_run(s, nsteps);
+    CK(cudaEventRecord(e1, s->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    return sync_and_check(s);
+}
+
+int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
+{
+    if (!s || !ms4) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    cudaEvent_t ev[5];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    const int parity = s->parity;
+    StageArgs a{};
+    a.g = s->g;
+    a.eta = s->eta;
+    a.row2 = s->g.bc == BC_SYMMETRIC ? s->row2 : nullptr;
+    a.ctl = s->ctl;
+    a.parity = parity;
+    auto launch = s->cfg.precision == RMHD2D_FP64_FAST ? fast::launch_stage : exact::launch_stage;
+    CK(cudaEventRecord(ev[0], s->stream));
+    a.src = s->A; a.un = s->A; a.dst = s->B;
+    launch(1, &s->mapA, a, s->stream);
+    CK(cudaEventRecord(ev[1], s->stream));
+    launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
+    CK(cudaEventRecord(ev[2], s->stream));
+    a.src = s->B; a.un = s->A; a.dst = s->A;
+    launch(2, &s->mapB, a, s->stream);
+    CK(cudaEventRecord(ev[3], s->stream));
+    launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
+    CK(cudaEventRecord(ev[4], s->stream));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev[4]));
+    for (int n = 0; n < 4; ++n) CK(cudaEventElapsedTime(&ms4[n], ev[n], ev[n + 1]));
+    for (auto &e : ev) cudaEventDestroy(e);
+    s->parity ^= 1;
+    s->steps += 1;
+    return sync_and_check(s);
+}
+
 int rmhd2d_get_dt(rmhd2d_solver *s, double *dt)
 {
     if (!s || !dt) return fail(s, RMHD2D_ERR_INVALID, "null argument");

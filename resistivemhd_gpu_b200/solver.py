@@ -128,6 +128,18 @@ class Solver:
     def run(self, nsteps: int) -> None:
         self._ck(self._lib.rmhd2d_run(self._h, int(nsteps)))
 
+    def run_timed(self, nsteps: int) -> float:
+        """run(nsteps) timed with CUDA events on the solver's stream; ms."""
+        ms = ctypes.c_float()
+        self._ck(self._lib.rmhd2d_run_timed(self._h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def profile_step(self) -> list[float]:
+        """One step; device ms of [stage 1, boundary, stage 2, boundary+CFL]."""
+        ms = (ctypes.c_float * 4)()
+        self._ck(self._lib.rmhd2d_profile_step(self._h, ms))
+        return [float(v) for v in ms]
+
     @property
     def dt(self) -> float:
         d = ctypes.c_double()
