@@ -12,6 +12,17 @@
 
 namespace rmhd2d {
 
+__host__ __device__ __forceinline__ double bits_to_double(unsigned long long b)
+{
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)b);
+#else
+    double d;
+    memcpy(&d, &b, sizeof(d));
+    return d;
+#endif
+}
+
 // thrust::min / thrust::max semantics ((b < a) ? b : a).
 __device__ __forceinline__ double tmin(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double tmax(double a, double b) { return (a < b) ? b : a; }
@@ -180,6 +191,116 @@ __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double g
     }
 }
 
+// HLLD flux of the fast variant: the same wave-speed estimates, star and
+// double-star states and candidate selection as hlld_flux (hlld.cu:256-565),
+// rearranged for the FP64 pipe.  It differs from the exact form by rounding
+// only: one correctly rounded reciprocal per distinct denominator (8 instead
+// of 28 divisions), squared sound/Alfven speeds used directly (the reference
+// squares their square roots), sqrt(rho*) and |bX|/sqrt(rho*) from one rsqrt,
+// and bX taken once (left and right states share the interface-normal B).
+__device__ __forceinline__ void hlld_flux_fast(const Prim &L, const Prim &R, double gm, double inv_gm1,
+                                               double EPS, double f[8])
+{
+    const double bX = L.bX;
+    const double bx2 = bX * bX;
+    const double iRL = __drcp_rn(L.rho), iRR = __drcp_rn(R.rho);
+    const double b2L = bx2 + L.bY * L.bY + L.bZ * L.bZ;
+    const double b2R = bx2 + R.bY * R.bY + R.bZ * R.bZ;
+    const double eL = L.p * inv_gm1 + 0.5 * L.rho * (L.u * L.u + L.v * L.v + L.w * L.w) + 0.5 * b2L;
+    const double eR = R.p * inv_gm1 + 0.5 * R.rho * (R.u * R.u + R.v * R.v + R.w * R.w) + 0.5 * b2R;
+    const double pTL = L.p + 0.5 * b2L, pTR = R.p + 0.5 * b2R;
+
+    const double cs2L = gm * L.p * iRL, ca2L = b2L * iRL, va2L = bx2 * iRL;
+    const double cs2R = gm * R.p * iRR, ca2R = b2R * iRR, va2R = bx2 * iRR;
+    const double sL = cs2L + ca2L, sR = cs2R + ca2R;
+    // The reference takes sqrt of each squared speed, so a negative one makes
+    // its fast speed NaN; keep that.
+    const double qnan = bits_to_double(0x7FF8000000000000ull);
+    const bool okL = (cs2L >= 0.0) & (ca2L >= 0.0) & (va2L >= 0.0);
+    const bool okR = (cs2R >= 0.0) & (ca2R >= 0.0) & (va2R >= 0.0);
+    const double cfL = okL ? sqrt(0.5 * (sL + sqrt(sL * sL - 4.0 * cs2L * va2L))) : qnan;
+    const double cfR = okR ? sqrt(0.5 * (sR + sqrt(sR * sR - 4.0 * cs2R * va2R))) : qnan;
+
+    const double uL = L.u, uR = R.u;
+    double SL = tmin(uL, uR) - tmax(cfL, cfR);
+    double SR = tmax(uL, uR) + tmax(cfL, cfR);
+    SL = tmin(SL, 0.0);
+    SR = tmax(SR, 0.0);
+
+    const double dSL = SL - uL, dSR = SR - uR;
+    const double rdSL = L.rho * dSL, rdSR = R.rho * dSR;
+    const double iden = __drcp_rn(rdSR - rdSL + EPS);
+    const double SM = (rdSR * uR - rdSL * uL - pTR + pTL) * iden;
+    const double pT1 = (rdSR * pTL - rdSL * pTR + rdSL * rdSR * (uR - uL)) * iden;
+
+    const double iSLM = __drcp_rn(SL - SM + EPS), iSRM = __drcp_rn(SR - SM + EPS);
+    const double rho1L = rdSL * iSLM, rho1R = rdSR * iSRM;
+    const double id1L = __drcp_rn(rdSL * (SL - SM) - bx2 + EPS);
+    const double id1R = __drcp_rn(rdSR * (SR - SM) - bx2 + EPS);
+    const double tL = bX * (SM - uL) * id1L, tR = bX * (SM - uR) * id1R;
+    const double v1L = L.v - L.bY * tL, w1L = L.w - L.bZ * tL;
+    const double v1R = R.v - R.bY * tR, w1R = R.w - R.bZ * tR;
+    const double gL = (rdSL * dSL - bx2) * id1L, gR = (rdSR * dSR - bx2) * id1R;
+    const double bY1L = L.bY * gL, bZ1L = L.bZ * gL;
+    const double bY1R = R.bY * gR, bZ1R = R.bZ * gR;
+    const double vbL = uL * bX + L.v * L.bY + L.w * L.bZ, vbR = uR * bX + R.v * R.bY + R.w * R.bZ;
+    const double vb1L = SM * bX + v1L * bY1L + w1L * bZ1L, vb1R = SM * bX + v1R * bY1R + w1R * bZ1R;
+    const double e1L = (dSL * eL - pTL * uL + pT1 * SM + bX * (vbL - vb1L)) * iSLM;
+    const double e1R = (dSR * eR - pTR * uR + pT1 * SM + bX * (vbR - vb1R)) * iSRM;
+
+    const double rsL = rsqrt(rho1L), rsR = rsqrt(rho1R);
+    const double sqL = rho1L * rsL, sqR = rho1R * rsR;
+    const double abx = fabs(bX);
+    const double S1L = SM - abx * rsL, S1R = SM + abx * rsR;
+    const double sb = sgn(bX);
+    const double id2 = __drcp_rn(sqL + sqR + EPS);
+    const double sqLR = sqL * sqR;
+    const double v2 = (sqL * v1L + sqR * v1R + (bY1R - bY1L) * sb) * id2;
+    const double w2 = (sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sb) * id2;
+    const double bY2 = (sqL * bY1R + sqR * bY1L + sqLR * (v1R - v1L) * sb) * id2;
+    const double bZ2 = (sqL * bZ1R + sqR * bZ1L + sqLR * (w1R - w1L) * sb) * id2;
+    const double vb2 = SM * bX + v2 * bY2 + w2 * bZ2;
+    const double e2L = e1L - sqL * (vb1L - vb2) * sb;
+    const double e2R = e1R + sqR * (vb1R - vb2) * sb;
+
+    const bool bOL = SL > 0.0;
+    const bool bML = (SL <= 0.0) && (0.0 < S1L);
+    const bool bIL = (S1L <= 0.0) && (0.0 < SM);
+    const bool bOR = SR <= 0.0;
+    const bool bMR = (S1R <= 0.0) && (0.0 < SR);
+    const bool bIR = (SM <= 0.0) && (0.0 < S1R);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) f[n] = 0.0;
+    if (bOL) add_one_flux(L.rho, uL, L.v, L.w, bX, L.bY, L.bZ, eL, pTL, f);
+    if (bML) add_one_flux(rho1L, SM, v1L, w1L, bX, bY1L, bZ1L, e1L, pT1, f);
+    if (bIL) add_one_flux(rho1L, SM, v2, w2, bX, bY2, bZ2, e2L, pT1, f);
+    if (bOR) add_one_flux(R.rho, uR, R.v, R.w, bX, R.bY, R.bZ, eR, pTR, f);
+    if (bMR) add_one_flux(rho1R, SM, v1R, w1R, bX, bY1R, bZ1R, e1R, pT1, f);
+    if (bIR) add_one_flux(rho1R, SM, v2, w2, bX, bY2, bZ2, e2R, pT1, f);
+    // NaN wave speeds select no candidate here, while the reference's
+    // weighted sum turns them into a NaN flux: do the same.
+    if ((SL != SL) | (SR != SR) | (SM != SM) | (S1L != S1L) | (S1R != S1R)) {
+#pragma unroll
+        for (int n = 0; n < 8; ++n) f[n] = qnan;
+    }
+}
+
+// calculateDtFunctor arithmetic with reciprocals (fast variant); a negative
+// squared sound speed gives NaN as the reference's sqrt(gamma p / rho) does.
+
+__device__ __forceinline__ double cfl_rate_fast(double rho, double mx, double my, double mz, double bX,
+                                                double bY, double bZ, double e, double gm, double idx,
+                                                double idy)
+{
+    const double ir = __drcp_rn(rho);
+    const double u = mx * ir, v = my * ir, w = mz * ir;
+    const double b2 = bX * bX + bY * bY + bZ * bZ;
+    const double p = (gm - 1.0) * (e - 0.5 * rho * (u * u + v * v + w * w) - 0.5 * b2);
+    const double cs2 = gm * p * ir, ca2 = b2 * ir;
+    const double c = ((cs2 >= 0.0) & (ca2 >= 0.0)) ? sqrt(cs2 + ca2) : bits_to_double(0x7FF8000000000000ull);
+    return (fabs(u) + c) * idx + (fabs(v) + c) * idy;
+}
+
 // resistiveMHD_2D.cu:247-274 calculateDtFunctor, returning the denominator
 // term a = maxSpeedX/dx + maxSpeedY/dy; the cell's dt candidate is
 // 1/(a + EPS), so the minimum over cells is 1/(max a + EPS).
@@ -209,16 +330,6 @@ __device__ __forceinline__ unsigned long long rate_bits(double a)
     return (unsigned long long)__double_as_longlong(a);
 }
 
-__host__ __device__ __forceinline__ double bits_to_double(unsigned long long b)
-{
-#ifdef __CUDA_ARCH__
-    return __longlong_as_double((long long)b);
-#else
-    double d;
-    memcpy(&d, &b, sizeof(d));
-    return d;
-#endif
-}
 
 // dt of a step from the reduced rates (resistiveMHD_2D.cu:286-288):
 // dtMin = 1/(max a + EPS), or NaN when cell 0's candidate is NaN;

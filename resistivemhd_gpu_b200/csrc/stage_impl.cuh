@@ -5,6 +5,10 @@
 
 #include "stage.cuh"
 
+#ifndef RMHD_FAST_MATH
+#define RMHD_FAST_MATH 0
+#endif
+
 #ifndef RMHD_VARIANT
 #error "define RMHD_VARIANT (exact or fast) before including stage_impl.cuh"
 #endif
@@ -125,6 +129,9 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageArgs a)
     }
 
     const double gm = g.gamma, EPS = g.eps;
+#if RMHD_FAST_MATH
+    const double inv_gm1 = 1.0 / (gm - 1.0);
+#endif
 
     // ---- primitives on (TI+4) x (TJ+4) cells ----
     // calculate_half_Q.cu:4-38 on the centred state (shift kernels,
@@ -136,9 +143,16 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageArgs a)
         const double *u0 = Ut + ui * UJ + uj;
         const int F = UI * UJ;
         const double rho = u0[RHO * F];
+#if RMHD_FAST_MATH
+        const double irho = __drcp_rn(rho);
+        const double u = u0[MX * F] * irho;
+        const double v = u0[MY * F] * irho;
+        const double w = u0[MZ * F] * irho;
+#else
         const double u = u0[MX * F] / rho;
         const double v = u0[MY * F] / rho;
         const double w = u0[MZ * F] / rho;
+#endif
         const double bXc = 0.5 * (u0[BXF * F] + u0[BXF * F - UJ]);
         const double bYc = 0.5 * (u0[BYF * F] + u0[BYF * F - 1]);
         const double bZ = u0[BZF * F];
@@ -166,13 +180,23 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageArgs a)
     {
         const int PF = PI_ * PJ_, RF = RI_ * RJ_;
         const double two_dx = 2.0 * g.dx, two_dy = 2.0 * g.dy;
+#if RMHD_FAST_MATH
+        const double i2dx = 1.0 / two_dx, i2dy = 1.0 / two_dy;
+#endif
         for (int c = tid; c < RF; c += STAGE_THREADS) {
             const int ri = c / RJ_, rj = c - ri * RJ_;
             const double *p0 = Ps + (ri + 1) * PJ_ + (rj + 1);
+#if RMHD_FAST_MATH
+            const double jY = -(p0[P_BZ * PF + PJ_] - p0[P_BZ * PF - PJ_]) * i2dx;
+            const double jX = (p0[P_BZ * PF + 1] - p0[P_BZ * PF - 1]) * i2dy;
+            const double jZ = (p0[P_BYC * PF + PJ_] - p0[P_BYC * PF - PJ_]) * i2dx
+                            - (p0[P_BXC * PF + 1] - p0[P_BXC * PF - 1]) * i2dy;
+#else
             const double jY = -(p0[P_BZ * PF + PJ_] - p0[P_BZ * PF - PJ_]) / two_dx;
             const double jX = (p0[P_BZ * PF + 1] - p0[P_BZ * PF - 1]) / two_dy;
             const double jZ = (p0[P_BYC * PF + PJ_] - p0[P_BYC * PF - PJ_]) / two_dx
                             - (p0[P_BXC * PF + 1] - p0[P_BXC * PF - 1]) / two_dy;
+#endif
             const int gi = i0 - 1 + ri, gj = j0 - 1 + rj;
             double eta = g.eta;
             if (a.eta) {
@@ -230,7 +254,11 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageArgs a)
             Prim L{qL[0], qL[1], qL[2], qL[3], bn, qL[4], qL[5], qL[6]};
             Prim R{qR[0], qR[1], qR[2], qR[3], bn, qR[4], qR[5], qR[6]};
             double f[8];
+#if RMHD_FAST_MATH
+            hlld_flux_fast(L, R, gm, inv_gm1, EPS, f);
+#else
             hlld_flux<RMHD_ALL_CANDIDATES>(L, R, gm, EPS, f);
+#endif
             const double *r0 = Rs + li * RJ_ + lj;   // cell (i, j) of the interface
             const int rs = isF ? RJ_ : 1;            // its neighbour across the interface
             if (isF) {
@@ -332,8 +360,13 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageArgs a)
         unsigned long long bits = 0ull;
         int nan_e = 0;
         if (own) {
+#if RMHD_FAST_MATH
+            const double r = cfl_rate_fast(nv[RHO], nv[MX], nv[MY], nv[MZ], nv[BXF], nv[BYF], nv[BZF], nv[EN],
+                                           gm, 1.0 / g.dx, 1.0 / g.dy);
+#else
             const double r = cfl_rate(nv[RHO], nv[MX], nv[MY], nv[MZ], nv[BXF], nv[BYF], nv[BZF], nv[EN],
                                       gm, g.dx, g.dy);
+#endif
             bits = rate_bits(r);
             nan_e = nv[EN] != nv[EN];
         }
