@@ -41,7 +41,7 @@ struct rmhd2d_solver {
     double *row2 = nullptr;      // nx doubles
     Control *ctl = nullptr;      // device control block
     Control *ctl_host = nullptr; // pinned mirror for readback
-    CUtensorMap mapA{}, mapB{};
+    CUtensorMap mapA{}, mapB{}, mapE{};
     int parity = 0;
     bool has_state = false;
     long long steps = 0;
@@ -101,6 +101,21 @@ bool encode_state_map(CUtensorMap *map, const Grid &g, double *base)
     return r == CUDA_SUCCESS;
 }
 
+// 2-D tensor map over the eta plane: (j: ny, i: nx), box (UJ, UI).
+bool encode_eta_map(CUtensorMap *map, const Grid &g, double *base)
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)g.ny, (cuuint64_t)g.nx};
+    cuuint64_t strides[1] = {(cuuint64_t)g.pitch * 8};
+    cuuint32_t box[2] = {(cuuint32_t)UJ, (cuuint32_t)UI};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 int sync_and_check(rmhd2d_solver *s)
 {
     CK(cudaStreamSynchronize(s->stream));
@@ -143,13 +158,13 @@ void enqueue_step(rmhd2d_solver *s, int parity)
     a.src = s->A;
     a.un = s->A;
     a.dst = s->B;
-    launch(1, &s->mapA, a, s->stream);
+    launch(1, &s->mapA, &s->mapE, a, s->stream);
     launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
     // stage 2: (U*, U^n) -> U^{n+1} in A
     a.src = s->B;
     a.un = s->A;
     a.dst = s->A;
-    launch(2, &s->mapB, a, s->stream);
+    launch(2, &s->mapB, &s->mapE, a, s->stream);
     launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
 }
 
@@ -349,6 +364,11 @@ int rmhd2d_set_eta_table(rmhd2d_solver *s, const double *host_eta)
     if (!s->eta) {
         CK(cudaMalloc(&s->eta, (size_t)s->g.plane * sizeof(double)));
         CK(cudaMemsetAsync(s->eta, 0, (size_t)s->g.plane * sizeof(double), s->stream));
+        if (!encode_eta_map(&s->mapE, s->g, s->eta)) {
+            cudaFree(s->eta);
+            s->eta = nullptr;
+            return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the eta table");
+        }
     }
     CK(cudaMemcpy2DAsync(s->eta, (size_t)s->g.pitch * sizeof(double), host_eta, (size_t)s->g.ny * sizeof(double),
                          (size_t)s->g.ny * sizeof(double), (size_t)s->g.nx, cudaMemcpyHostToDevice, s->stream));
@@ -456,12 +476,12 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
     auto launch = s->cfg.precision == RMHD2D_FP64_FAST ? fast::launch_stage : exact::launch_stage;
     CK(cudaEventRecord(ev[0], s->stream));
     a.src = s->A; a.un = s->A; a.dst = s->B;
-    launch(1, &s->mapA, a, s->stream);
+    launch(1, &s->mapA, &s->mapE, a, s->stream);
     CK(cudaEventRecord(ev[1], s->stream));
     launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
     CK(cudaEventRecord(ev[2], s->stream));
     a.src = s->B; a.un = s->A; a.dst = s->A;
-    launch(2, &s->mapB, a, s->stream);
+    launch(2, &s->mapB, &s->mapE, a, s->stream);
     CK(cudaEventRecord(ev[3], s->stream));
     launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
     CK(cudaEventRecord(ev[4], s->stream));

@@ -27,15 +27,36 @@ __host__ __device__ __forceinline__ double bits_to_double(unsigned long long b)
 __device__ __forceinline__ double tmin(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double tmax(double a, double b) { return (a < b) ? b : a; }
 
-// hlld.cu:26-32 Sign.
-__device__ __forceinline__ double sgn(double x) { return (double)((x > 0.0) - (x < 0.0)); }
+// hlld.cu:26-32 Sign, (x > 0) - (x < 0), as selects (no int conversion).
+__device__ __forceinline__ double sgn(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
 
-// minmod.hpp:6-16: sign_x * max(min(|x|, sign_x * y), EPS) with an int sign.
+// minmod.hpp:6-16: sign_x * max(min(|x|, sign_x * y), EPS) with an int
+// sign_x.  Written with selects: for x > 0 the reference computes
+// 1.0 * max(min(|x|, 1.0 * y), EPS), for x < 0 the negation of
+// max(min(|x|, -y), EPS), for x == 0 (or NaN) 0.0 * max(min(|x|, 0.0 * y), EPS);
+// multiplying by +-1 is exact, so this is bit-identical for every input.
 __device__ __forceinline__ double minmod(double x, double y, double eps)
 {
-    const int s = (x > 0.0) - (x < 0.0);
-    const double ds = (double)s;
-    return ds * tmax(tmin(fabs(x), ds * y), eps);
+    const double ax = fabs(x);
+    if (x > 0.0) return tmax(tmin(ax, y), eps);
+    if (x < 0.0) return -tmax(tmin(ax, -y), eps);
+    return 0.0 * tmax(tmin(ax, 0.0 * y), eps);
+}
+
+// Reciprocal by Newton-Raphson iteration on 1/a (x' = x + x (1 - a x), two
+// steps, each squaring the relative error) from the hardware seed
+// rcp.approx.ftz.f64; used by the fast variant only.  Accurate to about one
+// ulp for normal finite a; a = 0 or +-inf give NaN (the fast variant's
+// denominators carry the reference's +EPS and are never 0 in a finite state).
+__device__ __forceinline__ double rcp_nr(double a)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(a));
+    double e = fma(-a, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-a, r, 1.0);
+    r = fma(r, e, r);
+    return r;
 }
 
 // Interface state fed to HLLD: BasicParameter (basic_parameter_struct.hpp:5-27).
@@ -203,7 +224,7 @@ __device__ __forceinline__ void hlld_flux_fast(const Prim &L, const Prim &R, dou
 {
     const double bX = L.bX;
     const double bx2 = bX * bX;
-    const double iRL = __drcp_rn(L.rho), iRR = __drcp_rn(R.rho);
+    const double iRL = rcp_nr(L.rho), iRR = rcp_nr(R.rho);
     const double b2L = bx2 + L.bY * L.bY + L.bZ * L.bZ;
     const double b2R = bx2 + R.bY * R.bY + R.bZ * R.bZ;
     const double eL = L.p * inv_gm1 + 0.5 * L.rho * (L.u * L.u + L.v * L.v + L.w * L.w) + 0.5 * b2L;
@@ -229,14 +250,14 @@ __device__ __forceinline__ void hlld_flux_fast(const Prim &L, const Prim &R, dou
 
     const double dSL = SL - uL, dSR = SR - uR;
     const double rdSL = L.rho * dSL, rdSR = R.rho * dSR;
-    const double iden = __drcp_rn(rdSR - rdSL + EPS);
+    const double iden = rcp_nr(rdSR - rdSL + EPS);
     const double SM = (rdSR * uR - rdSL * uL - pTR + pTL) * iden;
     const double pT1 = (rdSR * pTL - rdSL * pTR + rdSL * rdSR * (uR - uL)) * iden;
 
-    const double iSLM = __drcp_rn(SL - SM + EPS), iSRM = __drcp_rn(SR - SM + EPS);
+    const double iSLM = rcp_nr(SL - SM + EPS), iSRM = rcp_nr(SR - SM + EPS);
     const double rho1L = rdSL * iSLM, rho1R = rdSR * iSRM;
-    const double id1L = __drcp_rn(rdSL * (SL - SM) - bx2 + EPS);
-    const double id1R = __drcp_rn(rdSR * (SR - SM) - bx2 + EPS);
+    const double id1L = rcp_nr(rdSL * (SL - SM) - bx2 + EPS);
+    const double id1R = rcp_nr(rdSR * (SR - SM) - bx2 + EPS);
     const double tL = bX * (SM - uL) * id1L, tR = bX * (SM - uR) * id1R;
     const double v1L = L.v - L.bY * tL, w1L = L.w - L.bZ * tL;
     const double v1R = R.v - R.bY * tR, w1R = R.w - R.bZ * tR;
@@ -253,7 +274,7 @@ __device__ __forceinline__ void hlld_flux_fast(const Prim &L, const Prim &R, dou
     const double abx = fabs(bX);
     const double S1L = SM - abx * rsL, S1R = SM + abx * rsR;
     const double sb = sgn(bX);
-    const double id2 = __drcp_rn(sqL + sqR + EPS);
+    const double id2 = rcp_nr(sqL + sqR + EPS);
     const double sqLR = sqL * sqR;
     const double v2 = (sqL * v1L + sqR * v1R + (bY1R - bY1L) * sb) * id2;
     const double w2 = (sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sb) * id2;
@@ -292,7 +313,7 @@ __device__ __forceinline__ double cfl_rate_fast(double rho, double mx, double my
                                                 double bY, double bZ, double e, double gm, double idx,
                                                 double idy)
 {
-    const double ir = __drcp_rn(rho);
+    const double ir = rcp_nr(rho);
     const double u = mx * ir, v = my * ir, w = mz * ir;
     const double b2 = bX * bX + bY * bY + bZ * bZ;
     const double p = (gm - 1.0) * (e - 0.5 * rho * (u * u + v * v + w * w) - 0.5 * b2);

@@ -41,6 +41,9 @@ constexpr int TJ = 32;
 constexpr int HALO = 3;
 constexpr int UI = TI + 2 * HALO;  // staged rows
 constexpr int UJ = TJ + 2 * HALO;  // staged columns (TMA inner box: UJ * 8 bytes, multiple of 16)
-constexpr int STAGE_THREADS = TI * TJ;
+// 320 threads: the 256 tile cells in the update phase, and stage 1's
+// (TI+1)(TJ+2) + (TI+2)(TJ+1) = 636 interfaces in two full rounds.
+constexpr int STAGE_THREADS = 320;
+static_assert(STAGE_THREADS >= TI * TJ, "one thread per tile cell in the update phase");
 
 }  // namespace rmhd2d

@@ -11,8 +11,9 @@
 // Data layout: 8 field planes of nx x pitch doubles (index i*pitch + j,
 // y contiguous), one allocation per state.  Each CTA owns TI x TJ interior
 // cells and stages them with a 3-cell halo on every side by one 3-D TMA load
-// (box TJ+6 x TI+6 x 8 fields) into shared memory; everything after that
-// load reads shared memory only.
+// (box TJ+6 x TI+6 x 8 fields) into shared memory, plus a 2-D TMA load of the
+// eta table on the same cells; everything after those loads reads shared
+// memory, except stage 2's read of U^n at its own cells.
 //
 // This header is compiled twice: into an "exact" variant (-fmad=false, all
 // six HLLD candidate fluxes formed), bit-identical to the reference
@@ -42,12 +43,14 @@ struct StageArgs {
 
 // One launcher per variant (stage_exact.cu, stage_fast.cu).
 namespace exact {
-void launch_stage(int stage, const CUtensorMap *tmap, const StageArgs &args, cudaStream_t stream);
+void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
+                  cudaStream_t stream);
 size_t stage_smem_bytes();
 int stage_regs(int stage);
 }  // namespace exact
 namespace fast {
-void launch_stage(int stage, const CUtensorMap *tmap, const StageArgs &args, cudaStream_t stream);
+void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
+                  cudaStream_t stream);
 size_t stage_smem_bytes();
 int stage_regs(int stage);
 }  // namespace fast
