@@ -41,7 +41,8 @@ struct rmhd2d_solver {
     double *row2 = nullptr;      // nx doubles
     Control *ctl = nullptr;      // device control block
     Control *ctl_host = nullptr; // pinned mirror for readback
-    CUtensorMap mapA{}, mapB{}, mapE{};
+    CUtensorMap mapA{}, mapB{};          // stage-1 source A, stage-2 source B (box rows per stage)
+    CUtensorMap mapE1{}, mapE2{};        // eta plane, stage-1 / stage-2 boxes
     int parity = 0;
     bool has_state = false;
     long long steps = 0;
@@ -86,14 +87,14 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-// 3-D tensor map over one state: (j: ny, i: nx, field: 8), box (UJ, UI, 8).
-bool encode_state_map(CUtensorMap *map, const Grid &g, double *base)
+// 3-D tensor map over one state: (j: ny, i: nx, field: 8), box (UJ, ui, 8).
+bool encode_state_map(CUtensorMap *map, const Grid &g, double *base, int ui)
 {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[3] = {(cuuint64_t)g.ny, (cuuint64_t)g.nx, (cuuint64_t)NFIELD};
     cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.plane * 8};
-    cuuint32_t box[3] = {(cuuint32_t)UJ, (cuuint32_t)UI, (cuuint32_t)NFIELD};
+    cuuint32_t box[3] = {(cuuint32_t)UJ, (cuuint32_t)ui, (cuuint32_t)NFIELD};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -101,14 +102,14 @@ bool encode_state_map(CUtensorMap *map, const Grid &g, double *base)
     return r == CUDA_SUCCESS;
 }
 
-// 2-D tensor map over the eta plane: (j: ny, i: nx), box (UJ, UI).
-bool encode_eta_map(CUtensorMap *map, const Grid &g, double *base)
+// 2-D tensor map over the eta plane: (j: ny, i: nx), box (UJ, ui).
+bool encode_eta_map(CUtensorMap *map, const Grid &g, double *base, int ui)
 {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[2] = {(cuuint64_t)g.ny, (cuuint64_t)g.nx};
     cuuint64_t strides[1] = {(cuuint64_t)g.pitch * 8};
-    cuuint32_t box[2] = {(cuuint32_t)UJ, (cuuint32_t)UI};
+    cuuint32_t box[2] = {(cuuint32_t)UJ, (cuuint32_t)ui};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -158,13 +159,13 @@ void enqueue_step(rmhd2d_solver *s, int parity)
     a.src = s->A;
     a.un = s->A;
     a.dst = s->B;
-    launch(1, &s->mapA, &s->mapE, a, s->stream);
+    launch(1, &s->mapA, &s->mapE1, a, s->stream);
     launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
     // stage 2: (U*, U^n) -> U^{n+1} in A
     a.src = s->B;
     a.un = s->A;
     a.dst = s->A;
-    launch(2, &s->mapB, &s->mapE, a, s->stream);
+    launch(2, &s->mapB, &s->mapE2, a, s->stream);
     launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
 }
 
@@ -296,7 +297,7 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
         cudaMemset(s->row2, 0, (size_t)g.nx * sizeof(double)) != cudaSuccess ||
         cudaMemset(s->ctl, 0, sizeof(Control)) != cudaSuccess)
         return bail(RMHD2D_ERR_CUDA, "device memset failed");
-    if (!encode_state_map(&s->mapA, g, s->A) || !encode_state_map(&s->mapB, g, s->B))
+    if (!encode_state_map(&s->mapA, g, s->A, stage_ui(1)) || !encode_state_map(&s->mapB, g, s->B, stage_ui(2)))
         return bail(RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     *out = s;
     return RMHD2D_OK;
@@ -364,7 +365,8 @@ int rmhd2d_set_eta_table(rmhd2d_solver *s, const double *host_eta)
     if (!s->eta) {
         CK(cudaMalloc(&s->eta, (size_t)s->g.plane * sizeof(double)));
         CK(cudaMemsetAsync(s->eta, 0, (size_t)s->g.plane * sizeof(double), s->stream));
-        if (!encode_eta_map(&s->mapE, s->g, s->eta)) {
+        if (!encode_eta_map(&s->mapE1, s->g, s->eta, stage_ui(1)) ||
+            !encode_eta_map(&s->mapE2, s->g, s->eta, stage_ui(2))) {
             cudaFree(s->eta);
             s->eta = nullptr;
             return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the eta table");
@@ -476,12 +478,12 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
     auto launch = s->cfg.precision == RMHD2D_FP64_FAST ? fast::launch_stage : exact::launch_stage;
     CK(cudaEventRecord(ev[0], s->stream));
     a.src = s->A; a.un = s->A; a.dst = s->B;
-    launch(1, &s->mapA, &s->mapE, a, s->stream);
+    launch(1, &s->mapA, &s->mapE1, a, s->stream);
     CK(cudaEventRecord(ev[1], s->stream));
     launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
     CK(cudaEventRecord(ev[2], s->stream));
     a.src = s->B; a.un = s->A; a.dst = s->A;
-    launch(2, &s->mapB, &s->mapE, a, s->stream);
+    launch(2, &s->mapB, &s->mapE2, a, s->stream);
     CK(cudaEventRecord(ev[3], s->stream));
     launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
     CK(cudaEventRecord(ev[4], s->stream));

@@ -292,12 +292,29 @@ __device__ __forceinline__ void hlld_flux_fast(const Prim &L, const Prim &R, dou
     const bool bIR = (SM <= 0.0) && (0.0 < S1R);
 #pragma unroll
     for (int n = 0; n < 8; ++n) f[n] = 0.0;
-    if (bOL) add_one_flux(L.rho, uL, L.v, L.w, bX, L.bY, L.bZ, eL, pTL, f);
-    if (bML) add_one_flux(rho1L, SM, v1L, w1L, bX, bY1L, bZ1L, e1L, pT1, f);
-    if (bIL) add_one_flux(rho1L, SM, v2, w2, bX, bY2, bZ2, e2L, pT1, f);
-    if (bOR) add_one_flux(R.rho, uR, R.v, R.w, bX, R.bY, R.bZ, eR, pTR, f);
-    if (bMR) add_one_flux(rho1R, SM, v1R, w1R, bX, bY1R, bZ1R, e1R, pT1, f);
-    if (bIR) add_one_flux(rho1R, SM, v2, w2, bX, bY2, bZ2, e2R, pT1, f);
+    const int nsel = (int)bOL + (int)bML + (int)bIL + (int)bOR + (int)bMR + (int)bIR;
+    if (nsel == 1) {
+        // The usual case: one region is selected; pick its state with
+        // selects and form one flux (no per-candidate divergence in a warp).
+        const bool lft = bOL | bML | bIL;
+        const bool outer = bOL | bOR, inner = bIL | bIR;
+        const double rho = bOL ? L.rho : (bOR ? R.rho : (lft ? rho1L : rho1R));
+        const double u = bOL ? uL : (bOR ? uR : SM);
+        const double v = outer ? (bOL ? L.v : R.v) : (inner ? v2 : (bML ? v1L : v1R));
+        const double w = outer ? (bOL ? L.w : R.w) : (inner ? w2 : (bML ? w1L : w1R));
+        const double by = outer ? (bOL ? L.bY : R.bY) : (inner ? bY2 : (bML ? bY1L : bY1R));
+        const double bz = outer ? (bOL ? L.bZ : R.bZ) : (inner ? bZ2 : (bML ? bZ1L : bZ1R));
+        const double e = bOL ? eL : (bOR ? eR : (bML ? e1L : (bIL ? e2L : (bMR ? e1R : e2R))));
+        const double pT = bOL ? pTL : (bOR ? pTR : pT1);
+        add_one_flux(rho, u, v, w, bX, by, bz, e, pT, f);
+    } else {
+        if (bOL) add_one_flux(L.rho, uL, L.v, L.w, bX, L.bY, L.bZ, eL, pTL, f);
+        if (bML) add_one_flux(rho1L, SM, v1L, w1L, bX, bY1L, bZ1L, e1L, pT1, f);
+        if (bIL) add_one_flux(rho1L, SM, v2, w2, bX, bY2, bZ2, e2L, pT1, f);
+        if (bOR) add_one_flux(R.rho, uR, R.v, R.w, bX, R.bY, R.bZ, eR, pTR, f);
+        if (bMR) add_one_flux(rho1R, SM, v1R, w1R, bX, bY1R, bZ1R, e1R, pT1, f);
+        if (bIR) add_one_flux(rho1R, SM, v2, w2, bX, bY2, bZ2, e2R, pT1, f);
+    }
     // NaN wave speeds select no candidate here, while the reference's
     // weighted sum turns them into a NaN flux: do the same.
     if ((SL != SL) | (SR != SR) | (SM != SM) | (S1L != S1L) | (S1R != S1R)) {

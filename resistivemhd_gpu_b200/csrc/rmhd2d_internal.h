@@ -35,15 +35,20 @@ struct Control {
 
 enum KernelError { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };
 
-// Tile of the fused stage kernel: TI cells along x (i) by TJ along y (j).
-constexpr int TI = 8;
+// Tiles of the fused stage kernels: TI cells along x (i) by TJ along y (j).
+// Stage 1 also computes the ring of fluxes its corner EMF needs, stage 2
+// only the tile's own interfaces, so their best tile heights differ: with
+// 320 threads stage 1 (8 x 32) has 636 interfaces and stage 2 (9 x 32) 617,
+// two nearly full rounds each.
 constexpr int TJ = 32;
 constexpr int HALO = 3;
-constexpr int UI = TI + 2 * HALO;  // staged rows
+constexpr int STAGE1_TI = 8;
+constexpr int STAGE2_TI = 9;
 constexpr int UJ = TJ + 2 * HALO;  // staged columns (TMA inner box: UJ * 8 bytes, multiple of 16)
-// 320 threads: the 256 tile cells in the update phase, and stage 1's
-// (TI+1)(TJ+2) + (TI+2)(TJ+1) = 636 interfaces in two full rounds.
 constexpr int STAGE_THREADS = 320;
-static_assert(STAGE_THREADS >= TI * TJ, "one thread per tile cell in the update phase");
+static_assert(STAGE_THREADS >= STAGE1_TI * TJ && STAGE_THREADS >= STAGE2_TI * TJ,
+              "one thread per tile cell in the update phase");
+constexpr int stage_ti(int stage) { return stage == 1 ? STAGE1_TI : STAGE2_TI; }
+constexpr int stage_ui(int stage) { return stage_ti(stage) + 2 * HALO; }
 
 }  // namespace rmhd2d

@@ -10,7 +10,7 @@
 //
 // Data layout: 8 field planes of nx x pitch doubles (index i*pitch + j,
 // y contiguous), one allocation per state.  Each CTA owns TI x TJ interior
-// cells and stages them with a 3-cell halo on every side by one 3-D TMA load
+// cells (TI = 8 in stage 1, 9 in stage 2, TJ = 32) and stages them with a 3-cell halo on every side by one 3-D TMA load
 // (box TJ+6 x TI+6 x 8 fields) into shared memory, plus a 2-D TMA load of the
 // eta table on the same cells; everything after those loads reads shared
 // memory, except stage 2's read of U^n at its own cells.
@@ -45,13 +45,13 @@ struct StageArgs {
 namespace exact {
 void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream);
-size_t stage_smem_bytes();
+size_t stage_smem_bytes(int stage);
 int stage_regs(int stage);
 }  // namespace exact
 namespace fast {
 void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream);
-size_t stage_smem_bytes();
+size_t stage_smem_bytes(int stage);
 int stage_regs(int stage);
 }  // namespace fast
 

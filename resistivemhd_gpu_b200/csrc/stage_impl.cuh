@@ -16,51 +16,58 @@
 namespace rmhd2d {
 namespace RMHD_VARIANT {
 
-// ---- shared-memory carve-up (doubles) ----
-// Ut [8][UI][UJ]       TMA: U at i0-3..i0+TI+2, j0-3..j0+TJ+2 (kept for the whole CTA)
-// Et [UI][UJ]          TMA: eta table on the same cells (when a table is set)
-// Ps [7][TI+4][TJ+4]   u, v, w, centred bX, centred bY, x- and y-sweep pressures
-// Rs [3][TI+2][TJ+2]   eta*Jx, eta*Jy, eta*Jz per cell; reused for the corner EMF
-// Fs [7][TI+1][TJ+2]   x fluxes f0 f1 f2 f3 f5 f6 f7 at i+1/2
-// Gs [7][TI+2][TJ+1]   y fluxes g0 g1 g2 g3 g4 g6 g7 at j+1/2
-constexpr int PI_ = TI + 4, PJ_ = TJ + 4;
-constexpr int RI_ = TI + 2, RJ_ = TJ + 2;
-constexpr int FI_ = TI + 1, FJ_ = TJ + 2;
-constexpr int GI_ = TI + 2, GJ_ = TJ + 1;
-constexpr int EI_ = TI + 1, EJ_ = TJ + 1;
-constexpr int UF = UI * UJ;          // doubles per staged field
-constexpr int PF = PI_ * PJ_;
-constexpr int RF = RI_ * RJ_;
-constexpr int SF = FI_ * FJ_;
-constexpr int SG = GI_ * GJ_;
-constexpr int U_DOUBLES = NFIELD * UF;
-constexpr int E_DOUBLES = UF;
-constexpr int P_DOUBLES = 7 * PF;
-constexpr int R_DOUBLES = 3 * RF;
-constexpr int F_DOUBLES = 7 * SF;
-constexpr int G_DOUBLES = 7 * SG;
-static_assert(EI_ * EJ_ <= R_DOUBLES, "corner EMF must fit in the eta*J region");
-static_assert(STAGE_THREADS / 32 <= P_DOUBLES, "per-warp maxima must fit in the primitive region");
-constexpr size_t SMEM_BYTES =
-    (size_t)(U_DOUBLES + E_DOUBLES + P_DOUBLES + R_DOUBLES + F_DOUBLES + G_DOUBLES) * 8 + 16;
-constexpr unsigned U_BYTES = (unsigned)(U_DOUBLES * 8);
-constexpr unsigned E_BYTES = (unsigned)(E_DOUBLES * 8);
+// ---- per-stage tile geometry and shared-memory carve-up (doubles) ----
+// Ut [8][UI][UJ]        TMA: U at i0-3..i0+TI+2, j0-3..j0+TJ+2 (kept for the whole CTA)
+// Et [UI][UJ]           TMA: eta table on the same cells (when a table is set)
+// Ps [7][TI+4][TJ+4]    u, v, w, centred bX, centred bY, x- and y-sweep pressures
+// Rs [3][TI+2][TJ+2]    eta*Jx, eta*Jy, eta*Jz per cell; reused for the corner EMF
+// Fs [NC][TI+1][F_NJ]   x fluxes f0 f1 f2 f3 f6 f7 (+ f5 in stage 1) at i+1/2
+// Gs [NC][G_NI][TJ+1]   y fluxes g0 g1 g2 g3 g6 g7 (+ g4 in stage 1) at j+1/2
+// Stage 1 needs x fluxes on rows j0-1..j0+TJ and y fluxes on columns
+// i0-1..i0+TI for its corner EMF; stage 2 only the tile's own interfaces and
+// no EMF components.
+template <int STAGE> struct Tile {
+    static constexpr int TI = stage_ti(STAGE);
+    static constexpr int UI = TI + 2 * HALO;
+    static constexpr int PI_ = TI + 4, PJ_ = TJ + 4;
+    static constexpr int RI_ = TI + 2, RJ_ = TJ + 2;
+    static constexpr int NC = STAGE == 1 ? 7 : 6;            // flux components stored
+    static constexpr int F_NI = TI + 1;
+    static constexpr int F_J0 = STAGE == 1 ? -1 : 0;         // row of fj = 0, relative to j0
+    static constexpr int F_NJ = STAGE == 1 ? TJ + 2 : TJ;
+    static constexpr int G_I0 = STAGE == 1 ? -1 : 0;         // column of gi = 0, relative to i0
+    static constexpr int G_NI = STAGE == 1 ? TI + 2 : TI;
+    static constexpr int G_NJ = TJ + 1;
+    static constexpr int EI_ = TI + 1, EJ_ = TJ + 1;
+    static constexpr int UF = UI * UJ;                       // doubles per staged field
+    static constexpr int PF = PI_ * PJ_;
+    static constexpr int RF = RI_ * RJ_;
+    static constexpr int SF = F_NI * F_NJ;
+    static constexpr int SG = G_NI * G_NJ;
+    static constexpr int NF = SF, NG = SG;                   // interfaces per sweep
+    static constexpr int U_DOUBLES = NFIELD * UF;
+    static constexpr int E_DOUBLES = UF;
+    static constexpr int P_DOUBLES = 7 * PF;
+    static constexpr int R_DOUBLES = 3 * RF;
+    static constexpr int F_DOUBLES = NC * SF;
+    static constexpr int G_DOUBLES = NC * SG;
+    static constexpr size_t SMEM_BYTES =
+        (size_t)(U_DOUBLES + E_DOUBLES + P_DOUBLES + R_DOUBLES + F_DOUBLES + G_DOUBLES) * 8 + 16;
+    static constexpr unsigned U_BYTES = (unsigned)(U_DOUBLES * 8);
+    static constexpr unsigned E_BYTES = (unsigned)(E_DOUBLES * 8);
+    static_assert(STAGE != 1 || EI_ * EJ_ <= R_DOUBLES, "corner EMF must fit in the eta*J region");
+    static_assert(STAGE_THREADS / 32 <= P_DOUBLES, "per-warp maxima must fit in the primitive region");
+    // Two CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA).
+    static_assert(SMEM_BYTES <= 113 * 1024, "shared memory for two CTAs per SM");
+};
 
 // primitive planes in Ps (rho and bZ are read from the staged tile)
 enum { P_U = 0, P_V, P_W, P_BXC, P_BYC, P_PX, P_PY };
 // eta*J planes in Rs
 enum { R_JX = 0, R_JY, R_JZ };
-
-// x-interfaces: stage 1 needs rows j0-1..j0+TJ (corner EMF), stage 2 only
-// the tile's rows; y-interfaces: stage 1 needs columns i0-1..i0+TI, stage 2
-// only the tile's columns.
-template <int STAGE> struct FluxRange;
-template <> struct FluxRange<1> {
-    static constexpr int f_j0 = 0, f_nj = FJ_, g_i0 = 0, g_ni = GI_;
-};
-template <> struct FluxRange<2> {
-    static constexpr int f_j0 = 1, f_nj = TJ, g_i0 = 1, g_ni = TI;
-};
+// flux component slots: 0..5 the hydro fields rho, rhoU, rhoV, rhoW, bZ, e;
+// slot 6 (stage 1) the EMF component F.f5 / G.f4.
+constexpr int SLOT_EMF = 6;
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
@@ -91,15 +98,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
 stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap emap,
              const StageArgs a)
 {
+    using T = Tile<STAGE>;
+    constexpr int TI = T::TI, UF = T::UF, PF = T::PF, RF = T::RF, SF = T::SF, SG = T::SG;
+    constexpr int PJ_ = T::PJ_, RJ_ = T::RJ_, F_NJ = T::F_NJ, G_NJ = T::G_NJ, EJ_ = T::EJ_;
     extern __shared__ __align__(1024) double smem[];
     double *Ut = smem;
-    double *Et = Ut + U_DOUBLES;
-    double *Ps = Et + E_DOUBLES;
-    double *Rs = Ps + P_DOUBLES;
+    double *Et = Ut + T::U_DOUBLES;
+    double *Ps = Et + T::E_DOUBLES;
+    double *Rs = Ps + T::P_DOUBLES;
     double *Ez = Rs;
-    double *Fs = Rs + R_DOUBLES;
-    double *Gs = Fs + F_DOUBLES;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(Gs + G_DOUBLES);
+    double *Fs = Rs + T::R_DOUBLES;
+    double *Gs = Fs + T::F_DOUBLES;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Gs + T::G_DOUBLES);
 
     const Grid &g = a.g;
     const int tid = threadIdx.x;
@@ -117,7 +127,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     __syncthreads();
     if (tid == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                     ::"r"(smem_addr(bar)), "r"(U_BYTES + (has_eta ? E_BYTES : 0u)) : "memory");
+                     ::"r"(smem_addr(bar)), "r"(T::U_BYTES + (has_eta ? T::E_BYTES : 0u)) : "memory");
         // x coordinate (j) = j0 - 3 = blockIdx.x * TJ: a multiple of TJ, so
         // 16-byte aligned in the global tensor as TMA requires.
         asm volatile(
@@ -247,80 +257,80 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
 
     // ---- HLLD fluxes (hlld.cu:110-233, muscl.cu:6-126, flux_solver.cu:10-33)
     // with the resistive terms ----
-    {
-        using FR = FluxRange<STAGE>;
-        constexpr int NF = FI_ * FR::f_nj, NG = FR::g_ni * GJ_;
-        for (int it = tid; it < NF + NG; it += STAGE_THREADS) {
-            const bool isF = it < NF;
-            int fi, fj;   // local flux index in Fs / Gs coordinates
-            if (isF) {
-                fi = it / FR::f_nj;
-                fj = FR::f_j0 + (it - fi * FR::f_nj);
-            } else {
-                const int t = it - NF;
-                fi = FR::g_i0 + t / GJ_;
-                fj = t - (t / GJ_) * GJ_;
-            }
-            // the cell left of / below the interface in each buffer
-            const double *uc = Ut + (fi + 2) * UJ + (fj + 2);
-            const double *pc = Ps + (fi + 1) * PJ_ + (fj + 1);
-            const int us = isF ? UJ : 1, ps = isF ? PJ_ : 1;
-            // sweep-frame components (the y sweep runs the x-sweep arithmetic
-            // on (rho, v, w, u, bY, bZ, bX, e), hlld.cu:134-152)
-            const double *cp[7] = {uc + RHO * UF,
-                                   pc + (isF ? P_U : P_V) * PF,
-                                   pc + (isF ? P_V : P_W) * PF,
-                                   pc + (isF ? P_W : P_U) * PF,
-                                   isF ? pc + P_BYC * PF : uc + BZF * UF,
-                                   isF ? uc + BZF * UF : pc + P_BXC * PF,
-                                   pc + (isF ? P_PX : P_PY) * PF};
-            const int cs[7] = {us, ps, ps, ps, isF ? ps : us, isF ? us : ps, ps};
-            double qL[7], qR[7];
+    for (int it = tid; it < T::NF + T::NG; it += STAGE_THREADS) {
+        const bool isF = it < T::NF;
+        int a0, a1;   // (fi, fj) or (gi, gj)
+        int ci, cj;   // the cell left of / below the interface, relative to (i0, j0)
+        if (isF) {
+            a0 = it / F_NJ;
+            a1 = it - a0 * F_NJ;
+            ci = a0 - 1;
+            cj = a1 + T::F_J0;
+        } else {
+            const int t = it - T::NF;
+            a0 = t / G_NJ;
+            a1 = t - a0 * G_NJ;
+            ci = a0 + T::G_I0;
+            cj = a1 - 1;
+        }
+        const double *uc = Ut + (ci + HALO) * UJ + (cj + HALO);
+        const double *pc = Ps + (ci + 2) * PJ_ + (cj + 2);
+        const double *r0 = Rs + (ci + 1) * RJ_ + (cj + 1);
+        const int us = isF ? UJ : 1, ps = isF ? PJ_ : 1;
+        // sweep-frame components (the y sweep runs the x-sweep arithmetic on
+        // (rho, v, w, u, bY, bZ, bX, e), hlld.cu:134-152)
+        const double *cp[7] = {uc + RHO * UF,
+                               pc + (isF ? P_U : P_V) * PF,
+                               pc + (isF ? P_V : P_W) * PF,
+                               pc + (isF ? P_W : P_U) * PF,
+                               isF ? pc + P_BYC * PF : uc + BZF * UF,
+                               isF ? uc + BZF * UF : pc + P_BXC * PF,
+                               pc + (isF ? P_PX : P_PY) * PF};
+        const int cs[7] = {us, ps, ps, ps, isF ? ps : us, isF ? us : ps, ps};
+        double qL[7], qR[7];
 #pragma unroll
-            for (int n = 0; n < 7; ++n) {
-                const double *q = cp[n];
-                const int st = cs[n];
-                const double qm = q[-st], q0 = q[0], qp = q[st], qpp = q[2 * st];
-                qL[n] = q0 + 0.5 * minmod(q0 - qm, qp - q0, EPS);
-                qR[n] = qp - 0.5 * minmod(qp - q0, qpp - qp, EPS);
-            }
-            const double *nb = pc + (isF ? P_BXC : P_BYC) * PF;
-            const double bn = 0.5 * (nb[0] + nb[ps]);
-            const Prim L{qL[0], qL[1], qL[2], qL[3], bn, qL[4], qL[5], qL[6]};
-            const Prim R{qR[0], qR[1], qR[2], qR[3], bn, qR[4], qR[5], qR[6]};
-            double f[8];
+        for (int n = 0; n < 7; ++n) {
+            const double *q = cp[n];
+            const int st = cs[n];
+            const double qm = q[-st], q0 = q[0], qp = q[st], qpp = q[2 * st];
+            qL[n] = q0 + 0.5 * minmod(q0 - qm, qp - q0, EPS);
+            qR[n] = qp - 0.5 * minmod(qp - q0, qpp - qp, EPS);
+        }
+        const double *nb = pc + (isF ? P_BXC : P_BYC) * PF;
+        const double bn = 0.5 * (nb[0] + nb[ps]);
+        const Prim L{qL[0], qL[1], qL[2], qL[3], bn, qL[4], qL[5], qL[6]};
+        const Prim R{qR[0], qR[1], qR[2], qR[3], bn, qR[4], qR[5], qR[6]};
+        double f[8];
 #if RMHD_FAST_MATH
-            hlld_flux_fast(L, R, gm, inv_gm1, EPS, f);
+        hlld_flux_fast(L, R, gm, inv_gm1, EPS, f);
 #else
-            hlld_flux<RMHD_ALL_CANDIDATES>(L, R, gm, EPS, f);
+        hlld_flux<RMHD_ALL_CANDIDATES>(L, R, gm, EPS, f);
 #endif
-            // eta*J of the two cells sharing the interface and their B
-            const double *r0 = Rs + fi * RJ_ + fj;
-            const int rs = isF ? RJ_ : 1;
-            const double z0 = uc[BZF * UF], z1 = uc[BZF * UF + us];
-            if (isF) {
-                const double eY0 = r0[R_JY * RF], eY1 = r0[R_JY * RF + rs];
-                const double eZ0 = r0[R_JZ * RF], eZ1 = r0[R_JZ * RF + rs];
-                const double y0 = pc[P_BYC * PF], y1 = pc[P_BYC * PF + ps];
-                const double f5 = f[5] - 0.5 * (eZ0 + eZ1);
-                const double f6 = f[6] + 0.5 * (eY0 + eY1);
-                const double f7 = f[7] + (0.5 * (eY0 * z0 + eY1 * z1) - 0.5 * (eZ0 * y0 + eZ1 * y1));
-                double *o = Fs + fi * FJ_ + fj;
-                o[0 * SF] = f[0]; o[1 * SF] = f[1]; o[2 * SF] = f[2]; o[3 * SF] = f[3];
-                o[4 * SF] = f5; o[5 * SF] = f6; o[6 * SF] = f7;
-            } else {
-                const double eX0 = r0[R_JX * RF], eX1 = r0[R_JX * RF + rs];
-                const double eZ0 = r0[R_JZ * RF], eZ1 = r0[R_JZ * RF + rs];
-                const double x0 = pc[P_BXC * PF], x1 = pc[P_BXC * PF + ps];
-                // un-permute (hlld.cu:170-194): g1 = f3, g2 = f1, g3 = f2,
-                // g4 = f6, g5 = f4 = 0, g6 = f5.
-                const double g4 = f[6] + 0.5 * (eZ0 + eZ1);
-                const double g6 = f[5] - 0.5 * (eX0 + eX1);
-                const double g7 = f[7] + (0.5 * (eZ0 * x0 + eZ1 * x1) - 0.5 * (eX0 * z0 + eX1 * z1));
-                double *o = Gs + fi * GJ_ + fj;
-                o[0 * SG] = f[0]; o[1 * SG] = f[3]; o[2 * SG] = f[1]; o[3 * SG] = f[2];
-                o[4 * SG] = g4; o[5 * SG] = g6; o[6 * SG] = g7;
-            }
+        // eta*J of the two cells sharing the interface and their B
+        const int rs = isF ? RJ_ : 1;
+        const double z0 = uc[BZF * UF], z1 = uc[BZF * UF + us];
+        if (isF) {
+            const double eY0 = r0[R_JY * RF], eY1 = r0[R_JY * RF + rs];
+            const double eZ0 = r0[R_JZ * RF], eZ1 = r0[R_JZ * RF + rs];
+            const double y0 = pc[P_BYC * PF], y1 = pc[P_BYC * PF + ps];
+            const double f6 = f[6] + 0.5 * (eY0 + eY1);
+            const double f7 = f[7] + (0.5 * (eY0 * z0 + eY1 * z1) - 0.5 * (eZ0 * y0 + eZ1 * y1));
+            double *o = Fs + a0 * F_NJ + a1;
+            o[0 * SF] = f[0]; o[1 * SF] = f[1]; o[2 * SF] = f[2]; o[3 * SF] = f[3];
+            o[4 * SF] = f6; o[5 * SF] = f7;
+            if (STAGE == 1) o[SLOT_EMF * SF] = f[5] - 0.5 * (eZ0 + eZ1);
+        } else {
+            const double eX0 = r0[R_JX * RF], eX1 = r0[R_JX * RF + rs];
+            const double eZ0 = r0[R_JZ * RF], eZ1 = r0[R_JZ * RF + rs];
+            const double x0 = pc[P_BXC * PF], x1 = pc[P_BXC * PF + ps];
+            // un-permute (hlld.cu:170-194): g1 = f3, g2 = f1, g3 = f2,
+            // g4 = f6, g5 = f4 = 0, g6 = f5.
+            const double g6 = f[5] - 0.5 * (eX0 + eX1);
+            const double g7 = f[7] + (0.5 * (eZ0 * x0 + eZ1 * x1) - 0.5 * (eX0 * z0 + eX1 * z1));
+            double *o = Gs + a0 * G_NJ + a1;
+            o[0 * SG] = f[0]; o[1 * SG] = f[3]; o[2 * SG] = f[1]; o[3 * SG] = f[2];
+            o[4 * SG] = g6; o[5 * SG] = g7;
+            if (STAGE == 1) o[SLOT_EMF * SG] = f[6] + 0.5 * (eZ0 + eZ1);
         }
     }
     __syncthreads();
@@ -328,36 +338,34 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     const double dtdx = dt / g.dx, dtdy = dt / g.dy;
 
     if (STAGE == 1) {
-        // ---- corner EMF (ct.cu:22-41) on (TI+1) x (TJ+1) corners ----
-        for (int c = tid; c < EI_ * EJ_; c += STAGE_THREADS) {
+        // ---- corner EMF (ct.cu:22-41) on (TI+1) x (TJ+1) corners (i, j) =
+        // (i0-1+ei, j0-1+ej), i.e. Fs (fi, fj) = (ei, ej) and Gs (gi, gj) = (ei, ej) ----
+        for (int c = tid; c < T::EI_ * EJ_; c += STAGE_THREADS) {
             const int ei = c / EJ_, ej = c - ei * EJ_;
-            const double eZG1 = Gs[4 * SG + ei * GJ_ + ej];
-            const double eZG2 = Gs[4 * SG + (ei + 1) * GJ_ + ej];
-            const double eZF1 = -1.0 * Fs[4 * SF + ei * FJ_ + ej];
-            const double eZF2 = -1.0 * Fs[4 * SF + ei * FJ_ + ej + 1];
+            const double eZG1 = Gs[SLOT_EMF * SG + ei * G_NJ + ej];
+            const double eZG2 = Gs[SLOT_EMF * SG + (ei + 1) * G_NJ + ej];
+            const double eZF1 = -1.0 * Fs[SLOT_EMF * SF + ei * F_NJ + ej];
+            const double eZF2 = -1.0 * Fs[SLOT_EMF * SF + ei * F_NJ + ej + 1];
             Ez[c] = 0.25 * (eZG1 + eZG2 + eZF1 + eZF2);
         }
         __syncthreads();
     }
 
     // ---- update of the tile's own cells ----
-    const double *fR = Fs + (li + 1) * FJ_ + (lj + 1);   // F(i)
-    const double *fL = fR - FJ_;                          // F(i-1)
-    const double *gU = Gs + (li + 1) * GJ_ + (lj + 1);   // G(j)
-    const double *gD = gU - 1;                            // G(j-1)
-    const double *uo = Ut + (li + HALO) * UJ + (lj + HALO);   // own cell in the staged tile
+    const double *fR = Fs + (li + 1) * F_NJ + (lj - T::F_J0);    // F(i)
+    const double *fL = fR - F_NJ;                                  // F(i-1)
+    const double *gU = Gs + (li - T::G_I0) * G_NJ + (lj + 1);    // G(j)
+    const double *gD = gU - 1;                                     // G(j-1)
+    const double *uo = Ut + (li + HALO) * UJ + (lj + HALO);        // own cell in the staged tile
     const int fld[6] = {RHO, MX, MY, MZ, BZF, EN};
-    const int slot[6] = {0, 1, 2, 3, 5, 6};
 
     if (STAGE == 1) {
         if (own) {
             // oneStepFirstFunctor (resistiveMHD_2D.cu:53-86)
 #pragma unroll
-            for (int n = 0; n < 6; ++n) {
-                const int s = slot[n];
-                a.dst[fld[n] * PL + k] = uo[fld[n] * UF] - dtdx * (fR[s * SF] - fL[s * SF])
-                                       - dtdy * (gU[s * SG] - gD[s * SG]);
-            }
+            for (int n = 0; n < 6; ++n)
+                a.dst[fld[n] * PL + k] = uo[fld[n] * UF] - dtdx * (fR[n * SF] - fL[n * SF])
+                                       - dtdy * (gU[n * SG] - gD[n * SG]);
             // CT_kernel (ct.cu:44-59) with the EMF of this stage
             const double *ez = Ez + (li + 1) * EJ_ + (lj + 1);
             a.dst[BXF * PL + k] = uo[BXF * UF] - dtdy * (ez[0] - ez[-1]);
@@ -376,10 +384,9 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         if (own) {
 #pragma unroll
             for (int n = 0; n < 6; ++n) {
-                const int s = slot[n];
                 const double u = a.un[fld[n] * PL + k];
                 const double ub = uo[fld[n] * UF];
-                nv[fld[n]] = 0.5 * (u + ub - dtdx * (fR[s * SF] - fL[s * SF]) - dtdy * (gU[s * SG] - gD[s * SG]));
+                nv[fld[n]] = 0.5 * (u + ub - dtdx * (fR[n * SF] - fL[n * SF]) - dtdy * (gU[n * SG] - gD[n * SG]));
             }
             nv[BXF] = uo[BXF * UF];
             nv[BYF] = uo[BYF * UF];
@@ -419,7 +426,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     }
 }
 
-size_t stage_smem_bytes() { return SMEM_BYTES; }
+size_t stage_smem_bytes(int stage) { return stage == 1 ? Tile<1>::SMEM_BYTES : Tile<2>::SMEM_BYTES; }
 
 int stage_regs(int stage)
 {
@@ -431,13 +438,17 @@ int stage_regs(int stage)
 void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream)
 {
-    cudaFuncSetAttribute(stage_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
-    cudaFuncSetAttribute(stage_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
-    const dim3 grid((args.g.ny - 2 * HALO + TJ - 1) / TJ, (args.g.nx - 2 * HALO + TI - 1) / TI);
-    if (stage == 1)
-        stage_kernel<1><<<grid, STAGE_THREADS, SMEM_BYTES, stream>>>(*tmap, *emap, args);
-    else
-        stage_kernel<2><<<grid, STAGE_THREADS, SMEM_BYTES, stream>>>(*tmap, *emap, args);
+    if (stage == 1) {
+        constexpr size_t sm = Tile<1>::SMEM_BYTES;
+        cudaFuncSetAttribute(stage_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        const dim3 grid((args.g.ny - 2 * HALO + TJ - 1) / TJ, (args.g.nx - 2 * HALO + Tile<1>::TI - 1) / Tile<1>::TI);
+        stage_kernel<1><<<grid, STAGE_THREADS, sm, stream>>>(*tmap, *emap, args);
+    } else {
+        constexpr size_t sm = Tile<2>::SMEM_BYTES;
+        cudaFuncSetAttribute(stage_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        const dim3 grid((args.g.ny - 2 * HALO + TJ - 1) / TJ, (args.g.nx - 2 * HALO + Tile<2>::TI - 1) / Tile<2>::TI);
+        stage_kernel<2><<<grid, STAGE_THREADS, sm, stream>>>(*tmap, *emap, args);
+    }
 }
 
 }  // namespace RMHD_VARIANT
