@@ -320,7 +320,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64_fast", "fp64_exact"], default="fp64_fast")
+    ap.add_argument("--precision", choices=["fp64_fast", "fp64_exact", "fp32_bulk"], default="fp64_fast")
     ap.add_argument("--workload", choices=["harris", "orszag_tang"], default="harris")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-baselines", dest="baselines", action="store_false")

@@ -56,7 +56,13 @@ typedef enum {
     RMHD2D_FP64_EXACT = 0,
     /* FP64 with fused multiply-add and only the selected HLLD candidate
        fluxes; differs from EXACT by rounding only. */
-    RMHD2D_FP64_FAST = 1
+    RMHD2D_FP64_FAST = 1,
+    /* FP32 bulk: MUSCL reconstruction, HLLD and eta*J fluxes in single
+       precision; pressure recovery from total energy, corner-EMF
+       accumulation, flux-difference update and dt reduction in FP64; state
+       stored in FP64.  No counterpart in the reference (its FP32 library
+       lib_ResistiveMHD_2D_GPU_single runs everything in float). */
+    RMHD2D_FP32_BULK = 2
 } rmhd2d_precision;
 
 typedef struct {

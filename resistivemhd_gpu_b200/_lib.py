@@ -18,7 +18,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no sm_100 device"
           5: "I/O error", 6: "kernel error"}
 
 BC = {"periodic": 0, "symmetric": 1}
-PRECISION = {"fp64_exact": 0, "exact": 0, "fp64_fast": 1, "fast": 1}
+PRECISION = {"fp64_exact": 0, "exact": 0, "fp64_fast": 1, "fast": 1, "fp32_bulk": 2, "bulk32": 2}
 
 
 class Config(ctypes.Structure):

@@ -6,7 +6,9 @@ Each translation unit is compiled by nvcc with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; the exact stage
 kernel, the boundary/CFL kernels and the host API are compiled with
 ``-fmad=false`` (no fused multiply-add, so they round as the reference's
-IEEE binary64 host build does), the fast stage kernel with FMA contraction.
+IEEE binary64 host build does), the fast stage kernel with FMA contraction,
+the FP32-bulk stage kernel with --use_fast_math (single-precision operations
+only; its FP64 parts round as in the fast kernel).
 The CUDA runtime is linked statically and the driver API is reached through
 cudaGetDriverEntryPoint, so the library loads on machines without a GPU.
 """
@@ -30,6 +32,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = {
     "stage_exact.cu": ["-fmad=false"],
     "stage_fast.cu": ["-fmad=true"],
+    "stage_bulk32.cu": ["-fmad=true", "--use_fast_math"],
     "aux_kernels.cu": ["-fmad=false"],
     "api.cu": ["-fmad=false"],
 }

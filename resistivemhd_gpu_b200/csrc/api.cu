@@ -146,6 +146,17 @@ int do_boundary(rmhd2d_solver *s)
     return RMHD2D_OK;
 }
 
+using StageLauncher = void (*)(int, const CUtensorMap *, const CUtensorMap *, const StageArgs &, cudaStream_t);
+
+StageLauncher stage_launcher(int precision)
+{
+    switch (precision) {
+    case RMHD2D_FP64_FAST: return fast::launch_stage;
+    case RMHD2D_FP32_BULK: return bulk32::launch_stage;
+    default: return exact::launch_stage;
+    }
+}
+
 void enqueue_step(rmhd2d_solver *s, int parity)
 {
     StageArgs a{};
@@ -154,7 +165,7 @@ void enqueue_step(rmhd2d_solver *s, int parity)
     a.row2 = s->g.bc == BC_SYMMETRIC ? s->row2 : nullptr;
     a.ctl = s->ctl;
     a.parity = parity;
-    auto launch = s->cfg.precision == RMHD2D_FP64_FAST ? fast::launch_stage : exact::launch_stage;
+    auto launch = stage_launcher(s->cfg.precision);
     // stage 1: U^n (A) -> U* (B)
     a.src = s->A;
     a.un = s->A;
@@ -244,7 +255,8 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
     if (!(cfg->eta >= 0.0)) return fail(s, RMHD2D_ERR_INVALID, "eta must be >= 0");
     if (cfg->bc != RMHD2D_BC_PERIODIC && cfg->bc != RMHD2D_BC_SYMMETRIC)
         return fail(s, RMHD2D_ERR_INVALID, "unknown boundary kind");
-    if (cfg->precision != RMHD2D_FP64_EXACT && cfg->precision != RMHD2D_FP64_FAST)
+    if (cfg->precision != RMHD2D_FP64_EXACT && cfg->precision != RMHD2D_FP64_FAST &&
+        cfg->precision != RMHD2D_FP32_BULK)
         return fail(s, RMHD2D_ERR_INVALID, "unknown precision");
 
     int ndev = 0;
@@ -475,7 +487,7 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
     a.row2 = s->g.bc == BC_SYMMETRIC ? s->row2 : nullptr;
     a.ctl = s->ctl;
     a.parity = parity;
-    auto launch = s->cfg.precision == RMHD2D_FP64_FAST ? fast::launch_stage : exact::launch_stage;
+    auto launch = stage_launcher(s->cfg.precision);
     CK(cudaEventRecord(ev[0], s->stream));
     a.src = s->A; a.un = s->A; a.dst = s->B;
     launch(1, &s->mapA, &s->mapE1, a, s->stream);

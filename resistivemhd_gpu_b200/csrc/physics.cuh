@@ -24,24 +24,47 @@ __host__ __device__ __forceinline__ double bits_to_double(unsigned long long b)
 }
 
 // thrust::min / thrust::max semantics ((b < a) ? b : a).
-__device__ __forceinline__ double tmin(double a, double b) { return (b < a) ? b : a; }
-__device__ __forceinline__ double tmax(double a, double b) { return (a < b) ? b : a; }
+template <typename T> __device__ __forceinline__ T tmin(T a, T b) { return (b < a) ? b : a; }
+template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return (a < b) ? b : a; }
 
 // hlld.cu:26-32 Sign, (x > 0) - (x < 0), as selects (no int conversion).
-__device__ __forceinline__ double sgn(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
+template <typename T> __device__ __forceinline__ T sgn(T x) { return x > T(0) ? T(1) : (x < T(0) ? T(-1) : T(0)); }
 
 // minmod.hpp:6-16: sign_x * max(min(|x|, sign_x * y), EPS) with an int
 // sign_x.  Written with selects: for x > 0 the reference computes
 // 1.0 * max(min(|x|, 1.0 * y), EPS), for x < 0 the negation of
 // max(min(|x|, -y), EPS), for x == 0 (or NaN) 0.0 * max(min(|x|, 0.0 * y), EPS);
 // multiplying by +-1 is exact, so this is bit-identical for every input.
-__device__ __forceinline__ double minmod(double x, double y, double eps)
+template <typename T> __device__ __forceinline__ T minmod(T x, T y, T eps)
 {
-    const double ax = fabs(x);
-    if (x > 0.0) return tmax(tmin(ax, y), eps);
-    if (x < 0.0) return -tmax(tmin(ax, -y), eps);
-    return 0.0 * tmax(tmin(ax, 0.0 * y), eps);
+    const T ax = fabs(x);
+    if (x > T(0)) return tmax(tmin(ax, y), eps);
+    if (x < T(0)) return -tmax(tmin(ax, -y), eps);
+    return T(0) * tmax(tmin(ax, T(0) * y), eps);
 }
+
+// Single-precision reciprocal and square roots of the FP32-bulk variant
+// (hardware approximations, ~1 ulp of float).
+__device__ __forceinline__ float rcp_nr(float a)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_t(float a)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ float sqrt_t(float a)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ double rsqrt_t(double a) { return rsqrt(a); }
+__device__ __forceinline__ double sqrt_t(double a) { return sqrt(a); }
 
 // Reciprocal by Newton-Raphson iteration on 1/a (x' = x + x (1 - a x), two
 // steps, each squaring the relative error) from the hardware seed
@@ -60,14 +83,15 @@ __device__ __forceinline__ double rcp_nr(double a)
 }
 
 // Interface state fed to HLLD: BasicParameter (basic_parameter_struct.hpp:5-27).
-struct Prim {
-    double rho, u, v, w, bX, bY, bZ, p;
+template <typename T> struct PrimT {
+    T rho, u, v, w, bX, bY, bZ, p;
 };
+using Prim = PrimT<double>;
 
 // hlld.cu:448-467 getOneFlux, accumulated into f (f4 is identically 0 and
 // is not produced).
-__device__ __forceinline__ void add_one_flux(double rho, double u, double v, double w, double bX,
-                                             double bY, double bZ, double e, double pT, double f[8])
+template <typename T>
+__device__ __forceinline__ void add_one_flux(T rho, T u, T v, T w, T bX, T bY, T bZ, T e, T pT, T f[8])
 {
     f[0] += rho * u;
     f[1] += rho * u * u + pT - bX * bX;
@@ -219,93 +243,93 @@ __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double g
 // of 28 divisions), squared sound/Alfven speeds used directly (the reference
 // squares their square roots), sqrt(rho*) and |bX|/sqrt(rho*) from one rsqrt,
 // and bX taken once (left and right states share the interface-normal B).
-__device__ __forceinline__ void hlld_flux_fast(const Prim &L, const Prim &R, double gm, double inv_gm1,
-                                               double EPS, double f[8])
+template <typename T>
+__device__ __forceinline__ void hlld_flux_fast(const PrimT<T> &L, const PrimT<T> &R, T gm, T inv_gm1, T EPS, T f[8])
 {
-    const double bX = L.bX;
-    const double bx2 = bX * bX;
-    const double iRL = rcp_nr(L.rho), iRR = rcp_nr(R.rho);
-    const double b2L = bx2 + L.bY * L.bY + L.bZ * L.bZ;
-    const double b2R = bx2 + R.bY * R.bY + R.bZ * R.bZ;
-    const double eL = L.p * inv_gm1 + 0.5 * L.rho * (L.u * L.u + L.v * L.v + L.w * L.w) + 0.5 * b2L;
-    const double eR = R.p * inv_gm1 + 0.5 * R.rho * (R.u * R.u + R.v * R.v + R.w * R.w) + 0.5 * b2R;
-    const double pTL = L.p + 0.5 * b2L, pTR = R.p + 0.5 * b2R;
+    const T bX = L.bX;
+    const T bx2 = bX * bX;
+    const T iRL = rcp_nr(L.rho), iRR = rcp_nr(R.rho);
+    const T b2L = bx2 + L.bY * L.bY + L.bZ * L.bZ;
+    const T b2R = bx2 + R.bY * R.bY + R.bZ * R.bZ;
+    const T eL = L.p * inv_gm1 + T(0.5) * L.rho * (L.u * L.u + L.v * L.v + L.w * L.w) + T(0.5) * b2L;
+    const T eR = R.p * inv_gm1 + T(0.5) * R.rho * (R.u * R.u + R.v * R.v + R.w * R.w) + T(0.5) * b2R;
+    const T pTL = L.p + T(0.5) * b2L, pTR = R.p + T(0.5) * b2R;
 
-    const double cs2L = gm * L.p * iRL, ca2L = b2L * iRL, va2L = bx2 * iRL;
-    const double cs2R = gm * R.p * iRR, ca2R = b2R * iRR, va2R = bx2 * iRR;
-    const double sL = cs2L + ca2L, sR = cs2R + ca2R;
+    const T cs2L = gm * L.p * iRL, ca2L = b2L * iRL, va2L = bx2 * iRL;
+    const T cs2R = gm * R.p * iRR, ca2R = b2R * iRR, va2R = bx2 * iRR;
+    const T sL = cs2L + ca2L, sR = cs2R + ca2R;
     // The reference takes sqrt of each squared speed, so a negative one makes
     // its fast speed NaN; keep that.
-    const double qnan = bits_to_double(0x7FF8000000000000ull);
-    const bool okL = (cs2L >= 0.0) & (ca2L >= 0.0) & (va2L >= 0.0);
-    const bool okR = (cs2R >= 0.0) & (ca2R >= 0.0) & (va2R >= 0.0);
-    const double cfL = okL ? sqrt(0.5 * (sL + sqrt(sL * sL - 4.0 * cs2L * va2L))) : qnan;
-    const double cfR = okR ? sqrt(0.5 * (sR + sqrt(sR * sR - 4.0 * cs2R * va2R))) : qnan;
+    const T qnan = T(bits_to_double(0x7FF8000000000000ull));
+    const bool okL = (cs2L >= T(0)) & (ca2L >= T(0)) & (va2L >= T(0));
+    const bool okR = (cs2R >= T(0)) & (ca2R >= T(0)) & (va2R >= T(0));
+    const T cfL = okL ? sqrt_t(T(0.5) * (sL + sqrt_t(sL * sL - T(4.0) * cs2L * va2L))) : qnan;
+    const T cfR = okR ? sqrt_t(T(0.5) * (sR + sqrt_t(sR * sR - T(4.0) * cs2R * va2R))) : qnan;
 
-    const double uL = L.u, uR = R.u;
-    double SL = tmin(uL, uR) - tmax(cfL, cfR);
-    double SR = tmax(uL, uR) + tmax(cfL, cfR);
-    SL = tmin(SL, 0.0);
-    SR = tmax(SR, 0.0);
+    const T uL = L.u, uR = R.u;
+    T SL = tmin(uL, uR) - tmax(cfL, cfR);
+    T SR = tmax(uL, uR) + tmax(cfL, cfR);
+    SL = tmin(SL, T(0));
+    SR = tmax(SR, T(0));
 
-    const double dSL = SL - uL, dSR = SR - uR;
-    const double rdSL = L.rho * dSL, rdSR = R.rho * dSR;
-    const double iden = rcp_nr(rdSR - rdSL + EPS);
-    const double SM = (rdSR * uR - rdSL * uL - pTR + pTL) * iden;
-    const double pT1 = (rdSR * pTL - rdSL * pTR + rdSL * rdSR * (uR - uL)) * iden;
+    const T dSL = SL - uL, dSR = SR - uR;
+    const T rdSL = L.rho * dSL, rdSR = R.rho * dSR;
+    const T iden = rcp_nr(rdSR - rdSL + EPS);
+    const T SM = (rdSR * uR - rdSL * uL - pTR + pTL) * iden;
+    const T pT1 = (rdSR * pTL - rdSL * pTR + rdSL * rdSR * (uR - uL)) * iden;
 
-    const double iSLM = rcp_nr(SL - SM + EPS), iSRM = rcp_nr(SR - SM + EPS);
-    const double rho1L = rdSL * iSLM, rho1R = rdSR * iSRM;
-    const double id1L = rcp_nr(rdSL * (SL - SM) - bx2 + EPS);
-    const double id1R = rcp_nr(rdSR * (SR - SM) - bx2 + EPS);
-    const double tL = bX * (SM - uL) * id1L, tR = bX * (SM - uR) * id1R;
-    const double v1L = L.v - L.bY * tL, w1L = L.w - L.bZ * tL;
-    const double v1R = R.v - R.bY * tR, w1R = R.w - R.bZ * tR;
-    const double gL = (rdSL * dSL - bx2) * id1L, gR = (rdSR * dSR - bx2) * id1R;
-    const double bY1L = L.bY * gL, bZ1L = L.bZ * gL;
-    const double bY1R = R.bY * gR, bZ1R = R.bZ * gR;
-    const double vbL = uL * bX + L.v * L.bY + L.w * L.bZ, vbR = uR * bX + R.v * R.bY + R.w * R.bZ;
-    const double vb1L = SM * bX + v1L * bY1L + w1L * bZ1L, vb1R = SM * bX + v1R * bY1R + w1R * bZ1R;
-    const double e1L = (dSL * eL - pTL * uL + pT1 * SM + bX * (vbL - vb1L)) * iSLM;
-    const double e1R = (dSR * eR - pTR * uR + pT1 * SM + bX * (vbR - vb1R)) * iSRM;
+    const T iSLM = rcp_nr(SL - SM + EPS), iSRM = rcp_nr(SR - SM + EPS);
+    const T rho1L = rdSL * iSLM, rho1R = rdSR * iSRM;
+    const T id1L = rcp_nr(rdSL * (SL - SM) - bx2 + EPS);
+    const T id1R = rcp_nr(rdSR * (SR - SM) - bx2 + EPS);
+    const T tL = bX * (SM - uL) * id1L, tR = bX * (SM - uR) * id1R;
+    const T v1L = L.v - L.bY * tL, w1L = L.w - L.bZ * tL;
+    const T v1R = R.v - R.bY * tR, w1R = R.w - R.bZ * tR;
+    const T gL = (rdSL * dSL - bx2) * id1L, gR = (rdSR * dSR - bx2) * id1R;
+    const T bY1L = L.bY * gL, bZ1L = L.bZ * gL;
+    const T bY1R = R.bY * gR, bZ1R = R.bZ * gR;
+    const T vbL = uL * bX + L.v * L.bY + L.w * L.bZ, vbR = uR * bX + R.v * R.bY + R.w * R.bZ;
+    const T vb1L = SM * bX + v1L * bY1L + w1L * bZ1L, vb1R = SM * bX + v1R * bY1R + w1R * bZ1R;
+    const T e1L = (dSL * eL - pTL * uL + pT1 * SM + bX * (vbL - vb1L)) * iSLM;
+    const T e1R = (dSR * eR - pTR * uR + pT1 * SM + bX * (vbR - vb1R)) * iSRM;
 
-    const double rsL = rsqrt(rho1L), rsR = rsqrt(rho1R);
-    const double sqL = rho1L * rsL, sqR = rho1R * rsR;
-    const double abx = fabs(bX);
-    const double S1L = SM - abx * rsL, S1R = SM + abx * rsR;
-    const double sb = sgn(bX);
-    const double id2 = rcp_nr(sqL + sqR + EPS);
-    const double sqLR = sqL * sqR;
-    const double v2 = (sqL * v1L + sqR * v1R + (bY1R - bY1L) * sb) * id2;
-    const double w2 = (sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sb) * id2;
-    const double bY2 = (sqL * bY1R + sqR * bY1L + sqLR * (v1R - v1L) * sb) * id2;
-    const double bZ2 = (sqL * bZ1R + sqR * bZ1L + sqLR * (w1R - w1L) * sb) * id2;
-    const double vb2 = SM * bX + v2 * bY2 + w2 * bZ2;
-    const double e2L = e1L - sqL * (vb1L - vb2) * sb;
-    const double e2R = e1R + sqR * (vb1R - vb2) * sb;
+    const T rsL = rsqrt_t(rho1L), rsR = rsqrt_t(rho1R);
+    const T sqL = rho1L * rsL, sqR = rho1R * rsR;
+    const T abx = fabs(bX);
+    const T S1L = SM - abx * rsL, S1R = SM + abx * rsR;
+    const T sb = sgn(bX);
+    const T id2 = rcp_nr(sqL + sqR + EPS);
+    const T sqLR = sqL * sqR;
+    const T v2 = (sqL * v1L + sqR * v1R + (bY1R - bY1L) * sb) * id2;
+    const T w2 = (sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sb) * id2;
+    const T bY2 = (sqL * bY1R + sqR * bY1L + sqLR * (v1R - v1L) * sb) * id2;
+    const T bZ2 = (sqL * bZ1R + sqR * bZ1L + sqLR * (w1R - w1L) * sb) * id2;
+    const T vb2 = SM * bX + v2 * bY2 + w2 * bZ2;
+    const T e2L = e1L - sqL * (vb1L - vb2) * sb;
+    const T e2R = e1R + sqR * (vb1R - vb2) * sb;
 
-    const bool bOL = SL > 0.0;
-    const bool bML = (SL <= 0.0) && (0.0 < S1L);
-    const bool bIL = (S1L <= 0.0) && (0.0 < SM);
-    const bool bOR = SR <= 0.0;
-    const bool bMR = (S1R <= 0.0) && (0.0 < SR);
-    const bool bIR = (SM <= 0.0) && (0.0 < S1R);
+    const bool bOL = SL > T(0);
+    const bool bML = (SL <= T(0)) && (T(0) < S1L);
+    const bool bIL = (S1L <= T(0)) && (T(0) < SM);
+    const bool bOR = SR <= T(0);
+    const bool bMR = (S1R <= T(0)) && (T(0) < SR);
+    const bool bIR = (SM <= T(0)) && (T(0) < S1R);
 #pragma unroll
-    for (int n = 0; n < 8; ++n) f[n] = 0.0;
+    for (int n = 0; n < 8; ++n) f[n] = T(0);
     const int nsel = (int)bOL + (int)bML + (int)bIL + (int)bOR + (int)bMR + (int)bIR;
     if (nsel == 1) {
         // The usual case: one region is selected; pick its state with
         // selects and form one flux (no per-candidate divergence in a warp).
         const bool lft = bOL | bML | bIL;
         const bool outer = bOL | bOR, inner = bIL | bIR;
-        const double rho = bOL ? L.rho : (bOR ? R.rho : (lft ? rho1L : rho1R));
-        const double u = bOL ? uL : (bOR ? uR : SM);
-        const double v = outer ? (bOL ? L.v : R.v) : (inner ? v2 : (bML ? v1L : v1R));
-        const double w = outer ? (bOL ? L.w : R.w) : (inner ? w2 : (bML ? w1L : w1R));
-        const double by = outer ? (bOL ? L.bY : R.bY) : (inner ? bY2 : (bML ? bY1L : bY1R));
-        const double bz = outer ? (bOL ? L.bZ : R.bZ) : (inner ? bZ2 : (bML ? bZ1L : bZ1R));
-        const double e = bOL ? eL : (bOR ? eR : (bML ? e1L : (bIL ? e2L : (bMR ? e1R : e2R))));
-        const double pT = bOL ? pTL : (bOR ? pTR : pT1);
+        const T rho = bOL ? L.rho : (bOR ? R.rho : (lft ? rho1L : rho1R));
+        const T u = bOL ? uL : (bOR ? uR : SM);
+        const T v = outer ? (bOL ? L.v : R.v) : (inner ? v2 : (bML ? v1L : v1R));
+        const T w = outer ? (bOL ? L.w : R.w) : (inner ? w2 : (bML ? w1L : w1R));
+        const T by = outer ? (bOL ? L.bY : R.bY) : (inner ? bY2 : (bML ? bY1L : bY1R));
+        const T bz = outer ? (bOL ? L.bZ : R.bZ) : (inner ? bZ2 : (bML ? bZ1L : bZ1R));
+        const T e = bOL ? eL : (bOR ? eR : (bML ? e1L : (bIL ? e2L : (bMR ? e1R : e2R))));
+        const T pT = bOL ? pTL : (bOR ? pTR : pT1);
         add_one_flux(rho, u, v, w, bX, by, bz, e, pT, f);
     } else {
         if (bOL) add_one_flux(L.rho, uL, L.v, L.w, bX, L.bY, L.bZ, eL, pTL, f);
@@ -320,6 +344,143 @@ __device__ __forceinline__ void hlld_flux_fast(const Prim &L, const Prim &R, dou
     if ((SL != SL) | (SR != SR) | (SM != SM) | (S1L != S1L) | (S1R != S1R)) {
 #pragma unroll
         for (int n = 0; n < 8; ++n) f[n] = qnan;
+    }
+}
+
+// Inputs of the FP32-bulk HLLD flux at one interface: the reconstructed
+// left/right states in single precision for the wave speeds and star states,
+// plus FP64 copies of the components that carry the large, balanced stresses
+// (pressure, tangential B, normal B).
+struct BulkStates {
+    float rhoL, uL, vL, wL, rhoR, uR, vR, wR;
+    double pL, pR, bYL, bYR, bZL, bZR, bn;
+};
+
+// HLLD flux of the FP32-bulk variant: the wave-speed estimates, star and
+// double-star states and candidate selection of hlld.cu:256-565 in single
+// precision, with the total pressure and the tangential B of every candidate
+// state carried as an FP64 value plus a single-precision correction:
+//   pT*  = pT_L + rdSL (pT_L - pT_R + rdSR (uR - uL)) / (rdSR - rdSL)
+//   bY*L = bY_L + bY_L rdSL (SM - uL) / den*L        (and bZ, and R)
+//   bY** = bY*L + (sqL (bY*R - bY*L) + sqLR (v*R - v*L) sgn bX) / (sqL + sqR)
+// (algebraically the reference's formulas), so the momentum flux
+// rho u^2 + pT - bX^2, rho u v - bX bY, rho u w - bX bZ is assembled in FP64
+// and pressure- or tension-balanced states keep their FP64 balance.  The
+// other flux components (mass, induction, energy) stay single precision.
+// fm[0..2]: the three momentum components (f1, f2, f3) in FP64;
+// fo[0]: f0, fo[1]: f5, fo[2]: f6, fo[3]: f7 in FP32.
+__device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, float inv_gm1, float EPS,
+                                               double fm[3], float fo[4])
+{
+    const double bn64 = s.bn;
+    const float bX = (float)bn64, bx2 = bX * bX;
+    const double b2L64 = bn64 * bn64 + s.bYL * s.bYL + s.bZL * s.bZL;
+    const double b2R64 = bn64 * bn64 + s.bYR * s.bYR + s.bZR * s.bZR;
+    const double pTL64 = s.pL + 0.5 * b2L64, pTR64 = s.pR + 0.5 * b2R64;
+    const float dpT = (float)(pTL64 - pTR64);
+    const float pL = (float)s.pL, pR = (float)s.pR;
+    const float bYL = (float)s.bYL, bYR = (float)s.bYR, bZL = (float)s.bZL, bZR = (float)s.bZR;
+    const float b2L = (float)b2L64, b2R = (float)b2R64, pTL = (float)pTL64, pTR = (float)pTR64;
+    const float rhoL = s.rhoL, rhoR = s.rhoR, uL = s.uL, uR = s.uR, vL = s.vL, vR = s.vR, wL = s.wL, wR = s.wR;
+
+    const float iRL = rcp_nr(rhoL), iRR = rcp_nr(rhoR);
+    const float eL = pL * inv_gm1 + 0.5f * rhoL * (uL * uL + vL * vL + wL * wL) + 0.5f * b2L;
+    const float eR = pR * inv_gm1 + 0.5f * rhoR * (uR * uR + vR * vR + wR * wR) + 0.5f * b2R;
+    const float cs2L = gm * pL * iRL, ca2L = b2L * iRL, va2L = bx2 * iRL;
+    const float cs2R = gm * pR * iRR, ca2R = b2R * iRR, va2R = bx2 * iRR;
+    const float sL = cs2L + ca2L, sR = cs2R + ca2R;
+    const float qnan = __int_as_float(0x7fc00000);
+    const bool okL = (cs2L >= 0.f) & (ca2L >= 0.f) & (va2L >= 0.f);
+    const bool okR = (cs2R >= 0.f) & (ca2R >= 0.f) & (va2R >= 0.f);
+    const float cfL = okL ? sqrt_t(0.5f * (sL + sqrt_t(sL * sL - 4.f * cs2L * va2L))) : qnan;
+    const float cfR = okR ? sqrt_t(0.5f * (sR + sqrt_t(sR * sR - 4.f * cs2R * va2R))) : qnan;
+
+    float SL = tmin(uL, uR) - tmax(cfL, cfR);
+    float SR = tmax(uL, uR) + tmax(cfL, cfR);
+    SL = tmin(SL, 0.f);
+    SR = tmax(SR, 0.f);
+
+    const float dSL = SL - uL, dSR = SR - uR;
+    const float rdSL = rhoL * dSL, rdSR = rhoR * dSR;
+    const float iden = rcp_nr(rdSR - rdSL + EPS);
+    const float SM = (rdSR * uR - rdSL * uL + dpT) * iden;
+    const float cpT1 = rdSL * (dpT + rdSR * (uR - uL)) * iden;      // pT* - pT_L
+    const double pT1_64 = pTL64 + (double)cpT1;
+    const float pT1 = pTL + cpT1;
+
+    const float iSLM = rcp_nr(SL - SM + EPS), iSRM = rcp_nr(SR - SM + EPS);
+    const float rho1L = rdSL * iSLM, rho1R = rdSR * iSRM;
+    const float id1L = rcp_nr(rdSL * (SL - SM) - bx2 + EPS);
+    const float id1R = rcp_nr(rdSR * (SR - SM) - bx2 + EPS);
+    const float tL = bX * (SM - uL) * id1L, tR = bX * (SM - uR) * id1R;
+    const float v1L = vL - bYL * tL, w1L = wL - bZL * tL;
+    const float v1R = vR - bYR * tR, w1R = wR - bZR * tR;
+    const float gcL = rdSL * (SM - uL) * id1L, gcR = rdSR * (SM - uR) * id1R;   // bY*/bY - 1
+    const float cYL = bYL * gcL, cZL = bZL * gcL, cYR = bYR * gcR, cZR = bZR * gcR;
+    const float bY1L = bYL + cYL, bZ1L = bZL + cZL, bY1R = bYR + cYR, bZ1R = bZR + cZR;
+    const float vbL = uL * bX + vL * bYL + wL * bZL, vbR = uR * bX + vR * bYR + wR * bZR;
+    const float vb1L = SM * bX + v1L * bY1L + w1L * bZ1L, vb1R = SM * bX + v1R * bY1R + w1R * bZ1R;
+    const float e1L = (dSL * eL - pTL * uL + pT1 * SM + bX * (vbL - vb1L)) * iSLM;
+    const float e1R = (dSR * eR - pTR * uR + pT1 * SM + bX * (vbR - vb1R)) * iSRM;
+
+    const float rsL = rsqrt_t(rho1L), rsR = rsqrt_t(rho1R);
+    const float sqL = rho1L * rsL, sqR = rho1R * rsR;
+    const float abx = fabsf(bX);
+    const float S1L = SM - abx * rsL, S1R = SM + abx * rsR;
+    const float sb = sgn(bX);
+    const float id2 = rcp_nr(sqL + sqR + EPS);
+    const float sqLR = sqL * sqR;
+    const float dBY = (float)(s.bYR - s.bYL) + (cYR - cYL);             // bY*R - bY*L
+    const float dBZ = (float)(s.bZR - s.bZL) + (cZR - cZL);
+    const float c2Y = (sqL * dBY + sqLR * (v1R - v1L) * sb) * id2;      // bY** - bY*L
+    const float c2Z = (sqL * dBZ + sqLR * (w1R - w1L) * sb) * id2;
+    const float v2 = (sqL * v1L + sqR * v1R + (bY1R - bY1L) * sb) * id2;
+    const float w2 = (sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sb) * id2;
+    const float bY2 = bY1L + c2Y, bZ2 = bZ1L + c2Z;
+    const float vb2 = SM * bX + v2 * bY2 + w2 * bZ2;
+    const float e2L = e1L - sqL * (vb1L - vb2) * sb;
+    const float e2R = e1R + sqR * (vb1R - vb2) * sb;
+
+    const bool ind[6] = {SL > 0.f, (SL <= 0.f) && (0.f < S1L), (S1L <= 0.f) && (0.f < SM), SR <= 0.f,
+                         (S1R <= 0.f) && (0.f < SR), (SM <= 0.f) && (0.f < S1R)};
+    fm[0] = fm[1] = fm[2] = 0.0;
+    fo[0] = fo[1] = fo[2] = fo[3] = 0.f;
+    // candidate r: 0 outer L, 1 middle L, 2 inner L, 3 outer R, 4 middle R, 5 inner R
+    auto add = [&](int r) {
+        const bool lft = r < 3;
+        const float rho = r == 0 ? rhoL : (r == 3 ? rhoR : (lft ? rho1L : rho1R));
+        const float u = r == 0 ? uL : (r == 3 ? uR : SM);
+        const float v = r == 0 ? vL : r == 3 ? vR : r == 1 ? v1L : r == 4 ? v1R : v2;
+        const float w = r == 0 ? wL : r == 3 ? wR : r == 1 ? w1L : r == 4 ? w1R : w2;
+        const float e = r == 0 ? eL : r == 3 ? eR : r == 1 ? e1L : r == 4 ? e1R : (r == 2 ? e2L : e2R);
+        // FP64 total pressure and tangential B of the candidate
+        const double pT = r == 0 ? pTL64 : (r == 3 ? pTR64 : pT1_64);
+        const double by = r == 0 ? s.bYL : r == 3 ? s.bYR : r == 1 ? s.bYL + (double)cYL
+                        : r == 4 ? s.bYR + (double)cYR : s.bYL + (double)(cYL + c2Y);
+        const double bz = r == 0 ? s.bZL : r == 3 ? s.bZR : r == 1 ? s.bZL + (double)cZL
+                        : r == 4 ? s.bZR + (double)cZR : s.bZL + (double)(cZL + c2Z);
+        const float by32 = (float)by, bz32 = (float)bz, pT32 = (float)pT;
+        const float ru = rho * u;
+        fm[0] += (double)(ru * u) + pT - bn64 * bn64;
+        fm[1] += (double)(ru * v) - bn64 * by;
+        fm[2] += (double)(ru * w) - bn64 * bz;
+        fo[0] += ru;
+        fo[1] += u * by32 - v * bX;
+        fo[2] += u * bz32 - w * bX;
+        fo[3] += (e + pT32) * u - bX * (bX * u + by32 * v + bz32 * w);
+    };
+    const int nsel = (int)ind[0] + (int)ind[1] + (int)ind[2] + (int)ind[3] + (int)ind[4] + (int)ind[5];
+    if (nsel == 1) {
+        const int r = ind[0] ? 0 : ind[1] ? 1 : ind[2] ? 2 : ind[3] ? 3 : ind[4] ? 4 : 5;
+        add(r);
+    } else {
+        for (int r = 0; r < 6; ++r)
+            if (ind[r]) add(r);
+    }
+    if ((SL != SL) | (SR != SR) | (SM != SM) | (S1L != S1L) | (S1R != S1R)) {
+        const double dn = bits_to_double(0x7FF8000000000000ull);
+        fm[0] = fm[1] = fm[2] = dn;
+        fo[0] = fo[1] = fo[2] = fo[3] = qnan;
     }
 }
 

@@ -15,10 +15,12 @@
 // eta table on the same cells; everything after those loads reads shared
 // memory, except stage 2's read of U^n at its own cells.
 //
-// This header is compiled twice: into an "exact" variant (-fmad=false, all
+// The kernel is compiled three times: an "exact" variant (-fmad=false, all
 // six HLLD candidate fluxes formed), bit-identical to the reference
-// evaluated in IEEE binary64, and a "fast" variant (FMA contraction, only
-// the selected HLLD candidates).
+// evaluated in IEEE binary64; a "fast" FP64 variant (FMA contraction, shared
+// reciprocals, only the selected HLLD candidate); and an "FP32-bulk" variant
+// (reconstruction and fluxes in single precision, pressure recovery, EMF,
+// update and dt in FP64).
 #pragma once
 
 #include <cuda.h>
@@ -54,5 +56,11 @@ void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, c
 size_t stage_smem_bytes(int stage);
 int stage_regs(int stage);
 }  // namespace fast
+namespace bulk32 {
+void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
+                  cudaStream_t stream);
+size_t stage_smem_bytes(int stage);
+int stage_regs(int stage);
+}  // namespace bulk32
 
 }  // namespace rmhd2d

@@ -9,6 +9,14 @@
 #define RMHD_FAST_MATH 0
 #endif
 
+#ifndef RMHD_BULK
+#define RMHD_BULK 0
+#endif
+
+#ifndef RMHD_REAL
+#define RMHD_REAL double
+#endif
+
 #ifndef RMHD_VARIANT
 #error "define RMHD_VARIANT (exact or fast) before including stage_impl.cuh"
 #endif
@@ -16,22 +24,24 @@
 namespace rmhd2d {
 namespace RMHD_VARIANT {
 
-// ---- per-stage tile geometry and shared-memory carve-up (doubles) ----
-// Ut [8][UI][UJ]        TMA: U at i0-3..i0+TI+2, j0-3..j0+TJ+2 (kept for the whole CTA)
-// Et [UI][UJ]           TMA: eta table on the same cells (when a table is set)
-// Ps [7][TI+4][TJ+4]    u, v, w, centred bX, centred bY, x- and y-sweep pressures
-// Rs [3][TI+2][TJ+2]    eta*Jx, eta*Jy, eta*Jz per cell; reused for the corner EMF
-// Fs [NC][TI+1][F_NJ]   x fluxes f0 f1 f2 f3 f6 f7 (+ f5 in stage 1) at i+1/2
-// Gs [NC][G_NI][TJ+1]   y fluxes g0 g1 g2 g3 g6 g7 (+ g4 in stage 1) at j+1/2
+// ---- per-stage tile geometry and shared-memory carve-up ----
+// Ut [8][UI][UJ] f64     TMA: U at i0-3..i0+TI+2, j0-3..j0+TJ+2 (kept for the whole CTA)
+// Et [UI][UJ] f64        TMA: eta table on the same cells (when a table is set)
+// Pv [3][TI+4][TJ+4]     u, v, w (flux-side type)
+// Pb [4][TI+4][TJ+4] f64 centred bX, centred bY, x- and y-sweep pressures
+// Rs [3][TI+2][TJ+2]     eta*Jx, eta*Jy, eta*Jz (flux-side type); reused for the corner EMF (f64)
+// Fm [3][TI+1][F_NJ] f64 x fluxes of rhoU, rhoV, rhoW at i+1/2
+// Fo [NO][TI+1][F_NJ]    x fluxes of rho, bZ, e (+ bY = EMF part, stage 1), flux-side type
+// Gm, Go                 the same for the y fluxes at j+1/2 (Go slot 3: the bX flux)
 // Stage 1 needs x fluxes on rows j0-1..j0+TJ and y fluxes on columns
-// i0-1..i0+TI for its corner EMF; stage 2 only the tile's own interfaces and
-// no EMF components.
+// i0-1..i0+TI for its corner EMF; stage 2 only the tile's own interfaces.
 template <int STAGE> struct Tile {
+    using Real = RMHD_REAL;                                  // flux-side arithmetic type
     static constexpr int TI = stage_ti(STAGE);
     static constexpr int UI = TI + 2 * HALO;
     static constexpr int PI_ = TI + 4, PJ_ = TJ + 4;
     static constexpr int RI_ = TI + 2, RJ_ = TJ + 2;
-    static constexpr int NC = STAGE == 1 ? 7 : 6;            // flux components stored
+    static constexpr int NO = STAGE == 1 ? 4 : 3;            // non-momentum flux components stored
     static constexpr int F_NI = TI + 1;
     static constexpr int F_J0 = STAGE == 1 ? -1 : 0;         // row of fj = 0, relative to j0
     static constexpr int F_NJ = STAGE == 1 ? TJ + 2 : TJ;
@@ -45,29 +55,56 @@ template <int STAGE> struct Tile {
     static constexpr int SF = F_NI * F_NJ;
     static constexpr int SG = G_NI * G_NJ;
     static constexpr int NF = SF, NG = SG;                   // interfaces per sweep
-    static constexpr int U_DOUBLES = NFIELD * UF;
-    static constexpr int E_DOUBLES = UF;
-    static constexpr int P_DOUBLES = 7 * PF;
-    static constexpr int R_DOUBLES = 3 * RF;
-    static constexpr int F_DOUBLES = NC * SF;
-    static constexpr int G_DOUBLES = NC * SG;
-    static constexpr size_t SMEM_BYTES =
-        (size_t)(U_DOUBLES + E_DOUBLES + P_DOUBLES + R_DOUBLES + F_DOUBLES + G_DOUBLES) * 8 + 16;
-    static constexpr unsigned U_BYTES = (unsigned)(U_DOUBLES * 8);
-    static constexpr unsigned E_BYTES = (unsigned)(E_DOUBLES * 8);
-    static_assert(STAGE != 1 || EI_ * EJ_ <= R_DOUBLES, "corner EMF must fit in the eta*J region");
-    static_assert(STAGE_THREADS / 32 <= P_DOUBLES, "per-warp maxima must fit in the primitive region");
+    static constexpr size_t up16(size_t b) { return (b + 15) / 16 * 16; }
+    static constexpr size_t U_BYTES_ = (size_t)NFIELD * UF * 8;
+    static constexpr size_t E_BYTES_ = (size_t)UF * 8;
+    static constexpr size_t PV_BYTES = up16((size_t)3 * PF * sizeof(Real));
+    static constexpr size_t PB_BYTES = up16((size_t)4 * PF * 8);
+    static constexpr size_t R_ETA = (size_t)3 * RF * sizeof(Real);
+    static constexpr size_t R_EMF = STAGE == 1 ? (size_t)EI_ * EJ_ * 8 : 0;
+    static constexpr size_t R_BYTES = up16(R_ETA > R_EMF ? R_ETA : R_EMF);
+    static constexpr size_t FM_BYTES = up16((size_t)3 * SF * 8);
+    static constexpr size_t FO_BYTES = up16((size_t)NO * SF * sizeof(Real));
+    static constexpr size_t GM_BYTES = up16((size_t)3 * SG * 8);
+    static constexpr size_t GO_BYTES = up16((size_t)NO * SG * sizeof(Real));
+    static constexpr size_t OFF_E = U_BYTES_;
+    static constexpr size_t OFF_PV = OFF_E + E_BYTES_;
+    static constexpr size_t OFF_PB = OFF_PV + PV_BYTES;
+    static constexpr size_t OFF_R = OFF_PB + PB_BYTES;
+    static constexpr size_t OFF_FM = OFF_R + R_BYTES;
+    static constexpr size_t OFF_FO = OFF_FM + FM_BYTES;
+    static constexpr size_t OFF_GM = OFF_FO + FO_BYTES;
+    static constexpr size_t OFF_GO = OFF_GM + GM_BYTES;
+    static constexpr size_t OFF_BAR = OFF_GO + GO_BYTES;
+    static constexpr size_t SMEM_BYTES = OFF_BAR + 16;
+    static constexpr unsigned U_BYTES = (unsigned)U_BYTES_;
+    static constexpr unsigned E_BYTES = (unsigned)E_BYTES_;
+    static_assert(STAGE_THREADS / 32 * 8 <= PB_BYTES, "per-warp maxima must fit in the primitive region");
     // Two CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA).
     static_assert(SMEM_BYTES <= 113 * 1024, "shared memory for two CTAs per SM");
 };
 
-// primitive planes in Ps (rho and bZ are read from the staged tile)
-enum { P_U = 0, P_V, P_W, P_BXC, P_BYC, P_PX, P_PY };
+// velocity planes (Pv) and B / pressure planes (Pb); rho and bZ are read from
+// the staged tile
+enum { V_U = 0, V_V, V_W };
+enum { B_XC = 0, B_YC, B_PX, B_PY };
 // eta*J planes in Rs
 enum { R_JX = 0, R_JY, R_JZ };
-// flux component slots: 0..5 the hydro fields rho, rhoU, rhoV, rhoW, bZ, e;
-// slot 6 (stage 1) the EMF component F.f5 / G.f4.
-constexpr int SLOT_EMF = 6;
+// non-momentum flux slots (Fo / Go): rho, bZ, e, and in stage 1 the EMF
+// component (F: bY flux f5, G: bX flux g4)
+enum { O_RHO = 0, O_BZ = 1, O_EN = 2, O_EMF = 3 };
+
+// FP64 value + single-precision limited slope (MUSCL, muscl.cu:6-126): the
+// differences are taken in FP64, the minmod in single precision.
+__device__ __forceinline__ void muscl_dev(double qm, double q0, double qp, double qpp, float eps, double &qL,
+                                          double &qR)
+{
+    const double d0 = q0 - qm, d1 = qp - q0, d2 = qpp - qp;
+    const float mL = minmod((float)d0, (float)d1, eps);
+    const float mR = minmod((float)d1, (float)d2, eps);
+    qL = q0 + (double)(0.5f * mL);
+    qR = qp - (double)(0.5f * mR);
+}
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
@@ -99,17 +136,21 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
              const StageArgs a)
 {
     using T = Tile<STAGE>;
+    using Real = typename T::Real;
     constexpr int TI = T::TI, UF = T::UF, PF = T::PF, RF = T::RF, SF = T::SF, SG = T::SG;
     constexpr int PJ_ = T::PJ_, RJ_ = T::RJ_, F_NJ = T::F_NJ, G_NJ = T::G_NJ, EJ_ = T::EJ_;
-    extern __shared__ __align__(1024) double smem[];
-    double *Ut = smem;
-    double *Et = Ut + T::U_DOUBLES;
-    double *Ps = Et + T::E_DOUBLES;
-    double *Rs = Ps + T::P_DOUBLES;
-    double *Ez = Rs;
-    double *Fs = Rs + T::R_DOUBLES;
-    double *Gs = Fs + T::F_DOUBLES;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(Gs + T::G_DOUBLES);
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    double *Ut = reinterpret_cast<double *>(smem_raw);
+    double *Et = reinterpret_cast<double *>(smem_raw + T::OFF_E);
+    Real *Pv = reinterpret_cast<Real *>(smem_raw + T::OFF_PV);
+    double *Pb = reinterpret_cast<double *>(smem_raw + T::OFF_PB);
+    Real *Rs = reinterpret_cast<Real *>(smem_raw + T::OFF_R);
+    double *Ez = reinterpret_cast<double *>(smem_raw + T::OFF_R);
+    double *Fm = reinterpret_cast<double *>(smem_raw + T::OFF_FM);
+    Real *Fo = reinterpret_cast<Real *>(smem_raw + T::OFF_FO);
+    double *Gm = reinterpret_cast<double *>(smem_raw + T::OFF_GM);
+    Real *Go = reinterpret_cast<Real *>(smem_raw + T::OFF_GO);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::OFF_BAR);
 
     const Grid &g = a.g;
     const int tid = threadIdx.x;
@@ -184,7 +225,9 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
 
     const double gm = g.gamma, EPS = g.eps;
 #if RMHD_FAST_MATH
-    const double inv_gm1 = 1.0 / (gm - 1.0);
+    const Real gmR = (Real)gm, EPSR = (Real)EPS, inv_gm1 = (Real)(1.0 / (gm - 1.0));
+#else
+    const Real EPSR = EPS;
 #endif
 
     // ---- primitives on (TI+4) x (TJ+4) cells ----
@@ -213,14 +256,17 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
                         - 0.5 * (bXc * bXc + bYc * bYc + bZ * bZ));
         const double py = (gm - 1.0) * (e - 0.5 * (rho * (v * v + w * w + u * u))
                         - 0.5 * (bYc * bYc + bZ * bZ + bXc * bXc));
-        double *p0 = Ps + c;
-        p0[P_U * PF] = u;
-        p0[P_V * PF] = v;
-        p0[P_W * PF] = w;
-        p0[P_BXC * PF] = bXc;
-        p0[P_BYC * PF] = bYc;
-        p0[P_PX * PF] = px;
-        p0[P_PY * PF] = py;
+        // primitives are recovered in FP64; the velocities are stored in the
+        // flux-side type, centred B and pressures in FP64
+        Real *v0 = Pv + c;
+        v0[V_U * PF] = (Real)u;
+        v0[V_V * PF] = (Real)v;
+        v0[V_W * PF] = (Real)w;
+        double *b0 = Pb + c;
+        b0[B_XC * PF] = bXc;
+        b0[B_YC * PF] = bYc;
+        b0[B_PX * PF] = px;
+        b0[B_PY * PF] = py;
     }
     __syncthreads();
 
@@ -229,25 +275,25 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     {
         const double two_dx = 2.0 * g.dx, two_dy = 2.0 * g.dy;
 #if RMHD_FAST_MATH
-        const double i2dx = 1.0 / two_dx, i2dy = 1.0 / two_dy;
+        const Real i2dx = (Real)(1.0 / two_dx), i2dy = (Real)(1.0 / two_dy);
 #endif
         for (int c = tid; c < RF; c += STAGE_THREADS) {
             const int ri = c / RJ_, rj = c - ri * RJ_;
-            const double *p0 = Ps + (ri + 1) * PJ_ + (rj + 1);
+            const double *p0 = Pb + (ri + 1) * PJ_ + (rj + 1);
             const double *z0 = Ut + BZF * UF + (ri + 2) * UJ + (rj + 2);
 #if RMHD_FAST_MATH
-            const double jY = -(z0[UJ] - z0[-UJ]) * i2dx;
-            const double jX = (z0[1] - z0[-1]) * i2dy;
-            const double jZ = (p0[P_BYC * PF + PJ_] - p0[P_BYC * PF - PJ_]) * i2dx
-                            - (p0[P_BXC * PF + 1] - p0[P_BXC * PF - 1]) * i2dy;
+            const Real jY = -(Real)(z0[UJ] - z0[-UJ]) * i2dx;
+            const Real jX = (Real)(z0[1] - z0[-1]) * i2dy;
+            const Real jZ = (Real)(p0[B_YC * PF + PJ_] - p0[B_YC * PF - PJ_]) * i2dx
+                          - (Real)(p0[B_XC * PF + 1] - p0[B_XC * PF - 1]) * i2dy;
 #else
             const double jY = -(z0[UJ] - z0[-UJ]) / two_dx;
             const double jX = (z0[1] - z0[-1]) / two_dy;
-            const double jZ = (p0[P_BYC * PF + PJ_] - p0[P_BYC * PF - PJ_]) / two_dx
-                            - (p0[P_BXC * PF + 1] - p0[P_BXC * PF - 1]) / two_dy;
+            const double jZ = (p0[B_YC * PF + PJ_] - p0[B_YC * PF - PJ_]) / two_dx
+                            - (p0[B_XC * PF + 1] - p0[B_XC * PF - 1]) / two_dy;
 #endif
-            const double eta = has_eta ? Et[(ri + 2) * UJ + (rj + 2)] : g.eta;
-            double *r0 = Rs + c;
+            const Real eta = (Real)(has_eta ? Et[(ri + 2) * UJ + (rj + 2)] : g.eta);
+            Real *r0 = Rs + c;
             r0[R_JX * RF] = eta * jX;
             r0[R_JY * RF] = eta * jY;
             r0[R_JZ * RF] = eta * jZ;
@@ -274,63 +320,125 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
             cj = a1 - 1;
         }
         const double *uc = Ut + (ci + HALO) * UJ + (cj + HALO);
-        const double *pc = Ps + (ci + 2) * PJ_ + (cj + 2);
-        const double *r0 = Rs + (ci + 1) * RJ_ + (cj + 1);
+        const Real *vc = Pv + (ci + 2) * PJ_ + (cj + 2);
+        const double *bc = Pb + (ci + 2) * PJ_ + (cj + 2);
+        const Real *r0 = Rs + (ci + 1) * RJ_ + (cj + 1);
         const int us = isF ? UJ : 1, ps = isF ? PJ_ : 1;
-        // sweep-frame components (the y sweep runs the x-sweep arithmetic on
-        // (rho, v, w, u, bY, bZ, bX, e), hlld.cu:134-152)
-        const double *cp[7] = {uc + RHO * UF,
-                               pc + (isF ? P_U : P_V) * PF,
-                               pc + (isF ? P_V : P_W) * PF,
-                               pc + (isF ? P_W : P_U) * PF,
-                               isF ? pc + P_BYC * PF : uc + BZF * UF,
-                               isF ? uc + BZF * UF : pc + P_BXC * PF,
-                               pc + (isF ? P_PX : P_PY) * PF};
-        const int cs[7] = {us, ps, ps, ps, isF ? ps : us, isF ? us : ps, ps};
-        double qL[7], qR[7];
-#pragma unroll
-        for (int n = 0; n < 7; ++n) {
-            const double *q = cp[n];
-            const int st = cs[n];
-            const double qm = q[-st], q0 = q[0], qp = q[st], qpp = q[2 * st];
-            qL[n] = q0 + 0.5 * minmod(q0 - qm, qp - q0, EPS);
-            qR[n] = qp - 0.5 * minmod(qp - q0, qpp - qp, EPS);
-        }
-        const double *nb = pc + (isF ? P_BXC : P_BYC) * PF;
+        // sweep frame: the y sweep runs the x-sweep arithmetic on
+        // (rho, v, w, u, bY, bZ, bX, e) (hlld.cu:134-152)
+        const int pu = isF ? V_U : V_V, pv = isF ? V_V : V_W, pw = isF ? V_W : V_U;
+        const double *pp = bc + (isF ? B_PX : B_PY) * PF;
+        const double *bt1 = isF ? bc + B_YC * PF : uc + BZF * UF;   // tangential B 1
+        const double *bt2 = isF ? uc + BZF * UF : bc + B_XC * PF;   // tangential B 2
+        const int s1 = isF ? ps : us, s2 = isF ? us : ps;
+        const double *nb = bc + (isF ? B_XC : B_YC) * PF;
         const double bn = 0.5 * (nb[0] + nb[ps]);
-        const Prim L{qL[0], qL[1], qL[2], qL[3], bn, qL[4], qL[5], qL[6]};
-        const Prim R{qR[0], qR[1], qR[2], qR[3], bn, qR[4], qR[5], qR[6]};
-        double f[8];
-#if RMHD_FAST_MATH
-        hlld_flux_fast(L, R, gm, inv_gm1, EPS, f);
+        double fmv[3];   // momentum fluxes (rhoU, rhoV, rhoW in the sweep frame)
+        Real fov[4];     // mass, bZ-frame tangential-2 induction, energy, tangential-1 induction
+#if RMHD_BULK
+        {
+            const float EPSF = (float)EPS;
+            BulkStates st;
+            {
+                const double *q = uc + RHO * UF;
+                double a0d, a1d;
+                muscl_dev(q[-us], q[0], q[us], q[2 * us], EPSF, a0d, a1d);
+                st.rhoL = (float)a0d;
+                st.rhoR = (float)a1d;
+            }
+            {
+                const Real *q = vc + pu * PF;
+                const float qm = q[-ps], q0 = q[0], qp = q[ps], qpp = q[2 * ps];
+                st.uL = q0 + 0.5f * minmod(q0 - qm, qp - q0, EPSF);
+                st.uR = qp - 0.5f * minmod(qp - q0, qpp - qp, EPSF);
+            }
+            {
+                const Real *q = vc + pv * PF;
+                const float qm = q[-ps], q0 = q[0], qp = q[ps], qpp = q[2 * ps];
+                st.vL = q0 + 0.5f * minmod(q0 - qm, qp - q0, EPSF);
+                st.vR = qp - 0.5f * minmod(qp - q0, qpp - qp, EPSF);
+            }
+            {
+                const Real *q = vc + pw * PF;
+                const float qm = q[-ps], q0 = q[0], qp = q[ps], qpp = q[2 * ps];
+                st.wL = q0 + 0.5f * minmod(q0 - qm, qp - q0, EPSF);
+                st.wR = qp - 0.5f * minmod(qp - q0, qpp - qp, EPSF);
+            }
+            muscl_dev(pp[-ps], pp[0], pp[ps], pp[2 * ps], EPSF, st.pL, st.pR);
+            muscl_dev(bt1[-s1], bt1[0], bt1[s1], bt1[2 * s1], EPSF, st.bYL, st.bYR);
+            muscl_dev(bt2[-s2], bt2[0], bt2[s2], bt2[2 * s2], EPSF, st.bZL, st.bZR);
+            st.bn = bn;
+            float fo4[4];
+            hlld_flux_bulk(st, gmR, inv_gm1, EPSF, fmv, fo4);
+            // fo4: f0, f5 (tangential-1 induction), f6 (tangential-2), f7
+            fov[0] = fo4[0]; fov[1] = fo4[2]; fov[2] = fo4[3]; fov[3] = fo4[1];
+        }
 #else
-        hlld_flux<RMHD_ALL_CANDIDATES>(L, R, gm, EPS, f);
+        {
+            Real qL[7], qR[7];
+            auto rec = [&](const Real qm, const Real q0, const Real qp, const Real qpp, Real &l, Real &r) {
+                l = q0 + Real(0.5) * minmod(q0 - qm, qp - q0, EPSR);
+                r = qp - Real(0.5) * minmod(qp - q0, qpp - qp, EPSR);
+            };
+            {
+                const double *q = uc + RHO * UF;
+                rec((Real)q[-us], (Real)q[0], (Real)q[us], (Real)q[2 * us], qL[0], qR[0]);
+            }
+            {
+                const Real *q = vc + pu * PF;
+                rec(q[-ps], q[0], q[ps], q[2 * ps], qL[1], qR[1]);
+            }
+            {
+                const Real *q = vc + pv * PF;
+                rec(q[-ps], q[0], q[ps], q[2 * ps], qL[2], qR[2]);
+            }
+            {
+                const Real *q = vc + pw * PF;
+                rec(q[-ps], q[0], q[ps], q[2 * ps], qL[3], qR[3]);
+            }
+            rec((Real)bt1[-s1], (Real)bt1[0], (Real)bt1[s1], (Real)bt1[2 * s1], qL[4], qR[4]);
+            rec((Real)bt2[-s2], (Real)bt2[0], (Real)bt2[s2], (Real)bt2[2 * s2], qL[5], qR[5]);
+            rec((Real)pp[-ps], (Real)pp[0], (Real)pp[ps], (Real)pp[2 * ps], qL[6], qR[6]);
+            const PrimT<Real> L{qL[0], qL[1], qL[2], qL[3], (Real)bn, qL[4], qL[5], qL[6]};
+            const PrimT<Real> R{qR[0], qR[1], qR[2], qR[3], (Real)bn, qR[4], qR[5], qR[6]};
+            Real f[8];
+#if RMHD_FAST_MATH
+            hlld_flux_fast(L, R, gmR, inv_gm1, EPSR, f);
+#else
+            hlld_flux<RMHD_ALL_CANDIDATES>(L, R, gm, EPS, f);
+#endif
+            fmv[0] = f[1]; fmv[1] = f[2]; fmv[2] = f[3];
+            fov[0] = f[0]; fov[1] = f[6]; fov[2] = f[7]; fov[3] = f[5];
+        }
 #endif
         // eta*J of the two cells sharing the interface and their B
         const int rs = isF ? RJ_ : 1;
-        const double z0 = uc[BZF * UF], z1 = uc[BZF * UF + us];
+        const Real z0 = (Real)uc[BZF * UF], z1 = (Real)uc[BZF * UF + us];
+        const Real h = Real(0.5);
         if (isF) {
-            const double eY0 = r0[R_JY * RF], eY1 = r0[R_JY * RF + rs];
-            const double eZ0 = r0[R_JZ * RF], eZ1 = r0[R_JZ * RF + rs];
-            const double y0 = pc[P_BYC * PF], y1 = pc[P_BYC * PF + ps];
-            const double f6 = f[6] + 0.5 * (eY0 + eY1);
-            const double f7 = f[7] + (0.5 * (eY0 * z0 + eY1 * z1) - 0.5 * (eZ0 * y0 + eZ1 * y1));
-            double *o = Fs + a0 * F_NJ + a1;
-            o[0 * SF] = f[0]; o[1 * SF] = f[1]; o[2 * SF] = f[2]; o[3 * SF] = f[3];
-            o[4 * SF] = f6; o[5 * SF] = f7;
-            if (STAGE == 1) o[SLOT_EMF * SF] = f[5] - 0.5 * (eZ0 + eZ1);
+            const Real eY0 = r0[R_JY * RF], eY1 = r0[R_JY * RF + rs];
+            const Real eZ0 = r0[R_JZ * RF], eZ1 = r0[R_JZ * RF + rs];
+            const Real y0 = (Real)bc[B_YC * PF], y1 = (Real)bc[B_YC * PF + ps];
+            double *om = Fm + a0 * F_NJ + a1;
+            Real *oo = Fo + a0 * F_NJ + a1;
+            om[0 * SF] = fmv[0]; om[1 * SF] = fmv[1]; om[2 * SF] = fmv[2];
+            oo[O_RHO * SF] = fov[0];
+            oo[O_BZ * SF] = fov[1] + h * (eY0 + eY1);
+            oo[O_EN * SF] = fov[2] + (h * (eY0 * z0 + eY1 * z1) - h * (eZ0 * y0 + eZ1 * y1));
+            if (STAGE == 1) oo[O_EMF * SF] = fov[3] - h * (eZ0 + eZ1);
         } else {
-            const double eX0 = r0[R_JX * RF], eX1 = r0[R_JX * RF + rs];
-            const double eZ0 = r0[R_JZ * RF], eZ1 = r0[R_JZ * RF + rs];
-            const double x0 = pc[P_BXC * PF], x1 = pc[P_BXC * PF + ps];
+            const Real eX0 = r0[R_JX * RF], eX1 = r0[R_JX * RF + rs];
+            const Real eZ0 = r0[R_JZ * RF], eZ1 = r0[R_JZ * RF + rs];
+            const Real x0 = (Real)bc[B_XC * PF], x1 = (Real)bc[B_XC * PF + ps];
             // un-permute (hlld.cu:170-194): g1 = f3, g2 = f1, g3 = f2,
             // g4 = f6, g5 = f4 = 0, g6 = f5.
-            const double g6 = f[5] - 0.5 * (eX0 + eX1);
-            const double g7 = f[7] + (0.5 * (eZ0 * x0 + eZ1 * x1) - 0.5 * (eX0 * z0 + eX1 * z1));
-            double *o = Gs + a0 * G_NJ + a1;
-            o[0 * SG] = f[0]; o[1 * SG] = f[3]; o[2 * SG] = f[1]; o[3 * SG] = f[2];
-            o[4 * SG] = g6; o[5 * SG] = g7;
-            if (STAGE == 1) o[SLOT_EMF * SG] = f[6] + 0.5 * (eZ0 + eZ1);
+            double *om = Gm + a0 * G_NJ + a1;
+            Real *oo = Go + a0 * G_NJ + a1;
+            om[0 * SG] = fmv[2]; om[1 * SG] = fmv[0]; om[2 * SG] = fmv[1];
+            oo[O_RHO * SG] = fov[0];
+            oo[O_BZ * SG] = fov[3] - h * (eX0 + eX1);
+            oo[O_EN * SG] = fov[2] + (h * (eZ0 * x0 + eZ1 * x1) - h * (eX0 * z0 + eX1 * z1));
+            if (STAGE == 1) oo[O_EMF * SG] = fov[1] + h * (eZ0 + eZ1);
         }
     }
     __syncthreads();
@@ -342,30 +450,39 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         // (i0-1+ei, j0-1+ej), i.e. Fs (fi, fj) = (ei, ej) and Gs (gi, gj) = (ei, ej) ----
         for (int c = tid; c < T::EI_ * EJ_; c += STAGE_THREADS) {
             const int ei = c / EJ_, ej = c - ei * EJ_;
-            const double eZG1 = Gs[SLOT_EMF * SG + ei * G_NJ + ej];
-            const double eZG2 = Gs[SLOT_EMF * SG + (ei + 1) * G_NJ + ej];
-            const double eZF1 = -1.0 * Fs[SLOT_EMF * SF + ei * F_NJ + ej];
-            const double eZF2 = -1.0 * Fs[SLOT_EMF * SF + ei * F_NJ + ej + 1];
+            // accumulated in FP64 whatever the flux-side type
+            const double eZG1 = (double)Go[O_EMF * SG + ei * G_NJ + ej];
+            const double eZG2 = (double)Go[O_EMF * SG + (ei + 1) * G_NJ + ej];
+            const double eZF1 = -1.0 * (double)Fo[O_EMF * SF + ei * F_NJ + ej];
+            const double eZF2 = -1.0 * (double)Fo[O_EMF * SF + ei * F_NJ + ej + 1];
             Ez[c] = 0.25 * (eZG1 + eZG2 + eZF1 + eZF2);
         }
         __syncthreads();
     }
 
     // ---- update of the tile's own cells ----
-    const double *fR = Fs + (li + 1) * F_NJ + (lj - T::F_J0);    // F(i)
-    const double *fL = fR - F_NJ;                                  // F(i-1)
-    const double *gU = Gs + (li - T::G_I0) * G_NJ + (lj + 1);    // G(j)
-    const double *gD = gU - 1;                                     // G(j-1)
+    const int fo_ = (li + 1) * F_NJ + (lj - T::F_J0);             // F(i); F(i-1) is F_NJ before
+    const int go_ = (li - T::G_I0) * G_NJ + (lj + 1);             // G(j); G(j-1) is 1 before
     const double *uo = Ut + (li + HALO) * UJ + (lj + HALO);        // own cell in the staged tile
     const int fld[6] = {RHO, MX, MY, MZ, BZF, EN};
+    // flux difference of hydro field n (0..5), in FP64
+    auto dF = [&](int n) -> double {
+        if (n >= 1 && n <= 3) return Fm[(n - 1) * SF + fo_] - Fm[(n - 1) * SF + fo_ - F_NJ];
+        const int o = n == 0 ? O_RHO : (n == 4 ? O_BZ : O_EN);
+        return (double)Fo[o * SF + fo_] - (double)Fo[o * SF + fo_ - F_NJ];
+    };
+    auto dG = [&](int n) -> double {
+        if (n >= 1 && n <= 3) return Gm[(n - 1) * SG + go_] - Gm[(n - 1) * SG + go_ - 1];
+        const int o = n == 0 ? O_RHO : (n == 4 ? O_BZ : O_EN);
+        return (double)Go[o * SG + go_] - (double)Go[o * SG + go_ - 1];
+    };
 
     if (STAGE == 1) {
         if (own) {
             // oneStepFirstFunctor (resistiveMHD_2D.cu:53-86)
 #pragma unroll
             for (int n = 0; n < 6; ++n)
-                a.dst[fld[n] * PL + k] = uo[fld[n] * UF] - dtdx * (fR[n * SF] - fL[n * SF])
-                                       - dtdy * (gU[n * SG] - gD[n * SG]);
+                a.dst[fld[n] * PL + k] = uo[fld[n] * UF] - dtdx * dF(n) - dtdy * dG(n);
             // CT_kernel (ct.cu:44-59) with the EMF of this stage
             const double *ez = Ez + (li + 1) * EJ_ + (lj + 1);
             a.dst[BXF * PL + k] = uo[BXF * UF] - dtdy * (ez[0] - ez[-1]);
@@ -386,7 +503,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
             for (int n = 0; n < 6; ++n) {
                 const double u = a.un[fld[n] * PL + k];
                 const double ub = uo[fld[n] * UF];
-                nv[fld[n]] = 0.5 * (u + ub - dtdx * (fR[n * SF] - fL[n * SF]) - dtdy * (gU[n * SG] - gD[n * SG]));
+                nv[fld[n]] = 0.5 * (u + ub - dtdx * dF(n) - dtdy * dG(n));
             }
             nv[BXF] = uo[BXF * UF];
             nv[BYF] = uo[BYF * UF];
@@ -413,8 +530,8 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
             const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
             bits = o > bits ? o : bits;
         }
-        // Ps is dead after the flux phase: reuse it for the per-warp maxima.
-        unsigned long long *wmax = reinterpret_cast<unsigned long long *>(Ps);
+        // Pb is dead after the flux phase: reuse it for the per-warp maxima.
+        unsigned long long *wmax = reinterpret_cast<unsigned long long *>(Pb);
         if ((tid & 31) == 0) wmax[tid >> 5] = bits;
         const int any_nan = __syncthreads_or(nan_e);
         if (tid == 0) {

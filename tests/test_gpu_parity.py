@@ -16,6 +16,9 @@ from conftest import GOLDEN_CASES, load_golden
 pytestmark = pytest.mark.gpu
 
 FAST_REL_L1 = 1e-12
+# FP32-bulk (single-precision reconstruction and fluxes, FP64 pressure
+# recovery, EMF, update and dt): relative L1 <= 1e-5 against FP64.
+BULK_REL_L1 = 1e-5
 
 
 def run_cuda(setup, nsteps, precision="fp64_exact", initial=None, use_run=False):
@@ -88,6 +91,29 @@ def test_fast_within_tolerance(gpu, oracle, bc, table, shape):
     out, _, _, crashed = run_cuda(s, 10, precision="fp64_fast")
     assert not crashed
     assert rel_l1(out, ref).max() <= FAST_REL_L1
+
+
+@pytest.mark.parametrize("bc,table,shape", CASES[:4])
+def test_fp32_bulk_within_tolerance(gpu, oracle, bc, table, shape):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(*shape, seed=6, bc=bc, with_table=table)
+    ref, _, _ = oracle.run(s, s.state, 10)
+    out, _, _, crashed = run_cuda(s, 10, precision="fp32_bulk")
+    assert not crashed
+    err = rel_l1(out, ref)
+    assert err.max() <= BULK_REL_L1
+    assert err.max() > 0.0   # it is a different arithmetic, not the FP64 path
+
+
+def test_fp32_bulk_orszag_tang_and_harris(gpu, oracle):
+    from resistivemhd_gpu_b200 import setups
+
+    for s, n in ((setups.orszag_tang(256), 100), (setups.harris_sheet(256, 128), 40)):
+        ref, _, _ = oracle.run(s, s.state, n)
+        out, _, _, crashed = run_cuda(s, n, precision="fp32_bulk")
+        assert not crashed
+        assert rel_l1(out, ref).max() <= BULK_REL_L1, s.name
 
 
 def test_run_graph_equals_step_loop(gpu):
