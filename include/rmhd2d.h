@@ -73,7 +73,10 @@ typedef struct {
     double eps;                 /* EPS regulariser of the reference (const.hpp:4) */
     double eta;                 /* scalar eta: the resistive term when no eta table is set,
                                    and always the diffusive dt limit dx^2/eta (resistiveMHD_2D.cu:288) */
-    int bc;                     /* rmhd2d_bc, applied in x and y */
+    int bc;                     /* rmhd2d_bc of the x walls (and of the y walls when bc_y = -1) */
+    int bc_y;                   /* rmhd2d_bc of the y walls, or -1 for the same as bc; periodic x with
+                                   symmetric y is the reference's oneStepRK2PeriodicXSymmetricY
+                                   (lib_ResistiveMHD_2D_GPU_single/resistiveMHD_2D.cu:198-259) */
     int precision;              /* rmhd2d_precision */
     int device;                 /* CUDA device ordinal */
     void *stream;               /* cudaStream_t to enqueue on, or NULL for a solver-owned stream */
@@ -81,7 +84,7 @@ typedef struct {
 
 typedef struct rmhd2d_solver rmhd2d_solver;
 
-/* Fills cfg with defaults (gamma 5/3, cfl 0.4, eps 1e-20, periodic, FP64 exact). */
+/* Fills cfg with defaults (gamma 5/3, cfl 0.4, eps 1e-20, periodic x and y, FP64 exact). */
 void rmhd2d_config_default(rmhd2d_config *cfg);
 
 /* Replaces the constructor ResistiveMHD2D::ResistiveMHD2D()

@@ -485,8 +485,8 @@ int orc_is_crashed(const orc_params *p, const double *U)
     return 0;
 }
 
-/* boundary.cu:4-57 periodicBoundaryX2nd_kernel + :59-110 Y2nd. */
-static void periodic_boundary(const orc_params *p, double *U)
+/* boundary.cu:4-57 periodicBoundaryX2nd_kernel. */
+static void periodic_x(const orc_params *p, double *U)
 {
     const int nx = p->nx, ny = p->ny;
     for (int j = 0; j < ny; ++j)
@@ -494,6 +494,12 @@ static void periodic_boundary(const orc_params *p, double *U)
             memcpy(&U[(j + g * ny) * NV], &U[(j + (nx - 6 + g) * ny) * NV], NV * sizeof(double));
             memcpy(&U[(j + (nx - 3 + g) * ny) * NV], &U[(j + (3 + g) * ny) * NV], NV * sizeof(double));
         }
+}
+
+/* boundary.cu:73-141 periodicBoundaryY2nd_kernel. */
+static void periodic_y(const orc_params *p, double *U)
+{
+    const int nx = p->nx, ny = p->ny;
     for (int i = 0; i < nx; ++i)
         for (int g = 0; g < 3; ++g) {
             memcpy(&U[(g + i * ny) * NV], &U[(ny - 6 + g + i * ny) * NV], NV * sizeof(double));
@@ -506,14 +512,15 @@ static void copy_except(double *dst, const double *src, int skip)
     for (int f = 0; f < NV; ++f) if (f != skip) dst[f] = src[f];
 }
 
-/* symmetricXY/boundary.cu:4-104 symmetricBoundaryX2nd (+BX) and :107-205
-   symmetricBoundaryY2nd (+BY): mirror copies of every field except the
-   normal B, whose ghosts are integrated from the discrete div B = 0. */
-static void symmetric_boundary(const orc_params *p, double *U)
+#define C(i, j) (&U[((j) + (i) * ny) * NV])
+
+/* symmetricXY/boundary.cu:4-104 symmetricBoundaryX2nd (+BX): mirror copies
+   of every field except bX, whose ghosts are integrated from the discrete
+   div B = 0. */
+static void symmetric_x(const orc_params *p, double *U)
 {
     const int nx = p->nx, ny = p->ny;
     const double dx = p->dx, dy = p->dy;
-#define C(i, j) (&U[((j) + (i) * ny) * NV])
     for (int j = 0; j < ny; ++j) {
         copy_except(C(0, j), C(5, j), BXF);
         copy_except(C(1, j), C(4, j), BXF);
@@ -540,6 +547,13 @@ static void symmetric_boundary(const orc_params *p, double *U)
             C(nx - 1, j)[BXF] = C(nx - 2, j)[BXF];
         }
     }
+}
+
+/* symmetricXY/boundary.cu:107-205 symmetricBoundaryY2nd (+BY). */
+static void symmetric_y(const orc_params *p, double *U)
+{
+    const int nx = p->nx, ny = p->ny;
+    const double dx = p->dx, dy = p->dy;
     for (int i = 0; i < nx; ++i) {
         copy_except(C(i, 0), C(i, 5), BYF);
         copy_except(C(i, 1), C(i, 4), BYF);
@@ -566,13 +580,19 @@ static void symmetric_boundary(const orc_params *p, double *U)
             C(i, ny - 1)[BYF] = C(i, ny - 2)[BYF];
         }
     }
-#undef C
 }
+#undef C
 
+/* The x pass then the y pass, as every oneStepRK2 variant calls them
+   (TP/TS resistiveMHD_2D.cu:171-172,193-194; the periodic-x / symmetric-y
+   composition is lib_ResistiveMHD_2D_GPU_single/resistiveMHD_2D.cu:229-230,252-253). */
 void orc_boundary(const orc_params *p, double *U)
 {
-    if (p->bc == ORC_BC_SYMMETRIC) symmetric_boundary(p, U);
-    else periodic_boundary(p, U);
+    const int bcy = p->bc_y < 0 ? p->bc : p->bc_y;
+    if (p->bc == ORC_BC_SYMMETRIC) symmetric_x(p, U);
+    else periodic_x(p, U);
+    if (bcy == ORC_BC_SYMMETRIC) symmetric_y(p, U);
+    else periodic_y(p, U);
 }
 
 size_t orc_work_doubles(int nx, int ny)

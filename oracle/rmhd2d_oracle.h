@@ -23,7 +23,8 @@ typedef struct {
     double eps;               /* EPS regulariser */
     double eta;               /* scalar eta: resistive term when eta_table is NULL, and dt limit */
     const double *eta_table;  /* optional cell-centred eta, k = j + i*ny */
-    int bc;                   /* ORC_BC_PERIODIC or ORC_BC_SYMMETRIC (both directions) */
+    int bc;                   /* x boundary: ORC_BC_PERIODIC or ORC_BC_SYMMETRIC */
+    int bc_y;                 /* y boundary, or -1 for the same as bc */
 } orc_params;
 
 double orc_calc_dt(const orc_params *p, const double *U);

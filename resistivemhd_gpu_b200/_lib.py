@@ -28,7 +28,7 @@ class Config(ctypes.Structure):
         ("dx", ctypes.c_double), ("dy", ctypes.c_double),
         ("gamma_mhd", ctypes.c_double), ("cfl", ctypes.c_double), ("eps", ctypes.c_double),
         ("eta", ctypes.c_double),
-        ("bc", ctypes.c_int), ("precision", ctypes.c_int), ("device", ctypes.c_int),
+        ("bc", ctypes.c_int), ("bc_y", ctypes.c_int), ("precision", ctypes.c_int), ("device", ctypes.c_int),
         ("stream", ctypes.c_void_p),
     ]
 

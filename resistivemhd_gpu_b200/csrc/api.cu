@@ -140,7 +140,7 @@ int refresh_rate(rmhd2d_solver *s)
 
 int do_boundary(rmhd2d_solver *s)
 {
-    if (s->g.bc == BC_SYMMETRIC) launch_snapshot_row2(s->g, s->A, s->row2, s->stream);
+    if (s->g.bc_x == BC_SYMMETRIC) launch_snapshot_row2(s->g, s->A, s->row2, s->stream);
     launch_boundary(s->g, s->A, s->row2, nullptr, 0, s->stream);
     CK(cudaGetLastError());
     return RMHD2D_OK;
@@ -162,7 +162,7 @@ void enqueue_step(rmhd2d_solver *s, int parity)
     StageArgs a{};
     a.g = s->g;
     a.eta = s->eta;
-    a.row2 = s->g.bc == BC_SYMMETRIC ? s->row2 : nullptr;
+    a.row2 = s->g.bc_x == BC_SYMMETRIC ? s->row2 : nullptr;
     a.ctl = s->ctl;
     a.parity = parity;
     auto launch = stage_launcher(s->cfg.precision);
@@ -215,6 +215,7 @@ void rmhd2d_config_default(rmhd2d_config *c)
     c->eps = 1e-20;
     c->eta = 0.0;
     c->bc = RMHD2D_BC_PERIODIC;
+    c->bc_y = -1;
     c->precision = RMHD2D_FP64_EXACT;
     c->device = 0;
     c->stream = nullptr;
@@ -255,6 +256,8 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
     if (!(cfg->eta >= 0.0)) return fail(s, RMHD2D_ERR_INVALID, "eta must be >= 0");
     if (cfg->bc != RMHD2D_BC_PERIODIC && cfg->bc != RMHD2D_BC_SYMMETRIC)
         return fail(s, RMHD2D_ERR_INVALID, "unknown boundary kind");
+    if (cfg->bc_y != -1 && cfg->bc_y != RMHD2D_BC_PERIODIC && cfg->bc_y != RMHD2D_BC_SYMMETRIC)
+        return fail(s, RMHD2D_ERR_INVALID, "unknown y boundary kind");
     if (cfg->precision != RMHD2D_FP64_EXACT && cfg->precision != RMHD2D_FP64_FAST &&
         cfg->precision != RMHD2D_FP32_BULK)
         return fail(s, RMHD2D_ERR_INVALID, "unknown precision");
@@ -280,7 +283,8 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
     g.cfl = cfg->cfl;
     g.eps = cfg->eps;
     g.eta = cfg->eta;
-    g.bc = cfg->bc;
+    g.bc_x = cfg->bc;
+    g.bc_y = cfg->bc_y < 0 ? cfg->bc : cfg->bc_y;
 
     auto bail = [&](int code, const std::string &msg) {
         {
@@ -484,7 +488,7 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
     StageArgs a{};
     a.g = s->g;
     a.eta = s->eta;
-    a.row2 = s->g.bc == BC_SYMMETRIC ? s->row2 : nullptr;
+    a.row2 = s->g.bc_x == BC_SYMMETRIC ? s->row2 : nullptr;
     a.ctl = s->ctl;
     a.parity = parity;
     auto launch = stage_launcher(s->cfg.precision);

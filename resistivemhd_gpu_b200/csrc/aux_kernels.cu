@@ -29,6 +29,9 @@ __device__ __forceinline__ int wrap(int c, int n)
     return c;
 }
 
+// Source index of a ghost cell along one direction: periodic wrap or mirror.
+__device__ __forceinline__ int image(int c, int n, int bc) { return bc == BC_PERIODIC ? wrap(c, n) : mirror(c, n); }
+
 // bY seen by the x-wall integration at interior column c and row r: the
 // lower-wall face row (r = 2) holds the stage's constrained-transport value
 // (row2), which the symmetric y pass replaces only afterwards.
@@ -59,11 +62,14 @@ __device__ double bX_xghost(const Grid &g, const double *bX, const double *bY, c
     return b - (bY_prewall(g, bY, row2, nx - 6, r) - bY_prewall(g, bY, row2, nx - 6, r - 1)) / dy * dx;    // nx-1
 }
 
-// bX after the x pass at column c (any) and interior row r.
+// bX after the x pass at column c (any) and interior row r: periodic x walls
+// copy it, symmetric ones integrate it.
 __device__ __forceinline__ double bX_afterx(const Grid &g, const double *bX, const double *bY, const double *row2,
                                             int c, int r)
 {
-    return (c >= 3 && c < g.nx - 3) ? bX[at(g, c, r)] : bX_xghost(g, bX, bY, row2, c, r);
+    if (c >= 3 && c < g.nx - 3) return bX[at(g, c, r)];
+    if (g.bc_x == BC_PERIODIC) return bX[at(g, wrap(c, g.nx), r)];
+    return bX_xghost(g, bX, bY, row2, c, r);
 }
 
 // y-wall ghost bY at column i, ghost row j
@@ -72,7 +78,7 @@ __device__ double bY_yghost(const Grid &g, const double *bX, const double *bY, c
 {
     const double dx = g.dx, dy = g.dy;
     const int ny = g.ny;
-    const int mi = mirror(i, g.nx);
+    const int mi = image(i, g.nx, g.bc_x);   // bY of ghost columns after the x pass
     if (j < 3) {
         double b = bY[at(g, mi, 3)];
         if (i == 0) return b;
@@ -110,9 +116,10 @@ __device__ __forceinline__ void ghost_cell(const Grid &g, long long t, int &i, i
     }
 }
 
-// Fills every ghost cell of `s` from its interior (and, for symmetric walls,
-// the CT'd lower-wall bY row), with the exact results of the reference's two
-// boundary passes (periodic: boundary.cu:4-141; symmetric: TS boundary.cu:4-206).
+// Fills every ghost cell of `s` from its interior (and, for symmetric x
+// walls, the CT'd lower-wall bY row), with the exact results of the
+// reference's x pass followed by its y pass, each periodic
+// (boundary.cu:4-141) or symmetric (TS boundary.cu:4-206).
 // With `ctl` set it also folds the ghost cells' CFL rate and NaN-energy test
 // into the reductions of the stage-2 kernel.
 __global__ void boundary_kernel(Grid g, double *s, const double *row2, Control *ctl, int slot)
@@ -127,20 +134,20 @@ __global__ void boundary_kernel(Grid g, double *s, const double *row2, Control *
         const long long P = g.plane;
         const long long k = at(g, i, j);
         double v[8];
-        if (g.bc == BC_PERIODIC) {
-            const long long src = at(g, wrap(i, g.nx), wrap(j, g.ny));
+        // hydro fields: the image of the x pass, then of the y pass
+        const int mi = image(i, g.nx, g.bc_x), mj = image(j, g.ny, g.bc_y);
+        const long long src = at(g, mi, mj);
+        const int hydro[6] = {RHO, MX, MY, MZ, BZF, EN};
 #pragma unroll
-            for (int f = 0; f < 8; ++f) v[f] = s[f * P + src];
-        } else {
-            const int mi = mirror(i, g.nx), mj = mirror(j, g.ny);
-            const long long src = at(g, mi, mj);
-            const int hydro[6] = {RHO, MX, MY, MZ, BZF, EN};
-#pragma unroll
-            for (int n = 0; n < 6; ++n) v[hydro[n]] = s[hydro[n] * P + src];
-            const double *bX = s + BXF * P, *bY = s + BYF * P;
-            v[BXF] = bX_afterx(g, bX, bY, row2, i, mj);
-            v[BYF] = (j >= 3 && j < g.ny - 3) ? bY[at(g, mi, j)] : bY_yghost(g, bX, bY, row2, i, j);
-        }
+        for (int n = 0; n < 6; ++n) v[hydro[n]] = s[hydro[n] * P + src];
+        const double *bX = s + BXF * P, *bY = s + BYF * P;
+        // bX: x pass (copy or integration), then the y pass copies rows
+        v[BXF] = bX_afterx(g, bX, bY, row2, i, mj);
+        // bY: x pass copies columns, then the y pass copies or integrates rows
+        if ((j >= 3 && j < g.ny - 3) || g.bc_y == BC_PERIODIC)
+            v[BYF] = bY[at(g, mi, mj)];
+        else
+            v[BYF] = bY_yghost(g, bX, bY, row2, i, j);
         // all reads of this thread precede its writes; a ghost cell is never
         // read by the boundary fill, so the in-place update is race free.
 #pragma unroll

@@ -20,7 +20,7 @@ struct Grid {
     long long plane;     // doubles per field plane = nx * pitch
     double dx, dy;
     double gamma, cfl, eps, eta;
-    int bc;
+    int bc_x, bc_y;      // Bc of the x walls (i) and the y walls (j)
 };
 
 // Device-side control block (one per solver), zero-initialised at create.

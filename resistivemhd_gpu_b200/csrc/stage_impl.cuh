@@ -441,6 +441,16 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
             if (STAGE == 1) oo[O_EMF * SG] = fov[1] + h * (eZ0 + eZ1);
         }
     }
+    // Stage 2 reads U^n only in the update: issue those loads now, so their
+    // latency overlaps the barrier wait of the CTA's slower warps.
+    double un_h[6];
+    if (STAGE == 2 && own) {
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const int f = n == 0 ? RHO : n == 1 ? MX : n == 2 ? MY : n == 3 ? MZ : n == 4 ? BZF : EN;
+            un_h[n] = a.un[f * PL + k];
+        }
+    }
     __syncthreads();
 
     const double dtdx = dt / g.dx, dtdy = dt / g.dy;
@@ -501,7 +511,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
         if (own) {
 #pragma unroll
             for (int n = 0; n < 6; ++n) {
-                const double u = a.un[fld[n] * PL + k];
+                const double u = un_h[n];
                 const double ub = uo[fld[n] * UF];
                 nv[fld[n]] = 0.5 * (u + ub - dtdx * dF(n) - dtdy * dG(n));
             }

@@ -64,9 +64,10 @@ class Setup:
     eps: float
     eta: float                   # scalar eta (uniform resistivity and the dt limit)
     eta_table: np.ndarray | None  # (nx, ny) cell-centred eta, or None for uniform
-    bc: str                      # "periodic" or "symmetric"
+    bc: str                      # x walls: "periodic" or "symmetric"
     xmin: float = 0.0
     ymin: float = 0.0
+    bc_y: str | None = None      # y walls, None for the same as bc
 
     @property
     def nx(self) -> int:
@@ -188,7 +189,8 @@ def plasmoid_sheet(n: int = 8192, m: int = 4096, **kw) -> Setup:
 
 
 def random_smooth_state(n: int, m: int, seed: int = 7, bc: str = "periodic", amp: float = 0.05,
-                        eta: float = 2e-3, with_table: bool = False, gamma: float = 5.0 / 3.0) -> Setup:
+                        eta: float = 2e-3, with_table: bool = False, gamma: float = 5.0 / 3.0,
+                        bc_y: str | None = None) -> Setup:
     """Generic smooth, positive, divergence-free state for parity tests on
     small and ragged grids: every field varies in both directions and carries
     a little noise, so every branch of the solver is exercised."""
@@ -218,4 +220,4 @@ def random_smooth_state(n: int, m: int, seed: int = 7, bc: str = "periodic", amp
         tab = np.ascontiguousarray(eta * (1.0 + 0.5 * np.sin(tw * xc) ** 2 * np.cos(tw * yc / 1.3) ** 2)
                                    * np.ones((nx, ny)))
     return Setup("random_smooth", _pack(rho, u, v, w, bx, by, bz, e), dx, dy, gamma, 0.4, 1e-20,
-                 float(eta * 1.5) if with_table else eta, tab, bc)
+                 float(eta * 1.5) if with_table else eta, tab, bc, bc_y=bc_y)

@@ -33,18 +33,19 @@ class Solver:
     ``stream`` may be a CUDA stream handle (int) to enqueue on."""
 
     def __init__(self, nx: int, ny: int, dx: float, dy: float, *, gamma: float = 5.0 / 3.0, cfl: float = 0.4,
-                 eps: float = 1e-20, eta: float = 0.0, bc: str = "periodic", precision: str = "fp64_exact",
-                 device: int = 0, stream: int | None = None):
+                 eps: float = 1e-20, eta: float = 0.0, bc: str = "periodic", bc_y: str | None = None,
+                 precision: str = "fp64_exact", device: int = 0, stream: int | None = None):
         lib = _lib.load()
         cfg = _lib.Config()
         lib.rmhd2d_config_default(ctypes.byref(cfg))
         cfg.nx, cfg.ny, cfg.dx, cfg.dy = int(nx), int(ny), float(dx), float(dy)
         cfg.gamma_mhd, cfg.cfl, cfg.eps, cfg.eta = float(gamma), float(cfl), float(eps), float(eta)
-        if bc not in _lib.BC:
-            raise ValueError(f"unknown boundary kind {bc!r}")
+        if bc not in _lib.BC or (bc_y is not None and bc_y not in _lib.BC):
+            raise ValueError(f"unknown boundary kind {bc!r} / {bc_y!r}")
         if precision not in _lib.PRECISION:
             raise ValueError(f"unknown precision {precision!r}")
         cfg.bc = _lib.BC[bc]
+        cfg.bc_y = -1 if bc_y is None else _lib.BC[bc_y]
         cfg.precision = _lib.PRECISION[precision]
         cfg.device = int(device)
         cfg.stream = stream
@@ -53,13 +54,13 @@ class Solver:
         self._lib = lib
         self._h = h
         self.nx, self.ny = int(nx), int(ny)
-        self.bc, self.precision = bc, precision
+        self.bc, self.bc_y, self.precision = bc, (bc if bc_y is None else bc_y), precision
 
     @classmethod
     def from_setup(cls, setup, precision: str = "fp64_exact", device: int = 0, apply_boundary: bool = True,
                    stream: int | None = None) -> "Solver":
         s = cls(setup.nx, setup.ny, setup.dx, setup.dy, gamma=setup.gamma, cfl=setup.cfl, eps=setup.eps,
-                eta=setup.eta, bc=setup.bc, precision=precision, device=device, stream=stream)
+                eta=setup.eta, bc=setup.bc, bc_y=setup.bc_y, precision=precision, device=device, stream=stream)
         if setup.eta_table is not None:
             s.set_eta_table(setup.eta_table)
         s.set_state(setup.state, apply_boundary=apply_boundary)
@@ -193,9 +194,9 @@ class ResistiveMHD2D:
     globals (const.hpp:20-23)."""
 
     def __init__(self, nx: int, ny: int, dx: float, dy: float, *, gamma_mhd: float = 5.0 / 3.0, CFL: float = 0.4,
-                 EPS: float = 1e-20, eta: float = 0.0, boundary: str = "periodic", eta_table=None,
-                 precision: str = "fp64_exact", device: int = 0):
-        self._s = Solver(nx, ny, dx, dy, gamma=gamma_mhd, cfl=CFL, eps=EPS, eta=eta, bc=boundary,
+                 EPS: float = 1e-20, eta: float = 0.0, boundary: str = "periodic", boundary_y: str | None = None,
+                 eta_table=None, precision: str = "fp64_exact", device: int = 0):
+        self._s = Solver(nx, ny, dx, dy, gamma=gamma_mhd, cfl=CFL, eps=EPS, eta=eta, bc=boundary, bc_y=boundary_y,
                          precision=precision, device=device)
         if eta_table is not None:
             self._s.set_eta_table(eta_table)
@@ -219,6 +220,9 @@ class ResistiveMHD2D:
         self._upload()
 
     def oneStepRK2(self) -> None:
+        """One RK2 step with the configured walls (the reference's oneStepRK2,
+        or oneStepRK2PeriodicXSymmetricY with boundary='periodic',
+        boundary_y='symmetric')."""
         self._s.step()
         self.dt = self._s.dt
         self.totalTime = self._s.total_time

@@ -82,6 +82,23 @@ def test_exact_bitwise_vs_oracle(gpu, oracle, bc, table, shape):
     assert np.array_equal(out, ref, equal_nan=True)
 
 
+@pytest.mark.parametrize("bc,bc_y,table,shape", [
+    ("periodic", "symmetric", False, (40, 33)),   # oneStepRK2PeriodicXSymmetricY
+    ("periodic", "symmetric", True, (17, 70)),
+    ("symmetric", "periodic", False, (35, 38)),
+])
+def test_mixed_walls_bitwise_vs_oracle(gpu, oracle, bc, bc_y, table, shape):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(*shape, seed=8, bc=bc, bc_y=bc_y, with_table=table)
+    ref, rdts, crashed_at = oracle.run(s, s.state, 8)
+    assert crashed_at == -1
+    out, cdts, _, crashed = run_cuda(s, 8)
+    assert not crashed
+    assert np.array_equal(cdts, rdts)
+    assert np.array_equal(out, ref)
+
+
 @pytest.mark.parametrize("bc,table,shape", CASES[:4])
 def test_fast_within_tolerance(gpu, oracle, bc, table, shape):
     from resistivemhd_gpu_b200 import setups
