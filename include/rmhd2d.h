@@ -165,6 +165,36 @@ int rmhd2d_load(rmhd2d_solver *s, const char *path);
    save/load round trip and by host tools. */
 int rmhd2d_write_snapshot(const char *path, const double *host_state, int nx, int ny);
 
+/* Tile shape of the fused stage kernels (0: 8x32 / 9x32 cells, 1: 16x16 /
+   18x16).  rmhd2d_autotune times trial_steps steps with each shape (the
+   state is restored afterwards) and keeps the fastest.  No counterpart in the
+   reference (its launches are fixed 16x16 thread blocks). */
+int rmhd2d_set_tile_shape(rmhd2d_solver *s, int shape);
+int rmhd2d_get_tile_shape(const rmhd2d_solver *s, int *shape);
+int rmhd2d_autotune(rmhd2d_solver *s, int trial_steps, int *best_shape);
+
+/* Batches of independent runs (grid size, eta, boundary kinds per run; one
+   precision and device per batch), stepped together: every RK2 stage of all
+   runs is one persistent launch over a table of all runs' tiles, captured in
+   a CUDA graph.  No counterpart in the reference (one run per process).
+   Each run is an rmhd2d_solver owned by the batch: use rmhd2d_batch_member
+   with the per-solver functions for its state, eta table, dt, total time,
+   crash flag and snapshots; stepping and destroying go through the batch. */
+typedef struct rmhd2d_batch rmhd2d_batch;
+int rmhd2d_batch_create(const rmhd2d_config *cfgs, int nruns, rmhd2d_batch **out);
+int rmhd2d_batch_destroy(rmhd2d_batch *b);
+int rmhd2d_batch_size(const rmhd2d_batch *b, int *nruns);
+int rmhd2d_batch_member(rmhd2d_batch *b, int run, rmhd2d_solver **member);
+int rmhd2d_batch_run(rmhd2d_batch *b, int nsteps);
+int rmhd2d_batch_run_timed(rmhd2d_batch *b, int nsteps, float *ms);
+/* Launch configuration: tile shape (0..1) and persistent CTAs per SM (1..2);
+   rmhd2d_batch_autotune times each (state restored afterwards) and keeps the
+   fastest. */
+int rmhd2d_batch_set_launch(rmhd2d_batch *b, int shape, int ctas_per_sm);
+int rmhd2d_batch_get_launch(const rmhd2d_batch *b, int *shape, int *ctas_per_sm);
+int rmhd2d_batch_autotune(rmhd2d_batch *b, int trial_steps, int *best_shape, int *best_ctas_per_sm);
+const char *rmhd2d_batch_last_error(const rmhd2d_batch *b);
+
 /* Text of the last error of this solver (or of the last failed create when
    s is NULL); never NULL. */
 const char *rmhd2d_last_error(const rmhd2d_solver *s);

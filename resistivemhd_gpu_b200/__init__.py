@@ -6,7 +6,7 @@ resistive term, Heun RK2 with a fused CFL reduction), exposed through the C
 ABI in include/rmhd2d.h (librmhd2d.so, built in this directory) and the
 Python mirror below.
 """
-from .solver import ResistiveMHD2D, Solver, read_snapshot, write_snapshot  # noqa: F401
+from .solver import Batch, ResistiveMHD2D, Solver, read_snapshot, write_snapshot  # noqa: F401
 from . import setups  # noqa: F401
 
-__all__ = ["ResistiveMHD2D", "Solver", "read_snapshot", "write_snapshot", "setups"]
+__all__ = ["Batch", "ResistiveMHD2D", "Solver", "read_snapshot", "write_snapshot", "setups"]

@@ -56,6 +56,20 @@ SIGNATURES = [
     ("rmhd2d_save", ctypes.c_int, [_S, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
     ("rmhd2d_load", ctypes.c_int, [_S, ctypes.c_char_p]),
     ("rmhd2d_write_snapshot", ctypes.c_int, [ctypes.c_char_p, _D, ctypes.c_int, ctypes.c_int]),
+    ("rmhd2d_set_tile_shape", ctypes.c_int, [_S, ctypes.c_int]),
+    ("rmhd2d_get_tile_shape", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_int)]),
+    ("rmhd2d_autotune", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("rmhd2d_batch_create", ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("rmhd2d_batch_destroy", ctypes.c_int, [_S]),
+    ("rmhd2d_batch_size", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_int)]),
+    ("rmhd2d_batch_member", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("rmhd2d_batch_run", ctypes.c_int, [_S, ctypes.c_int]),
+    ("rmhd2d_batch_run_timed", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    ("rmhd2d_batch_set_launch", ctypes.c_int, [_S, ctypes.c_int, ctypes.c_int]),
+    ("rmhd2d_batch_get_launch", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    ("rmhd2d_batch_autotune", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int)]),
+    ("rmhd2d_batch_last_error", ctypes.c_char_p, [_S]),
     ("rmhd2d_last_error", ctypes.c_char_p, [_S]),
     ("rmhd2d_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("rmhd2d_abi_version", ctypes.c_int, []),
@@ -92,4 +106,10 @@ class RMHDError(RuntimeError):
 def check(status: int, handle=None) -> None:
     if status != OK:
         msg = load().rmhd2d_last_error(handle)
+        raise RMHDError(status, msg.decode() if msg else "")
+
+
+def check_batch(status: int, handle=None) -> None:
+    if status != OK:
+        msg = load().rmhd2d_batch_last_error(handle)
         raise RMHDError(status, msg.decode() if msg else "")

@@ -41,8 +41,11 @@ struct rmhd2d_solver {
     double *row2 = nullptr;      // nx doubles
     Control *ctl = nullptr;      // device control block
     Control *ctl_host = nullptr; // pinned mirror for readback
-    CUtensorMap mapA{}, mapB{};          // stage-1 source A, stage-2 source B (box rows per stage)
-    CUtensorMap mapE1{}, mapE2{};        // eta plane, stage-1 / stage-2 boxes
+    // per tile shape: stage-1 source A, stage-2 source B, eta plane with the
+    // stage-1 and stage-2 boxes
+    CUtensorMap mapA[NSHAPE]{}, mapB[NSHAPE]{}, mapE1[NSHAPE]{}, mapE2[NSHAPE]{};
+    int shape = 0;
+    void *batch = nullptr;               // owning batch, if any
     int parity = 0;
     bool has_state = false;
     long long steps = 0;
@@ -87,14 +90,14 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-// 3-D tensor map over one state: (j: ny, i: nx, field: 8), box (UJ, ui, 8).
-bool encode_state_map(CUtensorMap *map, const Grid &g, double *base, int ui)
+// 3-D tensor map over one state: (j: ny, i: nx, field: 8), box (uj, ui, 8).
+bool encode_state_map(CUtensorMap *map, const Grid &g, double *base, int ui, int uj)
 {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[3] = {(cuuint64_t)g.ny, (cuuint64_t)g.nx, (cuuint64_t)NFIELD};
     cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.plane * 8};
-    cuuint32_t box[3] = {(cuuint32_t)UJ, (cuuint32_t)ui, (cuuint32_t)NFIELD};
+    cuuint32_t box[3] = {(cuuint32_t)uj, (cuuint32_t)ui, (cuuint32_t)NFIELD};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -102,14 +105,14 @@ bool encode_state_map(CUtensorMap *map, const Grid &g, double *base, int ui)
     return r == CUDA_SUCCESS;
 }
 
-// 2-D tensor map over the eta plane: (j: ny, i: nx), box (UJ, ui).
-bool encode_eta_map(CUtensorMap *map, const Grid &g, double *base, int ui)
+// 2-D tensor map over the eta plane: (j: ny, i: nx), box (uj, ui).
+bool encode_eta_map(CUtensorMap *map, const Grid &g, double *base, int ui, int uj)
 {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[2] = {(cuuint64_t)g.ny, (cuuint64_t)g.nx};
     cuuint64_t strides[1] = {(cuuint64_t)g.pitch * 8};
-    cuuint32_t box[2] = {(cuuint32_t)UJ, (cuuint32_t)ui};
+    cuuint32_t box[2] = {(cuuint32_t)uj, (cuuint32_t)ui};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -146,7 +149,9 @@ int do_boundary(rmhd2d_solver *s)
     return RMHD2D_OK;
 }
 
-using StageLauncher = void (*)(int, const CUtensorMap *, const CUtensorMap *, const StageArgs &, cudaStream_t);
+using StageLauncher = void (*)(int, int, const CUtensorMap *, const CUtensorMap *, const StageArgs &, cudaStream_t);
+using BatchLauncher = void (*)(int, int, const BatchRun *, const CUtensorMap *, const TileRef *, int, int, int,
+                               cudaStream_t);
 
 StageLauncher stage_launcher(int precision)
 {
@@ -154,6 +159,15 @@ StageLauncher stage_launcher(int precision)
     case RMHD2D_FP64_FAST: return fast::launch_stage;
     case RMHD2D_FP32_BULK: return bulk32::launch_stage;
     default: return exact::launch_stage;
+    }
+}
+
+BatchLauncher batch_launcher(int precision)
+{
+    switch (precision) {
+    case RMHD2D_FP64_FAST: return fast::launch_stage_batch;
+    case RMHD2D_FP32_BULK: return bulk32::launch_stage_batch;
+    default: return exact::launch_stage_batch;
     }
 }
 
@@ -170,13 +184,13 @@ void enqueue_step(rmhd2d_solver *s, int parity)
     a.src = s->A;
     a.un = s->A;
     a.dst = s->B;
-    launch(1, &s->mapA, &s->mapE1, a, s->stream);
+    launch(1, s->shape, &s->mapA[s->shape], &s->mapE1[s->shape], a, s->stream);
     launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
     // stage 2: (U*, U^n) -> U^{n+1} in A
     a.src = s->B;
     a.un = s->A;
     a.dst = s->A;
-    launch(2, &s->mapB, &s->mapE2, a, s->stream);
+    launch(2, s->shape, &s->mapB[s->shape], &s->mapE2[s->shape], a, s->stream);
     launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
 }
 
@@ -313,15 +327,25 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
         cudaMemset(s->row2, 0, (size_t)g.nx * sizeof(double)) != cudaSuccess ||
         cudaMemset(s->ctl, 0, sizeof(Control)) != cudaSuccess)
         return bail(RMHD2D_ERR_CUDA, "device memset failed");
-    if (!encode_state_map(&s->mapA, g, s->A, stage_ui(1)) || !encode_state_map(&s->mapB, g, s->B, stage_ui(2)))
-        return bail(RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    for (int sh = 0; sh < NSHAPE; ++sh)
+        if (!encode_state_map(&s->mapA[sh], g, s->A, stage_ui(1, sh), shape_uj(sh)) ||
+            !encode_state_map(&s->mapB[sh], g, s->B, stage_ui(2, sh), shape_uj(sh)))
+            return bail(RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     *out = s;
     return RMHD2D_OK;
 }
 
+static int destroy_solver(rmhd2d_solver *s);
+
 int rmhd2d_destroy(rmhd2d_solver *s)
 {
     if (!s) return RMHD2D_OK;
+    if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: destroy the batch");
+    return destroy_solver(s);
+}
+
+static int destroy_solver(rmhd2d_solver *s)
+{
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     destroy_graphs(s);
@@ -381,8 +405,11 @@ int rmhd2d_set_eta_table(rmhd2d_solver *s, const double *host_eta)
     if (!s->eta) {
         CK(cudaMalloc(&s->eta, (size_t)s->g.plane * sizeof(double)));
         CK(cudaMemsetAsync(s->eta, 0, (size_t)s->g.plane * sizeof(double), s->stream));
-        if (!encode_eta_map(&s->mapE1, s->g, s->eta, stage_ui(1)) ||
-            !encode_eta_map(&s->mapE2, s->g, s->eta, stage_ui(2))) {
+        bool ok = true;
+        for (int sh = 0; sh < NSHAPE; ++sh)
+            ok = ok && encode_eta_map(&s->mapE1[sh], s->g, s->eta, stage_ui(1, sh), shape_uj(sh)) &&
+                 encode_eta_map(&s->mapE2[sh], s->g, s->eta, stage_ui(2, sh), shape_uj(sh));
+        if (!ok) {
             cudaFree(s->eta);
             s->eta = nullptr;
             return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the eta table");
@@ -419,6 +446,7 @@ int rmhd2d_calculate_dt(rmhd2d_solver *s, double *dt)
 int rmhd2d_step_rk2(rmhd2d_solver *s)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
     enqueue_step(s, s->parity);
@@ -431,6 +459,7 @@ int rmhd2d_step_rk2(rmhd2d_solver *s)
 int rmhd2d_run(rmhd2d_solver *s, int nsteps)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (nsteps < 0) return fail(s, RMHD2D_ERR_INVALID, "nsteps < 0");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
@@ -480,6 +509,7 @@ int rmhd2d_run_timed(rmhd2d_solver *s, int nsteps, float *ms)
 int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
 {
     if (!s || !ms4) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
     cudaEvent_t ev[5];
@@ -494,12 +524,12 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
     auto launch = stage_launcher(s->cfg.precision);
     CK(cudaEventRecord(ev[0], s->stream));
     a.src = s->A; a.un = s->A; a.dst = s->B;
-    launch(1, &s->mapA, &s->mapE1, a, s->stream);
+    launch(1, s->shape, &s->mapA[s->shape], &s->mapE1[s->shape], a, s->stream);
     CK(cudaEventRecord(ev[1], s->stream));
     launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
     CK(cudaEventRecord(ev[2], s->stream));
     a.src = s->B; a.un = s->A; a.dst = s->A;
-    launch(2, &s->mapB, &s->mapE2, a, s->stream);
+    launch(2, s->shape, &s->mapB[s->shape], &s->mapE2[s->shape], a, s->stream);
     CK(cudaEventRecord(ev[3], s->stream));
     launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
     CK(cudaEventRecord(ev[4], s->stream));
@@ -584,6 +614,420 @@ int rmhd2d_load(rmhd2d_solver *s, const char *path)
     int rc = rmhd2d_set_state(s, h.data(), 0);
     if (rc) return rc;
     return sync_and_check(s);
+}
+
+
+// ---------------------------------------------------------------------------
+// Tile shape and autotuning of one solver
+// ---------------------------------------------------------------------------
+
+int rmhd2d_set_tile_shape(rmhd2d_solver *s, int shape)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (shape < 0 || shape >= NSHAPE) return fail(s, RMHD2D_ERR_INVALID, "unknown tile shape");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    destroy_graphs(s);
+    s->shape = shape;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_get_tile_shape(const rmhd2d_solver *s, int *shape)
+{
+    if (!s || !shape) return RMHD2D_ERR_INVALID;
+    *shape = s->shape;
+    return RMHD2D_OK;
+}
+
+// Saves the user-visible state (A and the control block) of a solver so that
+// trial steps can be undone.
+struct Snapshot {
+    double *A = nullptr;
+    Control ctl{};
+    int parity = 0;
+    long long steps = 0;
+};
+
+static int snapshot_take(rmhd2d_solver *s, Snapshot &sn)
+{
+    const size_t bytes = (size_t)s->g.plane * NFIELD * sizeof(double);
+    CK(cudaMalloc(&sn.A, bytes));
+    CK(cudaMemcpyAsync(sn.A, s->A, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync(&sn.ctl, s->ctl, sizeof(Control), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    sn.parity = s->parity;
+    sn.steps = s->steps;
+    return RMHD2D_OK;
+}
+
+static int snapshot_restore(rmhd2d_solver *s, Snapshot &sn)
+{
+    const size_t bytes = (size_t)s->g.plane * NFIELD * sizeof(double);
+    CK(cudaMemcpyAsync(s->A, sn.A, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->ctl, &sn.ctl, sizeof(Control), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    cudaFree(sn.A);
+    sn.A = nullptr;
+    s->parity = sn.parity;
+    s->steps = sn.steps;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_autotune(rmhd2d_solver *s, int trial_steps, int *best_shape)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: tune the batch");
+    if (trial_steps < 2) trial_steps = 2;
+    trial_steps += trial_steps & 1;   // even: the step parity comes back
+    CK(cudaSetDevice(s->device));
+    Snapshot sn;
+    int rc = snapshot_take(s, sn);
+    if (rc) return rc;
+    float best = 1e30f;
+    int best_sh = s->shape;
+    for (int sh = 0; sh < NSHAPE && rc == RMHD2D_OK; ++sh) {
+        rc = rmhd2d_set_tile_shape(s, sh);
+        float warm = 0.f, ms = 0.f;
+        if (!rc) rc = rmhd2d_run_timed(s, 2, &warm);             // graph capture + warm-up
+        if (!rc) rc = rmhd2d_run_timed(s, trial_steps, &ms);
+        if (!rc && ms < best) {
+            best = ms;
+            best_sh = sh;
+        }
+    }
+    const int rc2 = snapshot_restore(s, sn);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    rc = rmhd2d_set_tile_shape(s, best_sh);
+    if (best_shape) *best_shape = best_sh;
+    return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches of independent runs
+// ---------------------------------------------------------------------------
+
+struct rmhd2d_batch {
+    std::vector<rmhd2d_solver *> runs;
+    int device = 0;
+    int precision = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int nsm = 148;
+    int shape = 0;
+    int ctas_per_sm = 2;
+    int parity = 0;
+    long long steps = 0;
+    long long max_ghost = 0;
+    BatchRun *d_runs = nullptr;
+    CUtensorMap *d_maps = nullptr;            // MAPS_PER_RUN per run, for the current shape
+    TileRef *d_tiles[2] = {nullptr, nullptr}; // stage 1 / stage 2 tile tables
+    int ntiles[2] = {0, 0};
+    bool dirty = true;
+    cudaGraphExec_t graph2[2] = {nullptr, nullptr};
+    std::string err;
+};
+
+namespace {
+
+int bfail(rmhd2d_batch *b, int code, const std::string &msg)
+{
+    if (b) b->err = msg;
+    else {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_create_err = msg;
+    }
+    return code;
+}
+
+#define BCK(call)                                                                                 \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return bfail(b, RMHD2D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void batch_drop_graphs(rmhd2d_batch *b)
+{
+    for (auto &g : b->graph2) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+// (Re)builds the device run records, tensor maps and tile tables.
+int batch_build(rmhd2d_batch *b)
+{
+    if (!b->dirty) return RMHD2D_OK;
+    BCK(cudaStreamSynchronize(b->stream));
+    batch_drop_graphs(b);
+    const int n = (int)b->runs.size();
+    std::vector<BatchRun> runs(n);
+    std::vector<CUtensorMap> maps((size_t)n * MAPS_PER_RUN);
+    std::vector<TileRef> tiles[2];
+    b->max_ghost = 0;
+    for (int r = 0; r < n; ++r) {
+        rmhd2d_solver *s = b->runs[r];
+        if (!s->has_state) return bfail(b, RMHD2D_ERR_STATE, "run " + std::to_string(r) + " has no state");
+        runs[r] = BatchRun{s->g, s->A, s->B, s->eta, s->row2, s->ctl};
+        maps[(size_t)r * MAPS_PER_RUN + 0] = s->mapA[b->shape];
+        maps[(size_t)r * MAPS_PER_RUN + 1] = s->mapB[b->shape];
+        maps[(size_t)r * MAPS_PER_RUN + 2] = s->mapE1[b->shape];
+        maps[(size_t)r * MAPS_PER_RUN + 3] = s->mapE2[b->shape];
+        const long long ng = 6LL * s->g.ny + 6LL * (s->g.nx - 6);
+        b->max_ghost = ng > b->max_ghost ? ng : b->max_ghost;
+        for (int st = 1; st <= 2; ++st) {
+            const int ti = stage_ti(st, b->shape), tj = shape_tj(b->shape);
+            const int nti = (s->g.nx - 2 * HALO + ti - 1) / ti, ntj = (s->g.ny - 2 * HALO + tj - 1) / tj;
+            for (int a = 0; a < nti; ++a)
+                for (int c = 0; c < ntj; ++c) tiles[st - 1].push_back(TileRef{r, a, c, 0});
+        }
+    }
+    cudaFree(b->d_runs);
+    cudaFree(b->d_maps);
+    b->d_runs = nullptr;
+    b->d_maps = nullptr;
+    BCK(cudaMalloc(&b->d_runs, sizeof(BatchRun) * n));
+    BCK(cudaMalloc(&b->d_maps, sizeof(CUtensorMap) * maps.size()));
+    BCK(cudaMemcpy(b->d_runs, runs.data(), sizeof(BatchRun) * n, cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice));
+    for (int st = 0; st < 2; ++st) {
+        cudaFree(b->d_tiles[st]);
+        b->d_tiles[st] = nullptr;
+        b->ntiles[st] = (int)tiles[st].size();
+        BCK(cudaMalloc(&b->d_tiles[st], sizeof(TileRef) * tiles[st].size()));
+        BCK(cudaMemcpy(b->d_tiles[st], tiles[st].data(), sizeof(TileRef) * tiles[st].size(), cudaMemcpyHostToDevice));
+    }
+    b->dirty = false;
+    return RMHD2D_OK;
+}
+
+void batch_enqueue_step(rmhd2d_batch *b, int parity)
+{
+    auto launch = batch_launcher(b->precision);
+    const int n = (int)b->runs.size();
+    const int ctas = b->nsm * b->ctas_per_sm;
+    launch(1, b->shape, b->d_runs, b->d_maps, b->d_tiles[0], b->ntiles[0], ctas, parity, b->stream);
+    launch_boundary_batch(b->d_runs, n, b->max_ghost, 0, 0, b->stream);
+    launch(2, b->shape, b->d_runs, b->d_maps, b->d_tiles[1], b->ntiles[1], ctas, parity, b->stream);
+    launch_boundary_batch(b->d_runs, n, b->max_ghost, 1, parity ^ 1, b->stream);
+}
+
+void batch_advance(rmhd2d_batch *b, int nsteps)
+{
+    b->steps += nsteps;
+    if (nsteps & 1) b->parity ^= 1;
+    for (auto *s : b->runs) {
+        s->parity = b->parity;
+        s->steps += nsteps;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int rmhd2d_batch_create(const rmhd2d_config *cfgs, int nruns, rmhd2d_batch **out)
+{
+    rmhd2d_batch *b = nullptr;
+    if (!cfgs || !out || nruns <= 0) return bfail(b, RMHD2D_ERR_INVALID, "bad batch arguments");
+    *out = nullptr;
+    for (int r = 1; r < nruns; ++r)
+        if (cfgs[r].precision != cfgs[0].precision || cfgs[r].device != cfgs[0].device)
+            return bfail(b, RMHD2D_ERR_INVALID, "all runs of a batch share precision and device");
+    b = new rmhd2d_batch();
+    b->device = cfgs[0].device;
+    b->precision = cfgs[0].precision;
+    auto bail = [&](int code, const std::string &msg) {
+        {
+            std::lock_guard<std::mutex> lk(g_err_mu);
+            g_create_err = msg;
+        }
+        rmhd2d_batch_destroy(b);
+        return code;
+    };
+    if (cudaSetDevice(b->device) != cudaSuccess) return bail(RMHD2D_ERR_NO_DEVICE, "cudaSetDevice failed");
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, b->device) == cudaSuccess) b->nsm = prop.multiProcessorCount;
+    if (cfgs[0].stream) {
+        b->stream = (cudaStream_t)cfgs[0].stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(RMHD2D_ERR_CUDA, "cudaStreamCreate failed");
+        b->own_stream = true;
+    }
+    for (int r = 0; r < nruns; ++r) {
+        rmhd2d_config c = cfgs[r];
+        c.stream = b->stream;
+        rmhd2d_solver *s = nullptr;
+        const int rc = rmhd2d_create(&c, &s);
+        if (rc) return bail(rc, std::string("run ") + std::to_string(r) + ": " + rmhd2d_last_error(nullptr));
+        s->batch = b;
+        b->runs.push_back(s);
+    }
+    *out = b;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_batch_destroy(rmhd2d_batch *b)
+{
+    if (!b) return RMHD2D_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graphs(b);
+    for (auto *s : b->runs) {
+        s->batch = nullptr;
+        destroy_solver(s);
+    }
+    cudaFree(b->d_runs);
+    cudaFree(b->d_maps);
+    cudaFree(b->d_tiles[0]);
+    cudaFree(b->d_tiles[1]);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_batch_size(const rmhd2d_batch *b, int *nruns)
+{
+    if (!b || !nruns) return RMHD2D_ERR_INVALID;
+    *nruns = (int)b->runs.size();
+    return RMHD2D_OK;
+}
+
+int rmhd2d_batch_member(rmhd2d_batch *b, int run, rmhd2d_solver **out)
+{
+    if (!b || !out) return bfail(b, RMHD2D_ERR_INVALID, "null argument");
+    if (run < 0 || run >= (int)b->runs.size()) return bfail(b, RMHD2D_ERR_INVALID, "run index out of range");
+    *out = b->runs[run];
+    // state, eta tables or shape may change through the member: rebuild on the next step
+    b->dirty = true;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_batch_set_launch(rmhd2d_batch *b, int shape, int ctas_per_sm)
+{
+    if (!b) return bfail(b, RMHD2D_ERR_INVALID, "null batch");
+    if (shape < 0 || shape >= NSHAPE || ctas_per_sm < 1 || ctas_per_sm > 2)
+        return bfail(b, RMHD2D_ERR_INVALID, "tile shape must be 0..1 and CTAs per SM 1..2");
+    b->shape = shape;
+    b->ctas_per_sm = ctas_per_sm;
+    b->dirty = true;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_batch_get_launch(const rmhd2d_batch *b, int *shape, int *ctas_per_sm)
+{
+    if (!b) return RMHD2D_ERR_INVALID;
+    if (shape) *shape = b->shape;
+    if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_batch_run(rmhd2d_batch *b, int nsteps)
+{
+    if (!b) return bfail(b, RMHD2D_ERR_INVALID, "null batch");
+    if (nsteps < 0) return bfail(b, RMHD2D_ERR_INVALID, "nsteps < 0");
+    BCK(cudaSetDevice(b->device));
+    int rc = batch_build(b);
+    if (rc) return rc;
+    while (nsteps >= 2) {
+        cudaGraphExec_t &ge = b->graph2[b->parity];
+        if (!ge) {
+            cudaGraph_t graph = nullptr;
+            BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            batch_enqueue_step(b, b->parity);
+            batch_enqueue_step(b, b->parity ^ 1);
+            cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+            if (e != cudaSuccess) return bfail(b, RMHD2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&ge, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                ge = nullptr;
+                return bfail(b, RMHD2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            }
+        }
+        BCK(cudaGraphLaunch(ge, b->stream));
+        batch_advance(b, 2);
+        nsteps -= 2;
+    }
+    if (nsteps == 1) {
+        batch_enqueue_step(b, b->parity);
+        BCK(cudaGetLastError());
+        batch_advance(b, 1);
+    }
+    return RMHD2D_OK;
+}
+
+int rmhd2d_batch_run_timed(rmhd2d_batch *b, int nsteps, float *ms)
+{
+    if (!b || !ms) return bfail(b, RMHD2D_ERR_INVALID, "null argument");
+    BCK(cudaSetDevice(b->device));
+    int rc = batch_build(b);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    BCK(cudaEventRecord(e0, b->stream));
+    rc = rmhd2d_batch_run(b, nsteps);
+    BCK(cudaEventRecord(e1, b->stream));
+    BCK(cudaEventSynchronize(e1));
+    BCK(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    for (auto *s : b->runs) {
+        const int r2 = sync_and_check(s);
+        if (r2) return bfail(b, r2, rmhd2d_last_error(s));
+    }
+    return RMHD2D_OK;
+}
+
+int rmhd2d_batch_autotune(rmhd2d_batch *b, int trial_steps, int *best_shape, int *best_ctas_per_sm)
+{
+    if (!b) return bfail(b, RMHD2D_ERR_INVALID, "null batch");
+    if (trial_steps < 2) trial_steps = 2;
+    trial_steps += trial_steps & 1;   // even: the step parity comes back
+    BCK(cudaSetDevice(b->device));
+    std::vector<Snapshot> sn(b->runs.size());
+    for (size_t r = 0; r < b->runs.size(); ++r) {
+        const int rc = snapshot_take(b->runs[r], sn[r]);
+        if (rc) return bfail(b, rc, rmhd2d_last_error(b->runs[r]));
+    }
+    const int par0 = b->parity;
+    const long long steps0 = b->steps;
+    float best = 1e30f;
+    int bs = b->shape, bc = b->ctas_per_sm, rc = RMHD2D_OK;
+    for (int sh = 0; sh < NSHAPE && !rc; ++sh)
+        for (int c = 1; c <= 2 && !rc; ++c) {
+            rc = rmhd2d_batch_set_launch(b, sh, c);
+            float warm = 0.f, ms = 0.f;
+            if (!rc) rc = rmhd2d_batch_run_timed(b, 2, &warm);
+            if (!rc) rc = rmhd2d_batch_run_timed(b, trial_steps, &ms);
+            if (!rc && ms < best) {
+                best = ms;
+                bs = sh;
+                bc = c;
+            }
+        }
+    for (size_t r = 0; r < b->runs.size(); ++r) snapshot_restore(b->runs[r], sn[r]);
+    b->parity = par0;
+    b->steps = steps0;
+    if (rc) return rc;
+    rc = rmhd2d_batch_set_launch(b, bs, bc);
+    if (best_shape) *best_shape = bs;
+    if (best_ctas_per_sm) *best_ctas_per_sm = bc;
+    return rc;
+}
+
+const char *rmhd2d_batch_last_error(const rmhd2d_batch *b)
+{
+    if (b) return b->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_create_err.c_str();
 }
 
 }  // extern "C"

@@ -116,61 +116,92 @@ __device__ __forceinline__ void ghost_cell(const Grid &g, long long t, int &i, i
     }
 }
 
-// Fills every ghost cell of `s` from its interior (and, for symmetric x
+// Fills ghost cell number t of `s` from its interior (and, for symmetric x
 // walls, the CT'd lower-wall bY row), with the exact results of the
 // reference's x pass followed by its y pass, each periodic
-// (boundary.cu:4-141) or symmetric (TS boundary.cu:4-206).
-// With `ctl` set it also folds the ghost cells' CFL rate and NaN-energy test
-// into the reductions of the stage-2 kernel.
+// (boundary.cu:4-141) or symmetric (TS boundary.cu:4-206).  Returns the
+// cell's CFL rate bits and NaN-energy flag when `rate` is set.
+__device__ __forceinline__ void fill_ghost(const Grid &g, double *s, const double *row2, long long t, bool rate,
+                                           unsigned long long &bits, int &nan_e, bool &cell0_nan)
+{
+    int i, j;
+    ghost_cell(g, t, i, j);
+    const long long P = g.plane;
+    const long long k = at(g, i, j);
+    double v[8];
+    // hydro fields: the image of the x pass, then of the y pass
+    const int mi = image(i, g.nx, g.bc_x), mj = image(j, g.ny, g.bc_y);
+    const long long src = at(g, mi, mj);
+    const int hydro[6] = {RHO, MX, MY, MZ, BZF, EN};
+#pragma unroll
+    for (int n = 0; n < 6; ++n) v[hydro[n]] = s[hydro[n] * P + src];
+    const double *bX = s + BXF * P, *bY = s + BYF * P;
+    // bX: x pass (copy or integration), then the y pass copies rows
+    v[BXF] = bX_afterx(g, bX, bY, row2, i, mj);
+    // bY: x pass copies columns, then the y pass copies or integrates rows
+    if ((j >= 3 && j < g.ny - 3) || g.bc_y == BC_PERIODIC)
+        v[BYF] = bY[at(g, mi, mj)];
+    else
+        v[BYF] = bY_yghost(g, bX, bY, row2, i, j);
+    // all reads of this thread precede its writes; a ghost cell is never
+    // read by the boundary fill, so the in-place update is race free.
+#pragma unroll
+    for (int f = 0; f < 8; ++f) s[f * P + k] = v[f];
+    if (rate) {
+        const double r = cfl_rate(v[RHO], v[MX], v[MY], v[MZ], v[BXF], v[BYF], v[BZF], v[EN], g.gamma, g.dx, g.dy);
+        bits = rate_bits(r);
+        nan_e = v[EN] != v[EN];
+        cell0_nan = (i == 0 && j == 0 && r != r);
+    }
+}
+
+__device__ __forceinline__ void reduce_ghost_rates(Control *ctl, int slot, unsigned long long bits, int nan_e,
+                                                   bool cell0_nan)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
+        bits = o > bits ? o : bits;
+    }
+    const int any_nan = __any_sync(0xffffffffu, nan_e);
+    if (cell0_nan) ctl->first_nan[slot] = 1;
+    if ((threadIdx.x & 31) == 0) {
+        if (bits) atomicMax(&ctl->amax[slot], bits);
+        if (any_nan) atomicExch(&ctl->crashed, 1);
+    }
+}
+
+// Every ghost cell of one run.  With `ctl` set it also folds the ghost
+// cells' CFL rate and NaN-energy test into the reductions of the stage-2
+// kernel (slot = the next step's parity).
 __global__ void boundary_kernel(Grid g, double *s, const double *row2, Control *ctl, int slot)
 {
     const long long nghost = 6LL * g.ny + 6LL * (g.nx - 6);
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long bits = 0ull;
     int nan_e = 0;
-    if (t < nghost) {
-        int i, j;
-        ghost_cell(g, t, i, j);
-        const long long P = g.plane;
-        const long long k = at(g, i, j);
-        double v[8];
-        // hydro fields: the image of the x pass, then of the y pass
-        const int mi = image(i, g.nx, g.bc_x), mj = image(j, g.ny, g.bc_y);
-        const long long src = at(g, mi, mj);
-        const int hydro[6] = {RHO, MX, MY, MZ, BZF, EN};
-#pragma unroll
-        for (int n = 0; n < 6; ++n) v[hydro[n]] = s[hydro[n] * P + src];
-        const double *bX = s + BXF * P, *bY = s + BYF * P;
-        // bX: x pass (copy or integration), then the y pass copies rows
-        v[BXF] = bX_afterx(g, bX, bY, row2, i, mj);
-        // bY: x pass copies columns, then the y pass copies or integrates rows
-        if ((j >= 3 && j < g.ny - 3) || g.bc_y == BC_PERIODIC)
-            v[BYF] = bY[at(g, mi, mj)];
-        else
-            v[BYF] = bY_yghost(g, bX, bY, row2, i, j);
-        // all reads of this thread precede its writes; a ghost cell is never
-        // read by the boundary fill, so the in-place update is race free.
-#pragma unroll
-        for (int f = 0; f < 8; ++f) s[f * P + k] = v[f];
-        if (ctl) {
-            const double r = cfl_rate(v[RHO], v[MX], v[MY], v[MZ], v[BXF], v[BYF], v[BZF], v[EN], g.gamma, g.dx, g.dy);
-            bits = rate_bits(r);
-            nan_e = v[EN] != v[EN];
-            if (i == 0 && j == 0 && r != r) ctl->first_nan[slot] = 1;
-        }
-    }
-    if (ctl) {
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
-            bits = o > bits ? o : bits;
-        }
-        const int any_nan = __any_sync(0xffffffffu, nan_e);
-        if ((threadIdx.x & 31) == 0) {
-            if (bits) atomicMax(&ctl->amax[slot], bits);
-            if (any_nan) atomicExch(&ctl->crashed, 1);
-        }
-    }
+    bool c0 = false;
+    if (t < nghost) fill_ghost(g, s, row2, t, ctl != nullptr, bits, nan_e, c0);
+    if (ctl) reduce_ghost_rates(ctl, slot, bits, nan_e, c0);
+}
+
+// Every ghost cell of every run of a batch (blockIdx.y = run); `which`
+// selects the state (0: B after stage 1, 1: A after stage 2 with the CFL
+// and NaN reductions).
+__global__ void boundary_batch_kernel(const BatchRun *runs, int which, int slot)
+{
+    const BatchRun &r = runs[blockIdx.y];
+    const Grid &g = r.g;
+    const long long nghost = 6LL * g.ny + 6LL * (g.nx - 6);
+    const long long first = (long long)blockIdx.x * blockDim.x;
+    if (first >= nghost) return;   // whole warp-aligned block beyond this run
+    const long long t = first + threadIdx.x;
+    unsigned long long bits = 0ull;
+    int nan_e = 0;
+    bool c0 = false;
+    const bool rate = which == 1;
+    if (t < nghost) fill_ghost(g, which == 1 ? r.A : r.B, r.row2, t, rate, bits, nan_e, c0);
+    if (rate) reduce_ghost_rates(r.ctl, slot, bits, nan_e, c0);
 }
 
 // Copies the lower-wall face row bY(i, 2) into row2 (used when the boundary
@@ -260,6 +291,13 @@ void launch_boundary(const Grid &g, double *s, const double *row2, Control *ctl,
     const int threads = 256;
     const int blocks = (int)((nghost + threads - 1) / threads);
     boundary_kernel<<<blocks, threads, 0, st>>>(g, s, row2, ctl, slot);
+}
+
+void launch_boundary_batch(const BatchRun *runs, int nruns, long long max_ghost, int which, int slot, cudaStream_t st)
+{
+    const int threads = 256;
+    const dim3 grid((unsigned)((max_ghost + threads - 1) / threads), (unsigned)nruns);
+    boundary_batch_kernel<<<grid, threads, 0, st>>>(runs, which, slot);
 }
 
 void launch_snapshot_row2(const Grid &g, const double *s, double *row2, cudaStream_t st)

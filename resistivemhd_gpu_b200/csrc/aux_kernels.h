@@ -9,6 +9,7 @@
 namespace rmhd2d {
 
 void launch_boundary(const Grid &g, double *s, const double *row2, Control *ctl, int slot, cudaStream_t st);
+void launch_boundary_batch(const BatchRun *runs, int nruns, long long max_ghost, int which, int slot, cudaStream_t st);
 void launch_snapshot_row2(const Grid &g, const double *s, double *row2, cudaStream_t st);
 void launch_rate(const Grid &g, const double *s, Control *ctl, int slot, int set_crash, cudaStream_t st);
 void launch_aos_to_planes(const Grid &g, const double *aos, double *s, cudaStream_t st);

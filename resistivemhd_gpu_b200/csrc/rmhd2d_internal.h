@@ -37,18 +37,31 @@ enum KernelError { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };
 
 // Tiles of the fused stage kernels: TI cells along x (i) by TJ along y (j).
 // Stage 1 also computes the ring of fluxes its corner EMF needs, stage 2
-// only the tile's own interfaces, so their best tile heights differ: with
-// 320 threads stage 1 (8 x 32) has 636 interfaces and stage 2 (9 x 32) 617,
-// two nearly full rounds each.
-constexpr int TJ = 32;
+// only the tile's own interfaces, so their best tile heights differ.  With
+// 320 threads both shapes fill two nearly full rounds of interfaces:
+//   shape 0: stage 1  8 x 32 (636 interfaces), stage 2  9 x 32 (617)
+//   shape 1: stage 1 16 x 16 (612 interfaces), stage 2 18 x 16 (610)
 constexpr int HALO = 3;
-constexpr int STAGE1_TI = 8;
-constexpr int STAGE2_TI = 9;
-constexpr int UJ = TJ + 2 * HALO;  // staged columns (TMA inner box: UJ * 8 bytes, multiple of 16)
+constexpr int NSHAPE = 2;
 constexpr int STAGE_THREADS = 320;
-static_assert(STAGE_THREADS >= STAGE1_TI * TJ && STAGE_THREADS >= STAGE2_TI * TJ,
-              "one thread per tile cell in the update phase");
-constexpr int stage_ti(int stage) { return stage == 1 ? STAGE1_TI : STAGE2_TI; }
-constexpr int stage_ui(int stage) { return stage_ti(stage) + 2 * HALO; }
+constexpr int shape_tj(int shape) { return shape == 0 ? 32 : 16; }
+constexpr int stage_ti(int stage, int shape) { return shape == 0 ? (stage == 1 ? 8 : 9) : (stage == 1 ? 16 : 18); }
+constexpr int stage_ui(int stage, int shape) { return stage_ti(stage, shape) + 2 * HALO; }
+constexpr int shape_uj(int shape) { return shape_tj(shape) + 2 * HALO; }  // TMA inner box: UJ * 8 B, a multiple of 16
+static_assert(STAGE_THREADS >= 9 * 32 && STAGE_THREADS >= 18 * 16, "one thread per tile cell in the update phase");
+
+// Per-run record of a batch (device memory), and one entry of a batch's tile
+// table.
+struct BatchRun {
+    Grid g;
+    double *A, *B, *eta, *row2;
+    Control *ctl;
+};
+struct TileRef {
+    int run, ti, tj, pad;
+};
+// Tensor maps of one run in a batch: [stage-1 state A, stage-2 state B,
+// stage-1 eta, stage-2 eta].
+constexpr int MAPS_PER_RUN = 4;
 
 }  // namespace rmhd2d

@@ -43,24 +43,30 @@ struct StageArgs {
     int parity;          // step parity: dt from ctl->amax[parity]
 };
 
-// One launcher per variant (stage_exact.cu, stage_fast.cu).
+// One set of launchers per variant (stage_exact.cu, stage_fast.cu, stage_bulk32.cu).
 namespace exact {
-void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
+void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream);
-size_t stage_smem_bytes(int stage);
-int stage_regs(int stage);
+void launch_stage_batch(int stage, int shape, const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles,
+                        int ntiles, int ctas, int parity, cudaStream_t stream);
+size_t stage_smem_bytes(int stage, int shape);
+int stage_regs(int stage, int shape);
 }  // namespace exact
 namespace fast {
-void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
+void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream);
-size_t stage_smem_bytes(int stage);
-int stage_regs(int stage);
+void launch_stage_batch(int stage, int shape, const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles,
+                        int ntiles, int ctas, int parity, cudaStream_t stream);
+size_t stage_smem_bytes(int stage, int shape);
+int stage_regs(int stage, int shape);
 }  // namespace fast
 namespace bulk32 {
-void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
+void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream);
-size_t stage_smem_bytes(int stage);
-int stage_regs(int stage);
+void launch_stage_batch(int stage, int shape, const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles,
+                        int ntiles, int ctas, int parity, cudaStream_t stream);
+size_t stage_smem_bytes(int stage, int shape);
+int stage_regs(int stage, int shape);
 }  // namespace bulk32
 
 }  // namespace rmhd2d

@@ -35,9 +35,11 @@ namespace RMHD_VARIANT {
 // Gm, Go                 the same for the y fluxes at j+1/2 (Go slot 3: the bX flux)
 // Stage 1 needs x fluxes on rows j0-1..j0+TJ and y fluxes on columns
 // i0-1..i0+TI for its corner EMF; stage 2 only the tile's own interfaces.
-template <int STAGE> struct Tile {
+template <int STAGE, int SHAPE> struct Tile {
     using Real = RMHD_REAL;                                  // flux-side arithmetic type
-    static constexpr int TI = stage_ti(STAGE);
+    static constexpr int TI = stage_ti(STAGE, SHAPE);
+    static constexpr int TJ = shape_tj(SHAPE);
+    static constexpr int UJ = shape_uj(SHAPE);
     static constexpr int UI = TI + 2 * HALO;
     static constexpr int PI_ = TI + 4, PJ_ = TJ + 4;
     static constexpr int RI_ = TI + 2, RJ_ = TJ + 2;
@@ -130,16 +132,20 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase)
     return false;
 }
 
-template <int STAGE>
-__global__ void __launch_bounds__(STAGE_THREADS, 2)
-stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap emap,
-             const StageArgs a)
+// One tile of one stage: TMA-stage the tile and its halo, then the primitive,
+// eta*J, flux, EMF and update phases.  (ti, tj) is the tile index of the
+// run, `phase` the parity of the CTA's mbarrier for this tile's load, and
+// ctl_tile marks the tile that updates the run's control block.  Returns
+// false when the bounded wait for the staged tile expired (the CTA must stop).
+template <int STAGE, int SHAPE>
+__device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &a,
+                                           int ti, int tj, bool ctl_tile, unsigned char *smem_raw,
+                                           uint64_t *bar, uint32_t phase)
 {
-    using T = Tile<STAGE>;
+    using T = Tile<STAGE, SHAPE>;
     using Real = typename T::Real;
-    constexpr int TI = T::TI, UF = T::UF, PF = T::PF, RF = T::RF, SF = T::SF, SG = T::SG;
+    constexpr int TI = T::TI, TJ = T::TJ, UJ = T::UJ, UF = T::UF, PF = T::PF, RF = T::RF, SF = T::SF, SG = T::SG;
     constexpr int PJ_ = T::PJ_, RJ_ = T::RJ_, F_NJ = T::F_NJ, G_NJ = T::G_NJ, EJ_ = T::EJ_;
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
     double *Ut = reinterpret_cast<double *>(smem_raw);
     double *Et = reinterpret_cast<double *>(smem_raw + T::OFF_E);
     Real *Pv = reinterpret_cast<Real *>(smem_raw + T::OFF_PV);
@@ -150,38 +156,33 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     Real *Fo = reinterpret_cast<Real *>(smem_raw + T::OFF_FO);
     double *Gm = reinterpret_cast<double *>(smem_raw + T::OFF_GM);
     Real *Go = reinterpret_cast<Real *>(smem_raw + T::OFF_GO);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::OFF_BAR);
 
     const Grid &g = a.g;
     const int tid = threadIdx.x;
-    const int j0 = HALO + blockIdx.x * TJ;
-    const int i0 = HALO + blockIdx.y * TI;
+    const int j0 = HALO + tj * TJ;
+    const int i0 = HALO + ti * TI;
     const bool has_eta = a.eta != nullptr;
 
     // ---- stage the tile + halo: one 3-D TMA load of all 8 field planes
     // (and one 2-D load of the eta table) ----
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        // order this CTA's earlier shared-memory accesses before the async copy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-    __syncthreads();
-    if (tid == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                      ::"r"(smem_addr(bar)), "r"(T::U_BYTES + (has_eta ? T::E_BYTES : 0u)) : "memory");
-        // x coordinate (j) = j0 - 3 = blockIdx.x * TJ: a multiple of TJ, so
+        // x coordinate (j) = j0 - 3 = tj * TJ: a multiple of TJ (even), so
         // 16-byte aligned in the global tensor as TMA requires.
         asm volatile(
             "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
             " [%0], [%1, {%3, %4, %5}], [%2];"
-            ::"r"(smem_addr(Ut)), "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(smem_addr(bar)),
+            ::"r"(smem_addr(Ut)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(smem_addr(bar)),
               "r"(j0 - HALO), "r"(i0 - HALO), "r"(0)
             : "memory");
         if (has_eta)
             asm volatile(
                 "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
                 " [%0], [%1, {%3, %4}], [%2];"
-                ::"r"(smem_addr(Et)), "l"(reinterpret_cast<uint64_t>(&emap)), "r"(smem_addr(bar)),
+                ::"r"(smem_addr(Et)), "l"(reinterpret_cast<uint64_t>(emap)), "r"(smem_addr(bar)),
                   "r"(j0 - HALO), "r"(i0 - HALO)
                 : "memory");
     }
@@ -203,7 +204,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     // dt of this step from the CFL reduction of the previous state
     // (resistiveMHD_2D.cu:277-291), identical in every thread.
     const double dt = step_dt(a.ctl->amax[a.parity], a.ctl->first_nan[a.parity], g.dx, g.dy, g.eps, g.eta, g.cfl);
-    if (STAGE == 1 && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+    if (STAGE == 1 && ctl_tile && tid == 0) {
         a.ctl->dt = dt;
         a.ctl->total_time = a.ctl->total_time + dt;
         a.ctl->amax[a.parity ^ 1] = 0ull;
@@ -214,13 +215,13 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     // Every thread waits (bounded) for the staged tile; the CTA gives up as a
     // whole if any wait expired, after one more bounded wait for the copy in
     // flight, and reports it in the control block.
-    const bool staged = mbar_wait_bounded(bar, 0);
+    const bool staged = mbar_wait_bounded(bar, phase);
     if (__syncthreads_or(!staged)) {
         if (tid == 0) {
             atomicExch(&a.ctl->error, (int)KERR_TMA_TIMEOUT);
-            mbar_wait_bounded(bar, 0);
+            mbar_wait_bounded(bar, phase);
         }
-        return;
+        return false;
     }
 
     const double gm = g.gamma, EPS = g.eps;
@@ -551,30 +552,122 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
             if (any_nan) atomicExch(&a.ctl->crashed, 1);
         }
     }
+    return true;
 }
 
-size_t stage_smem_bytes(int stage) { return stage == 1 ? Tile<1>::SMEM_BYTES : Tile<2>::SMEM_BYTES; }
+__device__ __forceinline__ void init_tile_barrier(uint64_t *bar)
+{
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+}
 
-int stage_regs(int stage)
+// One CTA per tile of one run.
+template <int STAGE, int SHAPE>
+__global__ void __launch_bounds__(STAGE_THREADS, 2)
+stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap emap,
+             const StageArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    using T = Tile<STAGE, SHAPE>;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::OFF_BAR);
+    init_tile_barrier(bar);
+    stage_tile<STAGE, SHAPE>(&tmap, &emap, a, blockIdx.y, blockIdx.x, blockIdx.x == 0 && blockIdx.y == 0, smem_raw,
+                             bar, 0);
+}
+
+// Persistent CTAs over the tile table of a batch of independent runs (each
+// with its own grid, eta, state buffers, tensor maps and control block).
+template <int STAGE, int SHAPE>
+__global__ void __launch_bounds__(STAGE_THREADS, 2)
+stage_batch_kernel(const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles, int ntiles, int parity)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    using T = Tile<STAGE, SHAPE>;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::OFF_BAR);
+    init_tile_barrier(bar);
+    uint32_t phase = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const TileRef tr = tiles[t];
+        const BatchRun &r = runs[tr.run];
+        StageArgs a;
+        a.g = r.g;
+        a.src = STAGE == 1 ? r.A : r.B;
+        a.un = r.A;
+        a.dst = STAGE == 1 ? r.B : r.A;
+        a.eta = r.eta;
+        a.row2 = r.g.bc_x == BC_SYMMETRIC ? r.row2 : nullptr;
+        a.ctl = r.ctl;
+        a.parity = parity;
+        const CUtensorMap *m = maps + (size_t)tr.run * MAPS_PER_RUN;
+        if (!stage_tile<STAGE, SHAPE>(m + (STAGE - 1), m + 2 + (STAGE - 1), a, tr.ti, tr.tj,
+                                      tr.ti == 0 && tr.tj == 0, smem_raw, bar, phase))
+            return;
+        phase ^= 1;
+        __syncthreads();   // every thread is done with this tile's shared memory
+    }
+}
+
+template <int STAGE, int SHAPE> constexpr size_t smem_of() { return Tile<STAGE, SHAPE>::SMEM_BYTES; }
+
+size_t stage_smem_bytes(int stage, int shape)
+{
+    if (shape == 0) return stage == 1 ? smem_of<1, 0>() : smem_of<2, 0>();
+    return stage == 1 ? smem_of<1, 1>() : smem_of<2, 1>();
+}
+
+int stage_regs(int stage, int shape)
 {
     cudaFuncAttributes attr{};
-    cudaFuncGetAttributes(&attr, stage == 1 ? (const void *)stage_kernel<1> : (const void *)stage_kernel<2>);
+    const void *f = shape == 0 ? (stage == 1 ? (const void *)stage_kernel<1, 0> : (const void *)stage_kernel<2, 0>)
+                               : (stage == 1 ? (const void *)stage_kernel<1, 1> : (const void *)stage_kernel<2, 1>);
+    cudaFuncGetAttributes(&attr, f);
     return attr.numRegs;
 }
 
-void launch_stage(int stage, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
+template <int STAGE, int SHAPE>
+static void launch_one(const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args, cudaStream_t stream)
+{
+    using T = Tile<STAGE, SHAPE>;
+    cudaFuncSetAttribute(stage_kernel<STAGE, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_BYTES);
+    const dim3 grid((args.g.ny - 2 * HALO + T::TJ - 1) / T::TJ, (args.g.nx - 2 * HALO + T::TI - 1) / T::TI);
+    stage_kernel<STAGE, SHAPE><<<grid, STAGE_THREADS, T::SMEM_BYTES, stream>>>(*tmap, *emap, args);
+}
+
+void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream)
 {
-    if (stage == 1) {
-        constexpr size_t sm = Tile<1>::SMEM_BYTES;
-        cudaFuncSetAttribute(stage_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        const dim3 grid((args.g.ny - 2 * HALO + TJ - 1) / TJ, (args.g.nx - 2 * HALO + Tile<1>::TI - 1) / Tile<1>::TI);
-        stage_kernel<1><<<grid, STAGE_THREADS, sm, stream>>>(*tmap, *emap, args);
+    if (shape == 0) {
+        if (stage == 1) launch_one<1, 0>(tmap, emap, args, stream);
+        else launch_one<2, 0>(tmap, emap, args, stream);
     } else {
-        constexpr size_t sm = Tile<2>::SMEM_BYTES;
-        cudaFuncSetAttribute(stage_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        const dim3 grid((args.g.ny - 2 * HALO + TJ - 1) / TJ, (args.g.nx - 2 * HALO + Tile<2>::TI - 1) / Tile<2>::TI);
-        stage_kernel<2><<<grid, STAGE_THREADS, sm, stream>>>(*tmap, *emap, args);
+        if (stage == 1) launch_one<1, 1>(tmap, emap, args, stream);
+        else launch_one<2, 1>(tmap, emap, args, stream);
+    }
+}
+
+template <int STAGE, int SHAPE>
+static void launch_batch_one(const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles, int ntiles,
+                             int ctas, int parity, cudaStream_t stream)
+{
+    using T = Tile<STAGE, SHAPE>;
+    cudaFuncSetAttribute(stage_batch_kernel<STAGE, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)T::SMEM_BYTES);
+    stage_batch_kernel<STAGE, SHAPE><<<ctas, STAGE_THREADS, T::SMEM_BYTES, stream>>>(runs, maps, tiles, ntiles, parity);
+}
+
+void launch_stage_batch(int stage, int shape, const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles,
+                        int ntiles, int ctas, int parity, cudaStream_t stream)
+{
+    if (shape == 0) {
+        if (stage == 1) launch_batch_one<1, 0>(runs, maps, tiles, ntiles, ctas, parity, stream);
+        else launch_batch_one<2, 0>(runs, maps, tiles, ntiles, ctas, parity, stream);
+    } else {
+        if (stage == 1) launch_batch_one<1, 1>(runs, maps, tiles, ntiles, ctas, parity, stream);
+        else launch_batch_one<2, 1>(runs, maps, tiles, ntiles, ctas, parity, stream);
     }
 }
 

@@ -53,8 +53,33 @@ class Solver:
         _lib.check(lib.rmhd2d_create(ctypes.byref(cfg), ctypes.byref(h)), None)
         self._lib = lib
         self._h = h
+        self._owned = True
         self.nx, self.ny = int(nx), int(ny)
         self.bc, self.bc_y, self.precision = bc, (bc if bc_y is None else bc_y), precision
+
+    @staticmethod
+    def make_config(nx, ny, dx, dy, *, gamma=5.0 / 3.0, cfl=0.4, eps=1e-20, eta=0.0, bc="periodic", bc_y=None,
+                    precision="fp64_exact", device=0) -> "_lib.Config":
+        lib = _lib.load()
+        cfg = _lib.Config()
+        lib.rmhd2d_config_default(ctypes.byref(cfg))
+        cfg.nx, cfg.ny, cfg.dx, cfg.dy = int(nx), int(ny), float(dx), float(dy)
+        cfg.gamma_mhd, cfg.cfl, cfg.eps, cfg.eta = float(gamma), float(cfl), float(eps), float(eta)
+        cfg.bc = _lib.BC[bc]
+        cfg.bc_y = -1 if bc_y is None else _lib.BC[bc_y]
+        cfg.precision = _lib.PRECISION[precision]
+        cfg.device = int(device)
+        return cfg
+
+    @classmethod
+    def _member(cls, handle: ctypes.c_void_p, nx: int, ny: int) -> "Solver":
+        """Non-owning view of a batch member."""
+        s = cls.__new__(cls)
+        s._lib = _lib.load()
+        s._h = handle
+        s._owned = False
+        s.nx, s.ny = int(nx), int(ny)
+        return s
 
     @classmethod
     def from_setup(cls, setup, precision: str = "fp64_exact", device: int = 0, apply_boundary: bool = True,
@@ -69,7 +94,8 @@ class Solver:
     # -- lifetime --
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
-            self._lib.rmhd2d_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self._lib.rmhd2d_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
@@ -129,6 +155,21 @@ class Solver:
     def run(self, nsteps: int) -> None:
         self._ck(self._lib.rmhd2d_run(self._h, int(nsteps)))
 
+    def set_tile_shape(self, shape: int) -> None:
+        self._ck(self._lib.rmhd2d_set_tile_shape(self._h, int(shape)))
+
+    @property
+    def tile_shape(self) -> int:
+        v = ctypes.c_int()
+        self._ck(self._lib.rmhd2d_get_tile_shape(self._h, ctypes.byref(v)))
+        return v.value
+
+    def autotune(self, trial_steps: int = 4) -> int:
+        """Times each tile shape (state restored) and keeps the fastest."""
+        v = ctypes.c_int()
+        self._ck(self._lib.rmhd2d_autotune(self._h, int(trial_steps), ctypes.byref(v)))
+        return v.value
+
     def run_timed(self, nsteps: int) -> float:
         """run(nsteps) timed with CUDA events on the solver's stream; ms."""
         ms = ctypes.c_float()
@@ -165,6 +206,84 @@ class Solver:
 
     def load(self, path: str) -> None:
         self._ck(self._lib.rmhd2d_load(self._h, os.fsencode(path)))
+
+
+class Batch:
+    """Independent runs (own grid size, eta, walls) stepped together: each
+    RK2 stage of all runs is one persistent launch over all their tiles,
+    replayed from a CUDA graph.  ``batch[r]`` is a (non-owning) Solver view of
+    run r for its state, eta table, dt, crash flag and snapshots."""
+
+    def __init__(self, setups, precision: str = "fp64_exact", device: int = 0, apply_boundary: bool = True):
+        lib = _lib.load()
+        cfgs = (_lib.Config * len(setups))()
+        for r, s in enumerate(setups):
+            cfgs[r] = Solver.make_config(s.nx, s.ny, s.dx, s.dy, gamma=s.gamma, cfl=s.cfl, eps=s.eps, eta=s.eta,
+                                         bc=s.bc, bc_y=s.bc_y, precision=precision, device=device)
+        h = ctypes.c_void_p()
+        _lib.check_batch(lib.rmhd2d_batch_create(cfgs, len(setups), ctypes.byref(h)), None)
+        self._lib, self._h = lib, h
+        self.members = []
+        for r, s in enumerate(setups):
+            mh = ctypes.c_void_p()
+            self._ck(lib.rmhd2d_batch_member(h, r, ctypes.byref(mh)))
+            m = Solver._member(mh, s.nx, s.ny)
+            if s.eta_table is not None:
+                m.set_eta_table(s.eta_table)
+            m.set_state(s.state, apply_boundary=apply_boundary)
+            self.members.append(m)
+
+    def _ck(self, st: int) -> None:
+        _lib.check_batch(st, self._h)
+
+    def __len__(self) -> int:
+        return len(self.members)
+
+    def __getitem__(self, r: int) -> Solver:
+        mh = ctypes.c_void_p()
+        self._ck(self._lib.rmhd2d_batch_member(self._h, int(r), ctypes.byref(mh)))
+        return self.members[r]
+
+    def run(self, nsteps: int) -> None:
+        self._ck(self._lib.rmhd2d_batch_run(self._h, int(nsteps)))
+
+    def run_timed(self, nsteps: int) -> float:
+        ms = ctypes.c_float()
+        self._ck(self._lib.rmhd2d_batch_run_timed(self._h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def set_launch(self, shape: int, ctas_per_sm: int) -> None:
+        self._ck(self._lib.rmhd2d_batch_set_launch(self._h, int(shape), int(ctas_per_sm)))
+
+    @property
+    def launch(self) -> tuple[int, int]:
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._ck(self._lib.rmhd2d_batch_get_launch(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def autotune(self, trial_steps: int = 4) -> tuple[int, int]:
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._ck(self._lib.rmhd2d_batch_autotune(self._h, int(trial_steps), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            for m in self.members:
+                m._h = ctypes.c_void_p()
+            self._lib.rmhd2d_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def write_snapshot(path: str, state: np.ndarray) -> None:

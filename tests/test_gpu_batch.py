@@ -1,0 +1,134 @@
+"""Tile shapes and batches of independent runs.
+
+The tile decomposition changes no arithmetic: every interface flux and cell
+update is computed by the same expressions whatever tile or launch holds it,
+so a batched run, or a run on the other tile shape, equals the single run bit
+for bit in both FP64 precisions.  The FP32-bulk variant is compiled with
+fast math and FMA contraction left to the compiler, which may contract its
+float core differently in the persistent batch kernel than in the single-run
+kernel; its batch is held to BULK_BATCH_REL_L1 of the single run (100 times
+inside the bulk variant's own 1e-5 bound against FP64)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PRECISIONS = ["fp64_exact", "fp64_fast", "fp32_bulk"]
+BULK_BATCH_REL_L1 = 1e-7
+
+
+def assert_same(got, ref, precision, what):
+    if precision != "fp32_bulk":
+        assert np.array_equal(got, ref), what
+        return
+    for f in range(8):
+        den = np.abs(ref[..., f]).sum()
+        err = np.abs(got[..., f] - ref[..., f]).sum() / max(den, 1e-300)
+        assert err <= BULK_BATCH_REL_L1, f"{what} field {f}: rel L1 {err:.3e}"
+
+
+def single(setup, nsteps, precision, shape=0):
+    from resistivemhd_gpu_b200 import Solver
+
+    with Solver.from_setup(setup, precision=precision) as s:
+        s.set_tile_shape(shape)
+        dts = []
+        for _ in range(nsteps):
+            s.step()
+            dts.append(s.dt)
+        return s.get_state(), np.array(dts), s.total_time
+
+
+def mixed_setups():
+    from resistivemhd_gpu_b200 import setups
+
+    return [
+        setups.random_smooth_state(40, 36, seed=1, bc="periodic"),
+        setups.random_smooth_state(23, 70, seed=2, bc="symmetric", with_table=True),
+        setups.orszag_tang(48),
+        setups.random_smooth_state(64, 17, seed=3, bc="periodic", bc_y="symmetric", eta=5e-3),
+        setups.harris_sheet(96, 48),
+    ]
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_tile_shape_1_equals_shape_0(gpu, precision):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(45, 39, seed=4, bc="symmetric", with_table=True)
+    a, da, _ = single(s, 6, precision, shape=0)
+    b, db, _ = single(s, 6, precision, shape=1)
+    assert np.array_equal(da, db)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("launch", [(0, 2), (1, 1)])
+def test_batch_equals_single_runs(gpu, precision, launch):
+    from resistivemhd_gpu_b200 import Batch
+
+    sets = mixed_setups()
+    refs = [single(s, 5, precision) for s in sets]
+    with Batch(sets, precision=precision) as b:
+        b.set_launch(*launch)
+        b.run(5)
+        for r, (ref, dts, total) in enumerate(refs):
+            m = b[r]
+            assert_same(m.get_state(), ref, precision, f"run {r}")
+            rel = 0.0 if precision != "fp32_bulk" else 1e-6
+            assert m.dt == pytest.approx(dts[-1], rel=rel, abs=0)
+            assert m.total_time == pytest.approx(total, rel=max(rel, 1e-15))
+            assert not m.check_crashed()
+
+
+def test_batch_odd_steps_and_graph_replay(gpu):
+    """Graph replays of 2 steps plus a single step keep every run in step."""
+    from resistivemhd_gpu_b200 import Batch
+
+    sets = mixed_setups()[:3]
+    refs = [single(s, 7, "fp64_exact") for s in sets]
+    with Batch(sets, precision="fp64_exact") as b:
+        b.run(3)
+        b.run(4)
+        for r, (ref, _, _) in enumerate(refs):
+            assert np.array_equal(b[r].get_state(), ref)
+
+
+def test_batch_autotune_restores_state(gpu):
+    from resistivemhd_gpu_b200 import Batch
+
+    sets = mixed_setups()
+    with Batch(sets, precision="fp64_fast") as b:
+        before = [b[r].get_state().copy() for r in range(len(b))]
+        shape, ctas = b.autotune(trial_steps=2)
+        assert shape in (0, 1) and ctas in (1, 2)
+        assert b.launch == (shape, ctas)
+        for r in range(len(b)):
+            assert np.array_equal(b[r].get_state(), before[r])
+        b.run(3)
+    refs = [single(s, 3, "fp64_fast") for s in sets]
+    with Batch(sets, precision="fp64_fast") as b:
+        b.set_launch(shape, ctas)
+        b.run(3)
+        for r, (ref, _, _) in enumerate(refs):
+            assert np.array_equal(b[r].get_state(), ref)
+
+
+def test_member_cannot_step_alone(gpu):
+    from resistivemhd_gpu_b200 import Batch, _lib
+
+    with Batch(mixed_setups()[:2]) as b:
+        with pytest.raises(_lib.RMHDError) as e:
+            b[0].step()
+        assert e.value.status == 4
+
+
+def test_solver_autotune(gpu):
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.harris_sheet(256, 128)
+    with Solver.from_setup(s, precision="fp64_fast") as sol:
+        before = sol.get_state().copy()
+        shape = sol.autotune(trial_steps=2)
+        assert shape in (0, 1) and sol.tile_shape == shape
+        assert np.array_equal(sol.get_state(), before)
