@@ -195,6 +195,34 @@ int rmhd2d_batch_get_launch(const rmhd2d_batch *b, int *shape, int *ctas_per_sm)
 int rmhd2d_batch_autotune(rmhd2d_batch *b, int trial_steps, int *best_shape, int *best_ctas_per_sm);
 const char *rmhd2d_batch_last_error(const rmhd2d_batch *b);
 
+/* CFL dt of a state held in the caller's own device memory, computed
+   without allocating device memory.  No counterpart in the reference: it is
+   the dt of ResistiveMHD2D::calculateDt() (TP resistiveMHD_2D.cu:277-291),
+   the same value rmhd2d_calculate_dt returns for a solver holding that
+   state, for callers that cannot allocate while they run: host codes whose
+   own pool or arena owns the device memory and hands out pointers only, and
+   checks made inside a time loop, where the cudaFree that a temporary
+   buffer needs would synchronise the whole device.
+
+   device_state: nx*ny cells in the layout above (ghosts included, every
+   cell is scanned), on device cfg->device.  Reads cfg->nx, ny, dx, dy,
+   gamma_mhd, cfl, eps, eta, device and stream (NULL: the default stream);
+   bc, bc_y and precision are ignored.  The work is enqueued on that stream,
+   which is synchronised before *dt is written.  The current device is
+   restored before returning.  Errors are reported by
+   rmhd2d_last_error(NULL).
+
+   Scratch is a fixed device array inside the library: grids with more than
+   RMHD2D_NOALLOC_MAX_CELLS cells (nx*ny) are rejected with
+   RMHD2D_ERR_INVALID.  The first call on each device looks up that array's
+   address (cudaGetSymbolAddress), which loads the library's module onto
+   the device; make that first call before any stream capture, e.g. once
+   at initialisation.  All calls on one device share the array: calls that
+   overlap in time (from several host threads) race and may return a wrong
+   dt. */
+#define RMHD2D_NOALLOC_MAX_CELLS 16777216
+int rmhd2d_calculate_dt_noalloc(const rmhd2d_config *cfg, const double *device_state, double *dt);
+
 /* Text of the last error of this solver (or of the last failed create when
    s is NULL); never NULL. */
 const char *rmhd2d_last_error(const rmhd2d_solver *s);

@@ -70,6 +70,8 @@ SIGNATURES = [
     ("rmhd2d_batch_autotune", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int)]),
     ("rmhd2d_batch_last_error", ctypes.c_char_p, [_S]),
+    ("rmhd2d_calculate_dt_noalloc", ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_void_p,
+                                                    ctypes.POINTER(ctypes.c_double)]),
     ("rmhd2d_last_error", ctypes.c_char_p, [_S]),
     ("rmhd2d_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("rmhd2d_abi_version", ctypes.c_int, []),

@@ -34,6 +34,7 @@ UNITS = {
     "stage_fast.cu": ["-fmad=true"],
     "stage_bulk32.cu": ["-fmad=true", "--use_fast_math"],
     "aux_kernels.cu": ["-fmad=false"],
+    "noalloc_dt.cu": ["-fmad=false"],
     "api.cu": ["-fmad=false"],
 }
 

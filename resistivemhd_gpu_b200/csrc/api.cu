@@ -23,6 +23,7 @@
 
 #include "../../include/rmhd2d.h"
 #include "aux_kernels.h"
+#include "noalloc_dt.h"
 #include "physics.cuh"
 #include "rmhd2d_internal.h"
 #include "stage.cuh"
@@ -1031,3 +1032,52 @@ const char *rmhd2d_batch_last_error(const rmhd2d_batch *b)
 }
 
 }  // extern "C"
+
+namespace {
+
+// Restores the calling thread's current device on scope exit.
+struct DeviceRestore {
+    int prev = -1;
+    ~DeviceRestore()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+int rmhd2d_calculate_dt_noalloc(const rmhd2d_config *cfg, const double *device_state, double *dt)
+{
+    rmhd2d_solver *s = nullptr;
+    if (!cfg || !device_state || !dt) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (cfg->nx < 12 || cfg->ny < 12) return fail(s, RMHD2D_ERR_INVALID, "nx and ny must be >= 12 (3 ghosts per side)");
+    const long long ncell = (long long)cfg->nx * cfg->ny;
+    if (ncell > RMHD2D_NOALLOC_MAX_CELLS)
+        return fail(s, RMHD2D_ERR_INVALID,
+                    "nx*ny = " + std::to_string(ncell) + " cells is above RMHD2D_NOALLOC_MAX_CELLS (" +
+                        std::to_string((long long)RMHD2D_NOALLOC_MAX_CELLS) +
+                        "), the size of the no-allocation scratch; use rmhd2d_calculate_dt on a solver");
+    if (!(cfg->dx > 0) || !(cfg->dy > 0)) return fail(s, RMHD2D_ERR_INVALID, "dx and dy must be positive");
+    if (!(cfg->gamma_mhd > 1.0)) return fail(s, RMHD2D_ERR_INVALID, "gamma_mhd must be > 1");
+    if (!(cfg->eta >= 0.0)) return fail(s, RMHD2D_ERR_INVALID, "eta must be >= 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
+        return fail(s, RMHD2D_ERR_NO_DEVICE, "no CUDA device with that ordinal");
+    DeviceRestore restore;
+    CK(cudaGetDevice(&restore.prev));
+    if (restore.prev == cfg->device) restore.prev = -1;
+    else CK(cudaSetDevice(cfg->device));
+    int major = 0, minor = 0;
+    CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, cfg->device));
+    CK(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, cfg->device));
+    if (major != 10 || minor != 0) return fail(s, RMHD2D_ERR_NO_DEVICE, "librmhd2d is built for sm_100a (B200) only");
+    unsigned long long *scratch = nullptr;
+    CK(noalloc_scratch(cfg->device, &scratch));
+    const cudaStream_t st = static_cast<cudaStream_t>(cfg->stream);
+    double out = 0.0;
+    CK(enqueue_dt_noalloc(device_state, ncell, cfg->gamma_mhd, cfg->dx, cfg->dy, cfg->eps, cfg->eta, cfg->cfl,
+                          scratch, &out, st));
+    CK(cudaStreamSynchronize(st));
+    *dt = out;
+    return RMHD2D_OK;
+}
