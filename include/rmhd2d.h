@@ -195,6 +195,43 @@ int rmhd2d_batch_get_launch(const rmhd2d_batch *b, int *shape, int *ctas_per_sm)
 int rmhd2d_batch_autotune(rmhd2d_batch *b, int trial_steps, int *best_shape, int *best_ctas_per_sm);
 const char *rmhd2d_batch_last_error(const rmhd2d_batch *b);
 
+/* Discrete adjoint of the step (no counterpart in the reference).
+   The adjoint differentiates the map from the initial state and the eta
+   field to the state after nsteps steps, with the dt of every step held at
+   its recorded value.  Branch points (minmod's choice, the HLLD region, the
+   clamped wave speeds) take the derivative of the branch the forward run
+   took.  The walls must be periodic in x and y.
+
+   rmhd2d_run_fixed_dt: nsteps steps with the given dts (host array)
+   instead of the CFL dt; the state, dt and total time advance as in
+   rmhd2d_run.  Used to evaluate the frozen-dt map, e.g. for finite
+   differences against the adjoint.
+
+   rmhd2d_adjoint_forward: nsteps steps from the current state (as
+   rmhd2d_run), recording each step's dt and keeping the state every
+   checkpoint_interval steps (0: ceil(sqrt(nsteps))).  Memory: about
+   (nsteps / interval + 2 * interval + 6) states of nx*ny*8 doubles.
+
+   rmhd2d_adjoint_dts: the nsteps dts recorded by the last forward run.
+
+   rmhd2d_adjoint_backward: given seed = dJ/dU_N (nx*ny*8 doubles, the
+   state layout above; host memory), writes dJ/dU_0 into grad_state, the
+   gradient with respect to the state passed to rmhd2d_set_state with
+   apply_boundary = 1 (ghost entries 0), and, when grad_eta is not NULL,
+   dJ/d eta into grad_eta (nx*ny, k = j + i*ny; the cell-centred eta field,
+   the table when one is set, else the uniform eta spread over the cells).
+   Each segment between checkpoints is recomputed once; the solver's state
+   is restored to U_N afterwards, so backward may be called again with
+   another seed.
+
+   rmhd2d_adjoint_release: frees the recorded trajectory and workspace. */
+int rmhd2d_run_fixed_dt(rmhd2d_solver *s, int nsteps, const double *host_dts);
+int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoint_interval);
+int rmhd2d_adjoint_dts(rmhd2d_solver *s, double *host_dts);
+int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed, double *host_grad_state,
+                            double *host_grad_eta);
+int rmhd2d_adjoint_release(rmhd2d_solver *s);
+
 /* CFL dt of a state held in the caller's own device memory, computed
    without allocating device memory.  No counterpart in the reference: it is
    the dt of ResistiveMHD2D::calculateDt() (TP resistiveMHD_2D.cu:277-291),

@@ -22,6 +22,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liborc.so"
+TANGENT_LIB = HERE / "libtangent.so"
 REF_DIR = HERE / "_ref"
 
 BC = {"periodic": 0, "symmetric": 1}
@@ -46,6 +47,65 @@ def build(verbose: bool = False) -> Path:
            "-Wall", "-o", str(LIB), str(src), "-lm"]
     subprocess.run(cmd, check=True, capture_output=not verbose)
     return LIB
+
+
+def build_tangent(verbose: bool = False) -> Path:
+    """Compile the templated restatement (rmhd2d_tangent.cpp) into
+    oracle/libtangent.so."""
+    src = HERE / "rmhd2d_tangent.cpp"
+    deps = [src, HERE / "rmhd2d_oracle.h"]
+    if TANGENT_LIB.exists() and TANGENT_LIB.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return TANGENT_LIB
+    cmd = ["g++", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
+           "-Wall", "-o", str(TANGENT_LIB), str(src), "-lm"]
+    subprocess.run(cmd, check=True, capture_output=not verbose)
+    return TANGENT_LIB
+
+
+class TangentLib:
+    """The oracle step as a template, on doubles with given dts and on dual
+    numbers: the exact directional derivative of the frozen-dt map, against
+    which the CUDA adjoint is checked."""
+
+    def __init__(self):
+        build_tangent()
+        self.lib = ctypes.CDLL(str(TANGENT_LIB))
+        P = ctypes.POINTER(_Params)
+        D = ctypes.POINTER(ctypes.c_double)
+        self.lib.orc_run_fixed_dt.argtypes = [P, D, ctypes.c_int, D, ctypes.c_int]
+        self.lib.orc_tangent_run.argtypes = [P, D, D, D, ctypes.c_int, D]
+        self.lib.orc_hlld_jvp.argtypes = [D, D, D, D, ctypes.c_double, ctypes.c_double, D, D]
+
+    @staticmethod
+    def _d(a):
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+    def run_fixed_dt(self, setup, state, dts, apply_boundary=True):
+        keep = []
+        p = OracleLib._params(setup, keep)
+        s = np.ascontiguousarray(state, dtype=np.float64).copy()
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        self.lib.orc_run_fixed_dt(ctypes.byref(p), self._d(s), len(d), self._d(d), int(bool(apply_boundary)))
+        return s
+
+    def tangent(self, setup, state, dstate, dts, deta=None):
+        """(U_N, dU_N) for the run from `state` (before its boundary) with the
+        given dts, along the direction (dstate, deta)."""
+        keep = []
+        p = OracleLib._params(setup, keep)
+        s = np.ascontiguousarray(state, dtype=np.float64).copy()
+        ds = np.ascontiguousarray(dstate, dtype=np.float64).copy()
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        de = None if deta is None else np.ascontiguousarray(deta, dtype=np.float64)
+        self.lib.orc_tangent_run(ctypes.byref(p), self._d(s), self._d(ds), None if de is None else self._d(de),
+                                 len(d), self._d(d))
+        return s, ds
+
+    def hlld_jvp(self, L, R, dL, dR, gamma, eps):
+        f, df = np.zeros(8), np.zeros(8)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (L, R, dL, dR)]
+        self.lib.orc_hlld_jvp(*[self._d(a) for a in arrs], gamma, eps, self._d(f), self._d(df))
+        return f, df
 
 
 class OracleLib:

@@ -70,6 +70,12 @@ SIGNATURES = [
     ("rmhd2d_batch_autotune", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int)]),
     ("rmhd2d_batch_last_error", ctypes.c_char_p, [_S]),
+    ("rmhd2d_run_fixed_dt", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    ("rmhd2d_adjoint_forward", ctypes.c_int, [_S, ctypes.c_int, ctypes.c_int]),
+    ("rmhd2d_adjoint_dts", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_double)]),
+    ("rmhd2d_adjoint_backward", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_double)]),
+    ("rmhd2d_adjoint_release", ctypes.c_int, [_S]),
     ("rmhd2d_calculate_dt_noalloc", ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_void_p,
                                                     ctypes.POINTER(ctypes.c_double)]),
     ("rmhd2d_last_error", ctypes.c_char_p, [_S]),

@@ -35,6 +35,7 @@ UNITS = {
     "stage_bulk32.cu": ["-fmad=true", "--use_fast_math"],
     "aux_kernels.cu": ["-fmad=false"],
     "noalloc_dt.cu": ["-fmad=false"],
+    "adjoint.cu": ["-fmad=false"],
     "api.cu": ["-fmad=false"],
 }
 

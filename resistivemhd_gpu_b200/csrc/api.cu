@@ -14,6 +14,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,6 +23,7 @@
 #include <vector>
 
 #include "../../include/rmhd2d.h"
+#include "adjoint.h"
 #include "aux_kernels.h"
 #include "noalloc_dt.h"
 #include "physics.cuh"
@@ -29,6 +31,8 @@
 #include "stage.cuh"
 
 using namespace rmhd2d;
+
+struct AdjointWork;
 
 struct rmhd2d_solver {
     rmhd2d_config cfg{};
@@ -51,7 +55,28 @@ struct rmhd2d_solver {
     bool has_state = false;
     long long steps = 0;
     cudaGraphExec_t graph2[2] = {nullptr, nullptr};
+    AdjointWork *adj = nullptr;          // recorded trajectory and workspace of the discrete adjoint
     std::string err;
+};
+
+// Trajectory of rmhd2d_adjoint_forward and the workspace of
+// rmhd2d_adjoint_backward (all device buffers are pitched like the state).
+struct AdjointWork {
+    int nsteps = 0, interval = 0, nseg = 0;
+    size_t state_doubles = 0;
+    double *ckpt = nullptr;          // nseg states: U at steps 0, interval, 2*interval, ...
+    double *seg0 = nullptr;          // interval states: U^n of each step of a segment (recomputed)
+    double *seg1 = nullptr;          // interval states: U* of each step of a segment (recomputed)
+    double *ub[3] = {nullptr, nullptr, nullptr};   // adjoint states
+    double *IF = nullptr;            // 32 planes
+    double *RJ = nullptr;            // 6 planes
+    double *tmp = nullptr;           // 2 planes
+    double *etab = nullptr;          // 1 plane
+    double *dts = nullptr;           // nsteps, device
+    std::vector<double> dts_host;
+    double *final_state = nullptr;   // U at the end of the forward run
+    double *aos = nullptr;           // nx*ny*8 staging for seeds and gradients
+    Control ctl_final{};
 };
 
 namespace {
@@ -207,6 +232,37 @@ int upload_from_device_aos(rmhd2d_solver *s, const double *aos_dev, int apply_bo
     return refresh_rate(s);
 }
 
+void free_adjoint(AdjointWork *w)
+{
+    if (!w) return;
+    cudaFree(w->ckpt);
+    cudaFree(w->seg0);
+    cudaFree(w->seg1);
+    for (double *p : w->ub) cudaFree(p);
+    cudaFree(w->IF);
+    cudaFree(w->RJ);
+    cudaFree(w->tmp);
+    cudaFree(w->etab);
+    cudaFree(w->dts);
+    cudaFree(w->final_state);
+    cudaFree(w->aos);
+    delete w;
+}
+
+// Sets or clears Control::use_fixed_dt in stream order.
+int set_fixed_dt_mode(rmhd2d_solver *s, int on)
+{
+    static const int kOn = 1, kOff = 0;
+    CK(cudaMemcpyAsync(&s->ctl->use_fixed_dt, on ? &kOn : &kOff, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    return RMHD2D_OK;
+}
+
+// A device buffer freed on scope exit.
+struct DeviceBuffer {
+    double *p = nullptr;
+    ~DeviceBuffer() { cudaFree(p); }
+};
+
 void destroy_graphs(rmhd2d_solver *s)
 {
     for (auto &gx : s->graph2) {
@@ -355,6 +411,7 @@ static int destroy_solver(rmhd2d_solver *s)
     cudaFree(s->eta);
     cudaFree(s->row2);
     cudaFree(s->ctl);
+    free_adjoint(s->adj);
     if (s->ctl_host) cudaFreeHost(s->ctl_host);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -1079,5 +1136,193 @@ int rmhd2d_calculate_dt_noalloc(const rmhd2d_config *cfg, const double *device_s
                           scratch, &out, st));
     CK(cudaStreamSynchronize(st));
     *dt = out;
+    return RMHD2D_OK;
+}
+
+// ---- discrete adjoint -------------------------------------------------------
+
+extern "C" int rmhd2d_run_fixed_dt(rmhd2d_solver *s, int nsteps, const double *host_dts)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
+    if (nsteps < 0 || (nsteps > 0 && !host_dts)) return fail(s, RMHD2D_ERR_INVALID, "bad nsteps or dts");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    if (nsteps == 0) return RMHD2D_OK;
+    CK(cudaSetDevice(s->device));
+    DeviceBuffer d;
+    CK(cudaMalloc(&d.p, (size_t)nsteps * sizeof(double)));
+    CK(cudaMemcpyAsync(d.p, host_dts, (size_t)nsteps * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    int rc = set_fixed_dt_mode(s, 1);
+    if (rc) return rc;
+    for (int n = 0; n < nsteps; ++n) {
+        CK(cudaMemcpyAsync(&s->ctl->dt_fixed, d.p + n, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        enqueue_step(s, s->parity);
+        s->parity ^= 1;
+        s->steps += 1;
+    }
+    rc = set_fixed_dt_mode(s, 0);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    return sync_and_check(s);
+}
+
+extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoint_interval)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    if (nsteps < 1) return fail(s, RMHD2D_ERR_INVALID, "nsteps must be >= 1");
+    if (s->g.bc_x != BC_PERIODIC || s->g.bc_y != BC_PERIODIC)
+        return fail(s, RMHD2D_ERR_INVALID, "the discrete adjoint is implemented for periodic x and y walls");
+    CK(cudaSetDevice(s->device));
+    int interval = checkpoint_interval;
+    if (interval <= 0) interval = (int)std::ceil(std::sqrt((double)nsteps));
+    if (interval > nsteps) interval = nsteps;
+    free_adjoint(s->adj);
+    s->adj = nullptr;
+    AdjointWork *w = new AdjointWork();
+    w->nsteps = nsteps;
+    w->interval = interval;
+    w->nseg = (nsteps + interval - 1) / interval;
+    const Grid &g = s->g;
+    const size_t sd = (size_t)g.plane * NFIELD;
+    w->state_doubles = sd;
+    auto alloc = [&](double **p, size_t n) -> cudaError_t {
+        cudaError_t e = cudaMalloc(p, n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, n * sizeof(double), s->stream);
+        return e;
+    };
+    cudaError_t e = cudaSuccess;
+    const size_t P = (size_t)g.plane;
+    if (e == cudaSuccess) e = alloc(&w->ckpt, (size_t)w->nseg * sd);
+    if (e == cudaSuccess) e = alloc(&w->seg0, (size_t)interval * sd);
+    if (e == cudaSuccess) e = alloc(&w->seg1, (size_t)interval * sd);
+    for (double *&u : w->ub)
+        if (e == cudaSuccess) e = alloc(&u, sd);
+    if (e == cudaSuccess) e = alloc(&w->IF, 32 * P);
+    if (e == cudaSuccess) e = alloc(&w->RJ, 6 * P);
+    if (e == cudaSuccess) e = alloc(&w->tmp, 2 * P);
+    if (e == cudaSuccess) e = alloc(&w->etab, P);
+    if (e == cudaSuccess) e = alloc(&w->dts, (size_t)nsteps);
+    if (e == cudaSuccess) e = alloc(&w->final_state, sd);
+    if (e == cudaSuccess) e = alloc(&w->aos, (size_t)g.nx * g.ny * NFIELD);
+    if (e != cudaSuccess) {
+        free_adjoint(w);
+        return fail(s, RMHD2D_ERR_CUDA, std::string("adjoint workspace allocation: ") + cudaGetErrorString(e));
+    }
+    s->adj = w;
+    for (int n = 0; n < nsteps; ++n) {
+        if (n % interval == 0)
+            CK(cudaMemcpyAsync(w->ckpt + (size_t)(n / interval) * sd, s->A, sd * sizeof(double),
+                               cudaMemcpyDeviceToDevice, s->stream));
+        enqueue_step(s, s->parity);
+        s->parity ^= 1;
+        s->steps += 1;
+        CK(cudaMemcpyAsync(w->dts + n, &s->ctl->dt, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    }
+    CK(cudaMemcpyAsync(w->final_state, s->A, sd * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaGetLastError());
+    int rc = sync_and_check(s);
+    if (rc) return rc;
+    w->dts_host.resize(nsteps);
+    CK(cudaMemcpy(w->dts_host.data(), w->dts, (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
+    w->ctl_final = *s->ctl_host;
+    return RMHD2D_OK;
+}
+
+extern "C" int rmhd2d_adjoint_dts(rmhd2d_solver *s, double *host_dts)
+{
+    if (!s || !host_dts) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!s->adj) return fail(s, RMHD2D_ERR_STATE, "no recorded forward run (rmhd2d_adjoint_forward)");
+    std::memcpy(host_dts, s->adj->dts_host.data(), s->adj->dts_host.size() * sizeof(double));
+    return RMHD2D_OK;
+}
+
+extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed, double *host_grad_state,
+                                       double *host_grad_eta)
+{
+    if (!s || !host_seed || !host_grad_state) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!s->adj) return fail(s, RMHD2D_ERR_STATE, "no recorded forward run (rmhd2d_adjoint_forward)");
+    CK(cudaSetDevice(s->device));
+    AdjointWork *w = s->adj;
+    const Grid &g = s->g;
+    const size_t sd = w->state_doubles, naos = (size_t)g.nx * g.ny * NFIELD;
+    cudaStream_t st = s->stream;
+    CK(cudaMemcpyAsync(w->aos, host_seed, naos * sizeof(double), cudaMemcpyHostToDevice, st));
+    launch_aos_to_planes(g, w->aos, w->ub[0], st);
+    CK(cudaMemsetAsync(w->etab, 0, (size_t)g.plane * sizeof(double), st));
+    int rc = set_fixed_dt_mode(s, 1);
+    if (rc) return rc;
+    int cur = 0;
+    for (int seg = w->nseg - 1; seg >= 0; --seg) {
+        const int n0 = seg * w->interval;
+        const int n1 = std::min(n0 + w->interval, w->nsteps);
+        // recompute the segment from its checkpoint with the recorded dts
+        CK(cudaMemcpyAsync(s->A, w->ckpt + (size_t)seg * sd, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        for (int n = n0; n < n1; ++n) {
+            const size_t o = (size_t)(n - n0) * sd;
+            CK(cudaMemcpyAsync(w->seg0 + o, s->A, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(&s->ctl->dt_fixed, w->dts + n, sizeof(double), cudaMemcpyDeviceToDevice, st));
+            enqueue_step(s, 0);
+            CK(cudaMemcpyAsync(w->seg1 + o, s->B, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        }
+        // reverse sweep over the segment
+        for (int n = n1 - 1; n >= n0; --n) {
+            const size_t o = (size_t)(n - n0) * sd;
+            const int mid = (cur + 1) % 3, nxt = (cur + 2) % 3;
+            AdjStageArgs a{};
+            a.g = g;
+            a.eta = s->eta;
+            a.IF = w->IF;
+            a.RJ = w->RJ;
+            a.tmp = w->tmp;
+            a.etab = w->etab;
+            a.dt = w->dts_host[n];
+            launch_boundary_transpose(g, w->ub[cur], st);
+            a.W = w->seg1 + o;
+            a.Ub = w->ub[cur];
+            a.UbStep = w->ub[cur];
+            a.Ustage = w->ub[mid];
+            a.Uin = w->ub[nxt];
+            a.s = 0.5;
+            a.stage = 2;
+            launch_adjoint_stage(a, st);
+            launch_boundary_transpose(g, w->ub[mid], st);
+            a.W = w->seg0 + o;
+            a.Ub = w->ub[mid];
+            a.UbStep = w->ub[cur];
+            a.Ustage = nullptr;
+            a.s = 1.0;
+            a.stage = 1;
+            launch_adjoint_stage(a, st);
+            cur = nxt;
+        }
+        CK(cudaGetLastError());
+    }
+    // the boundary applied when the initial state was set
+    launch_boundary_transpose(g, w->ub[cur], st);
+    launch_planes_to_aos(g, w->ub[cur], w->aos, st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(host_grad_state, w->aos, naos * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (host_grad_eta) {
+        launch_plane_to_table(g, w->etab, w->aos, st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(host_grad_eta, w->aos, (size_t)g.nx * g.ny * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    // back to the end of the forward run
+    CK(cudaMemcpyAsync(s->A, w->final_state, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->ctl, &w->ctl_final, sizeof(Control), cudaMemcpyHostToDevice, st));
+    return sync_and_check(s);
+}
+
+extern "C" int rmhd2d_adjoint_release(rmhd2d_solver *s)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->adj) {
+        CK(cudaSetDevice(s->device));
+        CK(cudaStreamSynchronize(s->stream));
+        free_adjoint(s->adj);
+        s->adj = nullptr;
+    }
     return RMHD2D_OK;
 }

@@ -31,6 +31,8 @@ struct Control {
     double total_time;           // sum of dt over the steps taken
     int crashed;                 // NaN energy seen in the newest state
     int error;                   // kernel-side error code (bounded wait expired, ...)
+    double dt_fixed;             // dt of the next step when use_fixed_dt is set
+    int use_fixed_dt;            // 1: steps take dt_fixed instead of the CFL dt (frozen-dt runs)
 };
 
 enum KernelError { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };

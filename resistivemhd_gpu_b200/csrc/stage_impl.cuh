@@ -202,8 +202,11 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
     }
 
     // dt of this step from the CFL reduction of the previous state
-    // (resistiveMHD_2D.cu:277-291), identical in every thread.
-    const double dt = step_dt(a.ctl->amax[a.parity], a.ctl->first_nan[a.parity], g.dx, g.dy, g.eps, g.eta, g.cfl);
+    // (resistiveMHD_2D.cu:277-291), identical in every thread, unless the
+    // run holds dt fixed (a recorded trajectory being replayed).
+    const double dt = a.ctl->use_fixed_dt
+                          ? a.ctl->dt_fixed
+                          : step_dt(a.ctl->amax[a.parity], a.ctl->first_nan[a.parity], g.dx, g.dy, g.eps, g.eta, g.cfl);
     if (STAGE == 1 && ctl_tile && tid == 0) {
         a.ctl->dt = dt;
         a.ctl->total_time = a.ctl->total_time + dt;

@@ -155,6 +155,37 @@ class Solver:
     def run(self, nsteps: int) -> None:
         self._ck(self._lib.rmhd2d_run(self._h, int(nsteps)))
 
+    # -- discrete adjoint (frozen dt) --
+    def run_fixed_dt(self, dts) -> None:
+        """Steps with the given dts instead of the CFL dt."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        self._ck(self._lib.rmhd2d_run_fixed_dt(self._h, len(d), d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def adjoint_forward(self, nsteps: int, checkpoint_interval: int = 0) -> None:
+        """nsteps steps, recording the dts and sqrt(N) checkpoints for adjoint_backward."""
+        self._ck(self._lib.rmhd2d_adjoint_forward(self._h, int(nsteps), int(checkpoint_interval)))
+        self._adj_steps = int(nsteps)
+
+    def adjoint_dts(self) -> np.ndarray:
+        out = np.empty(getattr(self, "_adj_steps", 0), dtype=np.float64)
+        self._ck(self._lib.rmhd2d_adjoint_dts(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def adjoint_backward(self, seed: np.ndarray, want_eta: bool = True):
+        """(dJ/dU_0, dJ/d eta) for the seed dJ/dU_N of the recorded run."""
+        sd = _as_f64(seed)
+        if sd.size != self.nx * self.ny * 8:
+            raise ValueError("seed must hold nx*ny*8 doubles")
+        gs = np.empty((self.nx, self.ny, 8), dtype=np.float64)
+        ge = np.empty((self.nx, self.ny), dtype=np.float64) if want_eta else None
+        P = ctypes.POINTER(ctypes.c_double)
+        self._ck(self._lib.rmhd2d_adjoint_backward(self._h, sd.ctypes.data_as(P), gs.ctypes.data_as(P),
+                                                   ge.ctypes.data_as(P) if ge is not None else None))
+        return gs, ge
+
+    def adjoint_release(self) -> None:
+        self._ck(self._lib.rmhd2d_adjoint_release(self._h))
+
     def set_tile_shape(self, shape: int) -> None:
         self._ck(self._lib.rmhd2d_set_tile_shape(self._h, int(shape)))
 

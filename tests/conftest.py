@@ -38,6 +38,13 @@ def oracle():
 
 
 @pytest.fixture(scope="session")
+def tangent():
+    from oracle.oracle import TangentLib
+
+    return TangentLib()
+
+
+@pytest.fixture(scope="session")
 def gpu():
     """Skips nothing: a GPU test run without a usable B200 is a failure."""
     import ctypes

@@ -1,0 +1,170 @@
+"""The discrete adjoint of the CUDA step (rmhd2d_adjoint_forward/backward).
+
+* Against the oracle's tangent (the templated restatement on dual numbers):
+  <seed, dU_N/d(direction)> must equal <gradient, direction> -- both are
+  exact derivatives of the same frozen-dt map, so to round-off (ADJ_REL).
+* Against central finite differences (h = 1e-6) of the CUDA fixed-dt
+  forward: FD_REL, the agreement the adjoint is specified to reach.
+* The checkpoint interval changes nothing (segments are recomputed bit for
+  bit), and backward leaves the solver at the end of the forward run."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ADJ_REL = 1e-10
+FD_REL = 1e-6
+
+
+def _dirs(setup, seed):
+    rng = np.random.default_rng(seed)
+    d = rng.standard_normal(setup.state.shape)
+    d[..., (1, 2, 3)] *= 1e-2
+    d[..., (0, 4, 5, 6, 7)] *= 1e-3
+    deta = rng.standard_normal((setup.nx, setup.ny)) * 1e-4
+    return d, deta
+
+
+def _eta_field(setup):
+    return setup.eta_table if setup.eta_table is not None else np.full((setup.nx, setup.ny), setup.eta)
+
+
+@pytest.mark.parametrize("with_table,shape,nsteps,interval", [
+    (False, (20, 18), 5, 2),
+    (True, (26, 21), 6, 0),
+    (True, (16, 16), 4, 4),
+])
+def test_adjoint_matches_oracle_tangent(gpu, oracle, tangent, with_table, shape, nsteps, interval):
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.random_smooth_state(*shape, seed=21, bc="periodic", with_table=with_table)
+    ref, ref_dts, crashed = oracle.run(s, s.state, nsteps)
+    assert crashed == -1
+    w = np.random.default_rng(5).standard_normal(s.state.shape)
+    with Solver.from_setup(s, precision="fp64_exact") as sol:
+        sol.adjoint_forward(nsteps, interval)
+        dts = sol.adjoint_dts()
+        assert np.array_equal(dts, ref_dts)
+        assert np.array_equal(sol.get_state(), ref)
+        gs, ge = sol.adjoint_backward(w)
+    assert np.all(gs[:3] == 0) and np.all(gs[-3:] == 0) and np.all(gs[:, :3] == 0) and np.all(gs[:, -3:] == 0)
+    for k in range(3):
+        d, deta = _dirs(s, 100 + k)
+        _, dU = tangent.tangent(s, s.state, d, dts, deta=deta)
+        jvp = float((w * dU).sum())
+        vjp_state = float((gs * d).sum())
+        vjp_eta = float((ge * deta).sum())
+        _, dU_eta = tangent.tangent(s, s.state, np.zeros_like(d), dts, deta=deta)
+        assert vjp_eta == pytest.approx(float((w * dU_eta).sum()), rel=ADJ_REL, abs=1e-14)
+        assert vjp_state + vjp_eta == pytest.approx(jvp, rel=ADJ_REL, abs=1e-14)
+
+
+def test_adjoint_full_gradient_on_a_small_grid(gpu, tangent):
+    """Every component of dJ/dU_0 and dJ/d eta on a 12x12 interior against
+    the oracle's tangent along each unit direction."""
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.random_smooth_state(12, 12, seed=8, bc="periodic", with_table=True)
+    w = np.random.default_rng(9).standard_normal(s.state.shape)
+    with Solver.from_setup(s, precision="fp64_exact") as sol:
+        sol.adjoint_forward(3, 0)
+        dts = sol.adjoint_dts()
+        gs, ge = sol.adjoint_backward(w)
+    rng = np.random.default_rng(10)
+    cells = [(i, j) for i in range(3, s.nx - 3) for j in range(3, s.ny - 3)]
+    pick = [cells[t] for t in rng.choice(len(cells), 24, replace=False)]
+    for (i, j) in pick:
+        for f in range(8):
+            d = np.zeros_like(s.state)
+            d[i, j, f] = 1.0
+            _, dU = tangent.tangent(s, s.state, d, dts)
+            want = float((w * dU).sum())
+            assert gs[i, j, f] == pytest.approx(want, rel=1e-9, abs=1e-12), (i, j, f)
+        de = np.zeros((s.nx, s.ny))
+        de[i, j] = 1.0
+        _, dU = tangent.tangent(s, s.state, np.zeros_like(s.state), dts, deta=de)
+        assert ge[i, j] == pytest.approx(float((w * dU).sum()), rel=1e-9, abs=1e-12), (i, j)
+
+
+def test_checkpoint_interval_changes_nothing_and_state_is_restored(gpu):
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.orszag_tang(48)
+    w = np.random.default_rng(1).standard_normal(s.state.shape)
+    grads = []
+    for interval in (1, 3, 0, 10):
+        with Solver.from_setup(s, precision="fp64_exact") as sol:
+            sol.adjoint_forward(10, interval)
+            end = sol.get_state().copy()
+            t_end, dt_end = sol.total_time, sol.dt
+            g1 = sol.adjoint_backward(w)
+            assert np.array_equal(sol.get_state(), end)
+            assert sol.total_time == t_end and sol.dt == dt_end
+            g2 = sol.adjoint_backward(w)
+            assert np.array_equal(g1[0], g2[0]) and np.array_equal(g1[1], g2[1])
+            grads.append(g1)
+    for g in grads[1:]:
+        assert np.array_equal(g[0], grads[0][0]) and np.array_equal(g[1], grads[0][1])
+
+
+def test_adjoint_against_central_differences(gpu):
+    """Misfit of the final (rho, bX, bY, bZ), differentiated through the
+    torch.autograd harness, against central differences (h = 1e-6) of the
+    CUDA forward with the recorded dts, along localized directions
+    (momentum and eta on a 3x3 patch).
+
+    The state is a generic smooth one: where a minmod slope is exactly zero
+    (e.g. the uniform density and pressure of the Orszag-Tang start) the
+    step map has a kink at the base point itself, central differences then
+    converge to the mean of the two one-sided derivatives, and no gradient
+    agrees with them.  A limiter kink within h of the base point spoils a
+    difference quotient of that h only, so each direction is held to the
+    better of h = 1e-6 and 1e-7."""
+    import torch
+
+    from adjoint_harness import FrozenDtRun, misfit
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.random_smooth_state(48, 48, seed=3, bc="periodic", with_table=True)
+    nsteps = 10
+    eta0 = s.eta_table.copy()
+    target = s.state.copy()
+    sol = Solver.from_setup(s, precision="fp64_exact")
+    try:
+        st0 = torch.tensor(s.state, requires_grad=True)
+        eta = torch.tensor(eta0, requires_grad=True)
+        final = FrozenDtRun.apply(st0, eta, sol, nsteps, 0)
+        J = misfit(final, torch.from_numpy(target))
+        J.backward()
+        dts = sol.adjoint_dts()
+
+        def J_of(state, eta_f):
+            sol.set_eta_table(eta_f)
+            sol.set_state(state, apply_boundary=True)
+            sol.run_fixed_dt(dts)
+            return float(misfit(torch.from_numpy(sol.get_state()), torch.from_numpy(target)))
+
+        rng = np.random.default_rng(7)
+        for _ in range(4):
+            d = np.zeros_like(s.state)
+            de = np.zeros_like(eta0)
+            i0, j0 = rng.integers(3, s.nx - 6), rng.integers(3, s.ny - 6)
+            d[i0:i0 + 3, j0:j0 + 3, 1:3] = rng.standard_normal((3, 3, 2))
+            de[i0:i0 + 3, j0:j0 + 3] = rng.standard_normal((3, 3)) * eta0[i0:i0 + 3, j0:j0 + 3]
+            ad = float((st0.grad.numpy() * d).sum() + (eta.grad.numpy() * de).sum())
+            errs = []
+            for h in (1e-6, 1e-7):
+                fd = (J_of(s.state + h * d, eta0 + h * de) - J_of(s.state - h * d, eta0 - h * de)) / (2 * h)
+                errs.append(abs(fd - ad) / abs(ad))
+            assert min(errs) <= FD_REL, (errs, ad)
+    finally:
+        sol.close()
+
+
+def test_adjoint_rejects_symmetric_walls(gpu):
+    from resistivemhd_gpu_b200 import Solver, _lib, setups
+
+    s = setups.harris_sheet(64, 32)
+    with Solver.from_setup(s, precision="fp64_exact") as sol:
+        with pytest.raises(_lib.RMHDError):
+            sol.adjoint_forward(2)
