@@ -35,7 +35,8 @@ UNITS = {
     "stage_bulk32.cu": ["-fmad=true", "--use_fast_math"],
     "aux_kernels.cu": ["-fmad=false"],
     "noalloc_dt.cu": ["-fmad=false"],
-    "adjoint.cu": ["-fmad=false"],
+    "adjoint_prep.cu": ["-fmad=false"],
+    "adjoint.cu": ["-fmad=true"],
     "api.cu": ["-fmad=false"],
 }
 

@@ -15,6 +15,7 @@ struct AdjStageArgs {
     const double *Ub;      // adjoint of the stage's output, boundary already transposed
     const double *UbStep;  // stage 1: adjoint of the step's output (its CT faces share the stage-1 EMF)
     const double *eta;     // eta plane, or nullptr for the uniform g.eta
+    double *Q;             // 18 planes: interface primitives of each cell and its own b_n (x sweep, then y sweep)
     double *IF;            // 32 planes of per-interface adjoints (x sweep, then y sweep)
     double *RJ;            // 6 planes: adjoints of J_x, J_y, J_z and direct B adjoints of the eta*J terms
     double *tmp;           // 2 planes: adjoint of the cell-centred bX, bY

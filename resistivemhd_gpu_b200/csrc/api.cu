@@ -63,11 +63,13 @@ struct rmhd2d_solver {
 // rmhd2d_adjoint_backward (all device buffers are pitched like the state).
 struct AdjointWork {
     int nsteps = 0, interval = 0, nseg = 0;
+    int cap_steps = 0, cap_interval = 0, cap_seg = 0;   // sizes the buffers were allocated for
     size_t state_doubles = 0;
     double *ckpt = nullptr;          // nseg states: U at steps 0, interval, 2*interval, ...
     double *seg0 = nullptr;          // interval states: U^n of each step of a segment (recomputed)
     double *seg1 = nullptr;          // interval states: U* of each step of a segment (recomputed)
     double *ub[3] = {nullptr, nullptr, nullptr};   // adjoint states
+    double *Q = nullptr;             // 18 planes
     double *IF = nullptr;            // 32 planes
     double *RJ = nullptr;            // 6 planes
     double *tmp = nullptr;           // 2 planes
@@ -239,6 +241,7 @@ void free_adjoint(AdjointWork *w)
     cudaFree(w->seg0);
     cudaFree(w->seg1);
     for (double *p : w->ub) cudaFree(p);
+    cudaFree(w->Q);
     cudaFree(w->IF);
     cudaFree(w->RJ);
     cudaFree(w->tmp);
@@ -1178,39 +1181,53 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
     int interval = checkpoint_interval;
     if (interval <= 0) interval = (int)std::ceil(std::sqrt((double)nsteps));
     if (interval > nsteps) interval = nsteps;
-    free_adjoint(s->adj);
-    s->adj = nullptr;
-    AdjointWork *w = new AdjointWork();
-    w->nsteps = nsteps;
-    w->interval = interval;
-    w->nseg = (nsteps + interval - 1) / interval;
+    const int nseg = (nsteps + interval - 1) / interval;
     const Grid &g = s->g;
     const size_t sd = (size_t)g.plane * NFIELD;
-    w->state_doubles = sd;
-    auto alloc = [&](double **p, size_t n) -> cudaError_t {
-        cudaError_t e = cudaMalloc(p, n * sizeof(double));
-        if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, n * sizeof(double), s->stream);
-        return e;
-    };
-    cudaError_t e = cudaSuccess;
-    const size_t P = (size_t)g.plane;
-    if (e == cudaSuccess) e = alloc(&w->ckpt, (size_t)w->nseg * sd);
-    if (e == cudaSuccess) e = alloc(&w->seg0, (size_t)interval * sd);
-    if (e == cudaSuccess) e = alloc(&w->seg1, (size_t)interval * sd);
-    for (double *&u : w->ub)
-        if (e == cudaSuccess) e = alloc(&u, sd);
-    if (e == cudaSuccess) e = alloc(&w->IF, 32 * P);
-    if (e == cudaSuccess) e = alloc(&w->RJ, 6 * P);
-    if (e == cudaSuccess) e = alloc(&w->tmp, 2 * P);
-    if (e == cudaSuccess) e = alloc(&w->etab, P);
-    if (e == cudaSuccess) e = alloc(&w->dts, (size_t)nsteps);
-    if (e == cudaSuccess) e = alloc(&w->final_state, sd);
-    if (e == cudaSuccess) e = alloc(&w->aos, (size_t)g.nx * g.ny * NFIELD);
-    if (e != cudaSuccess) {
+    // keep the workspace of an earlier run when it is large enough
+    AdjointWork *w = s->adj;
+    if (w && (w->cap_seg < nseg || w->cap_interval < interval || w->cap_steps < nsteps)) {
+        CK(cudaStreamSynchronize(s->stream));
         free_adjoint(w);
-        return fail(s, RMHD2D_ERR_CUDA, std::string("adjoint workspace allocation: ") + cudaGetErrorString(e));
+        w = s->adj = nullptr;
     }
-    s->adj = w;
+    if (!w) {
+        w = new AdjointWork();
+        w->state_doubles = sd;
+        auto alloc = [&](double **p, size_t n, bool zero) -> cudaError_t {
+            cudaError_t e = cudaMalloc(p, n * sizeof(double));
+            if (e == cudaSuccess && zero) e = cudaMemsetAsync(*p, 0, n * sizeof(double), s->stream);
+            return e;
+        };
+        cudaError_t e = cudaSuccess;
+        const size_t P = (size_t)g.plane;
+        // checkpoints and segment states are written before they are read;
+        // the adjoint planes are cleared once so their unused padding is 0
+        if (e == cudaSuccess) e = alloc(&w->ckpt, (size_t)nseg * sd, false);
+        if (e == cudaSuccess) e = alloc(&w->seg0, (size_t)interval * sd, false);
+        if (e == cudaSuccess) e = alloc(&w->seg1, (size_t)interval * sd, false);
+        for (double *&u : w->ub)
+            if (e == cudaSuccess) e = alloc(&u, sd, true);
+        if (e == cudaSuccess) e = alloc(&w->Q, 18 * P, true);
+        if (e == cudaSuccess) e = alloc(&w->IF, 32 * P, true);
+        if (e == cudaSuccess) e = alloc(&w->RJ, 6 * P, true);
+        if (e == cudaSuccess) e = alloc(&w->tmp, 2 * P, true);
+        if (e == cudaSuccess) e = alloc(&w->etab, P, true);
+        if (e == cudaSuccess) e = alloc(&w->dts, (size_t)nsteps, false);
+        if (e == cudaSuccess) e = alloc(&w->final_state, sd, false);
+        if (e == cudaSuccess) e = alloc(&w->aos, (size_t)g.nx * g.ny * NFIELD, false);
+        if (e != cudaSuccess) {
+            free_adjoint(w);
+            return fail(s, RMHD2D_ERR_CUDA, std::string("adjoint workspace allocation: ") + cudaGetErrorString(e));
+        }
+        w->cap_seg = nseg;
+        w->cap_interval = interval;
+        w->cap_steps = nsteps;
+        s->adj = w;
+    }
+    w->nsteps = nsteps;
+    w->interval = interval;
+    w->nseg = nseg;
     for (int n = 0; n < nsteps; ++n) {
         if (n % interval == 0)
             CK(cudaMemcpyAsync(w->ckpt + (size_t)(n / interval) * sd, s->A, sd * sizeof(double),
@@ -1273,6 +1290,7 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
             AdjStageArgs a{};
             a.g = g;
             a.eta = s->eta;
+            a.Q = w->Q;
             a.IF = w->IF;
             a.RJ = w->RJ;
             a.tmp = w->tmp;

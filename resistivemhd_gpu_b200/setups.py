@@ -221,3 +221,67 @@ def random_smooth_state(n: int, m: int, seed: int = 7, bc: str = "periodic", amp
                                    * np.ones((nx, ny)))
     return Setup("random_smooth", _pack(rho, u, v, w, bx, by, bz, e), dx, dy, gamma, 0.4, 1e-20,
                  float(eta * 1.5) if with_table else eta, tab, bc, bc_y=bc_y)
+
+
+def gaussian_random_field(n: int, m: int, lx: float, ly: float, corr: float, seed: int) -> np.ndarray:
+    """Periodic Gaussian random field on an n x m cell-centred grid of a
+    lx x ly box: white noise (Box-Muller on the counter-based generator)
+    filtered in Fourier space by exp(-|k|^2 corr^2 / 4), the square root of
+    the spectrum of the covariance exp(-r^2 / (2 corr^2)), then scaled to
+    zero mean and unit variance."""
+    u1 = 0.5 * (uniform_noise(seed, 101, n, m) + 1.0)
+    u2 = 0.5 * (uniform_noise(seed, 102, n, m) + 1.0)
+    white = np.sqrt(-2.0 * np.log(np.maximum(u1, 1e-300))) * np.cos(2.0 * math.pi * u2)
+    kx = 2.0 * math.pi * np.fft.fftfreq(n, d=lx / n)[:, None]
+    ky = 2.0 * math.pi * np.fft.fftfreq(m, d=ly / m)[None, :]
+    g = np.real(np.fft.ifft2(np.fft.fft2(white) * np.exp(-(kx * kx + ky * ky) * corr * corr / 4.0)))
+    g -= g.mean()
+    return g / g.std()
+
+
+def _periodic_extend(a: np.ndarray) -> np.ndarray:
+    """Interior (n, m) array -> (n + 6, m + 6) with periodic ghosts."""
+    return np.pad(a, GHOST, mode="wrap")
+
+
+def ot_adjoint(n: int = 512, seed: int = 5, eta0: float = 1e-3, corr: float = 0.3, **kw) -> Setup:
+    """Orszag-Tang vortex with a spatial resistivity eta = eta0 exp(g / 2),
+    g a periodic Gaussian random field of correlation length `corr` (the
+    inverse problem's parameter field), tabulated at cell centres; the dt
+    limit uses the table's maximum."""
+    s = orszag_tang(n, **kw)
+    g = gaussian_random_field(n, n, 2.0 * math.pi, 2.0 * math.pi, corr, seed)
+    tab = np.ascontiguousarray(_periodic_extend(eta0 * np.exp(0.5 * g)))
+    s.name = "ot_adjoint"
+    s.eta_table = tab
+    s.eta = float(tab.max())
+    return s
+
+
+def kelvin_helmholtz(n: int = 256, m: int | None = None, width: float = 0.05, amp: float = 1e-2,
+                     guide: float = 0.1, rho0: float = 1.0, p0: float = 1.0, eta: float = 1e-3,
+                     seed: int = 4, cfl: float = 0.4, gamma: float = 5.0 / 3.0) -> Setup:
+    """Periodic double shear layer on [0, 1)^2: vx = (tanh((y - 1/4)/w) -
+    tanh((y - 3/4)/w) - 1) / 2 (two tanh layers, so the flow is periodic in
+    y), vy = amp (sin(2 pi x) + noise) times Gaussians of width w about the
+    layers, uniform rho = rho0 and p = p0, and an in-plane guide field
+    Bx = guide along the flow (By = Bz = 0), uniform eta."""
+    m = n if m is None else m
+    nx, ny = n + 2 * GHOST, m + 2 * GHOST
+    dx, dy = 1.0 / n, 1.0 / m
+    xc, yc = _centres(nx, 0.0, dx)[:, None], _centres(ny, 0.0, dy)[None, :]
+    shape = (nx, ny)
+    # periodic images of the layer positions keep the ghosts consistent
+    yw = np.mod(yc, 1.0)
+    u = np.broadcast_to(0.5 * (np.tanh((yw - 0.25) / width) - np.tanh((yw - 0.75) / width) - 1.0), shape).copy()
+    env = np.exp(-((yw - 0.25) ** 2) / (2 * width * width)) + np.exp(-((yw - 0.75) ** 2) / (2 * width * width))
+    v = amp * (np.sin(2.0 * math.pi * xc) + uniform_noise(seed, 2, nx, ny)) * env
+    rho = np.full(shape, rho0)
+    p = np.full(shape, p0)
+    w = np.zeros(shape)
+    bx = np.full(shape, guide)
+    by = np.zeros(shape)
+    bz = np.zeros(shape)
+    e = _energy(rho, u, v, w, bx, by, bz, p, gamma)
+    return Setup("kelvin_helmholtz", _pack(rho, u, v, w, bx, by, bz, e), dx, dy, gamma, cfl, 1e-20, eta,
+                 None, "periodic")

@@ -20,7 +20,9 @@ void host_basic_param(const double *c, double bn_next, double gm, double *q)
 void host_basic_param_adj(const double *c, double gm, const double *qb, double *cb)
 {
     for (int k = 0; k < 8; ++k) cb[k] = 0.0;
-    rmhd2d::adj::basic_param_adj(c, gm, qb, cb);
+    double q[8];
+    rmhd2d::adj::basic_param(c, 0.3, gm, q);
+    rmhd2d::adj::basic_param_adj(q, c[4], gm, qb, cb);
 }
 
 unsigned host_muscl_states(const double *q0, const double *q1, const double *q2, const double *q3, double eps,
