@@ -259,12 +259,19 @@ __device__ __forceinline__ void hlld_flux_fast(const PrimT<T> &L, const PrimT<T>
     const T cs2R = gm * R.p * iRR, ca2R = b2R * iRR, va2R = bx2 * iRR;
     const T sL = cs2L + ca2L, sR = cs2R + ca2R;
     // The reference takes sqrt of each squared speed, so a negative one makes
-    // its fast speed NaN; keep that.
+    // its fast speed NaN; keep that.  The discriminant
+    // (cs2 + ca2)^2 - 4 cs2 va2 is formed as (cs2 - ca2)^2 + 4 cs2 bt2 / rho
+    // (bt2 the tangential |B|^2, ca2 - va2 = bt2 / rho): the same number
+    // without the cancellation that rounds it below zero where the
+    // tangential field vanishes and cs ~ ca.
     const T qnan = T(bits_to_double(0x7FF8000000000000ull));
     const bool okL = (cs2L >= T(0)) & (ca2L >= T(0)) & (va2L >= T(0));
     const bool okR = (cs2R >= T(0)) & (ca2R >= T(0)) & (va2R >= T(0));
-    const T cfL = okL ? sqrt_t(T(0.5) * (sL + sqrt_t(sL * sL - T(4.0) * cs2L * va2L))) : qnan;
-    const T cfR = okR ? sqrt_t(T(0.5) * (sR + sqrt_t(sR * sR - T(4.0) * cs2R * va2R))) : qnan;
+    const T dcL = cs2L - ca2L, dcR = cs2R - ca2R;
+    const T discL = dcL * dcL + T(4.0) * cs2L * (L.bY * L.bY + L.bZ * L.bZ) * iRL;
+    const T discR = dcR * dcR + T(4.0) * cs2R * (R.bY * R.bY + R.bZ * R.bZ) * iRR;
+    const T cfL = okL ? sqrt_t(T(0.5) * (sL + sqrt_t(discL))) : qnan;
+    const T cfR = okR ? sqrt_t(T(0.5) * (sR + sqrt_t(discR))) : qnan;
 
     const T uL = L.u, uR = R.u;
     T SL = tmin(uL, uR) - tmax(cfL, cfR);
@@ -392,8 +399,12 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
     const float qnan = __int_as_float(0x7fc00000);
     const bool okL = (cs2L >= 0.f) & (ca2L >= 0.f) & (va2L >= 0.f);
     const bool okR = (cs2R >= 0.f) & (ca2R >= 0.f) & (va2R >= 0.f);
-    const float cfL = okL ? sqrt_t(0.5f * (sL + sqrt_t(sL * sL - 4.f * cs2L * va2L))) : qnan;
-    const float cfR = okR ? sqrt_t(0.5f * (sR + sqrt_t(sR * sR - 4.f * cs2R * va2R))) : qnan;
+    // discriminant without cancellation, as in hlld_flux_fast
+    const float dcL = cs2L - ca2L, dcR = cs2R - ca2R;
+    const float bt2L = (float)(s.bYL * s.bYL + s.bZL * s.bZL), bt2R = (float)(s.bYR * s.bYR + s.bZR * s.bZR);
+    const float discL = dcL * dcL + 4.f * cs2L * bt2L * iRL, discR = dcR * dcR + 4.f * cs2R * bt2R * iRR;
+    const float cfL = okL ? sqrt_t(0.5f * (sL + sqrt_t(discL))) : qnan;
+    const float cfR = okR ? sqrt_t(0.5f * (sR + sqrt_t(discR))) : qnan;
 
     float SL = tmin(uL, uR) - tmax(cfL, cfR);
     float SR = tmax(uL, uR) + tmax(cfL, cfR);

@@ -285,3 +285,21 @@ def kelvin_helmholtz(n: int = 256, m: int | None = None, width: float = 0.05, am
     e = _energy(rho, u, v, w, bx, by, bz, p, gamma)
     return Setup("kelvin_helmholtz", _pack(rho, u, v, w, bx, by, bz, e), dx, dy, gamma, cfl, 1e-20, eta,
                  None, "periodic")
+
+
+ENSEMBLE_SIZES = (128, 192, 256, 384, 512)
+
+
+def ensemble(nruns: int = 256, seed: int = 4, eta_range: tuple[float, float] = (1e-4, 1e-2)) -> list[Setup]:
+    """Independent periodic runs of uneven size: grid n x n with n drawn from
+    ENSEMBLE_SIZES, eta log-uniform in eta_range, even runs Orszag-Tang and
+    odd runs Kelvin-Helmholtz, all drawn from one seeded generator."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice(ENSEMBLE_SIZES, size=nruns)
+    etas = np.exp(rng.uniform(math.log(eta_range[0]), math.log(eta_range[1]), size=nruns))
+    out = []
+    for r in range(nruns):
+        n, eta = int(sizes[r]), float(etas[r])
+        s = orszag_tang(n, eta=eta, seed=1000 + r) if r % 2 == 0 else kelvin_helmholtz(n, eta=eta, seed=1000 + r)
+        out.append(s)
+    return out

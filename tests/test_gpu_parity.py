@@ -257,3 +257,27 @@ def test_full_size_properties(gpu):
     for f in (0, 7):
         a0, a1 = u0[3:-3, 3:-3, f].sum(), u1[3:-3, 3:-3, f].sum()
         assert abs(a1 - a0) <= 1e-11 * abs(a0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp32_bulk", "fp64_fast"])
+def test_orszag_tang_past_the_degenerate_fast_speed(gpu, precision):
+    """Orszag-Tang keeps bZ = 0 and lets bY cross zero, so the fast-speed
+    discriminant (cs2 + ca2)^2 - 4 cs2 va2 reaches 0 where cs ~ ca; formed
+    with cancellation it rounded below zero in single precision and the
+    FP32-bulk run crashed near t = 2.  The run must stay finite and follow
+    the FP64 run."""
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.ot_adjoint(256)
+    with Solver.from_setup(s, precision="fp64_exact") as ref:
+        ref.run(1100)
+        assert not ref.check_crashed()
+        want, t_want = ref.get_state(), ref.total_time
+    with Solver.from_setup(s, precision=precision) as sol:
+        sol.run(1100)
+        assert not sol.check_crashed()
+        got = sol.get_state()
+        assert sol.total_time == pytest.approx(t_want, rel=1e-6)
+    rho = np.abs(got[3:-3, 3:-3, 0] - want[3:-3, 3:-3, 0]).sum() / np.abs(want[3:-3, 3:-3, 0]).sum()
+    assert rho < (1e-4 if precision == "fp32_bulk" else 1e-9)
