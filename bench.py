@@ -63,9 +63,9 @@ def workload(name: str):
     from resistivemhd_gpu_b200 import setups
 
     if name == "harris":
-        return setups.harris_sheet(2048, 1024), "harris_2048x1024_fp64"
+        return setups.harris_sheet(2048, 1024), "harris_2048x1024"
     if name == "orszag_tang":
-        return setups.orszag_tang(256), "orszag_tang_256x256_fp64"
+        return setups.orszag_tang(256), "orszag_tang_256x256"
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -235,7 +235,7 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
     ab = algorithmic_bytes(setup)
     peak, peak_kind = hbm_peak()
     achieved = (ab["stage1"] + ab["stage2"]) / ((st1 + st2) * 1e-3) / 1e9
-    traffic = traffic_from_profile(label)
+    traffic = traffic_from_profile(f"{label}_{args.precision}")
     roofline = {
         "kernel": "stage_kernel (stage 1 + stage 2 per step)", "bound": "hbm", "achieved": achieved,
         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
@@ -287,7 +287,8 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "fp32_bulk" else "f64", "data": "synthetic",
             "config": {"workload": label, "cells": cells, "nx": setup.nx, "ny": setup.ny, "bc": setup.bc,
                        "eta": "uniform 1e-3 + gaussian bump (cell-centred table)" if setup.eta_table is not None
                        else f"uniform {setup.eta}",
@@ -302,7 +303,7 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
             line["e2e"] = e2e
         # FP64 issue bound: executed FP64 instruction rate is in the ncu summary.
         line["fp64"] = {"peak_nominal_tflops": B200_FP64_TFLOPS_NOMINAL,
-                        "see": f"profiles/stage_kernel_{label}.md"}
+                        "see": f"profiles/stage_kernel_{label}_{args.precision}.md"}
     sol.close()
 
     if rank == 0 and world == 1 and args.baselines:
