@@ -18,6 +18,10 @@
 // end of their initializeU; errors throw rmhd2d::Error.
 #pragma once
 
+#include <cstdio>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -107,5 +111,33 @@ private:
     rmhd2d_solver *s_ = nullptr;
     std::vector<double> hU_;
 };
+
+// The reference drivers' main loop (examples2D/plasmoid/main_plasmoid.cu:297-329):
+// for step = 0 .. totalStep, every recordStep steps save the state as
+// directoryname/filenameWithoutStep_step.bin and append "step,totalTime"
+// (4 significant digits) to logfile, then take one step; stop at the first
+// crashed state.  Returns the step at which the run stopped (totalStep + 1
+// when it ran through) and leaves the elapsed time in totalTime.
+inline int runLikeReference(ResistiveMHD2D &sim, int totalStep, int recordStep, const std::string &directoryname,
+                            const std::string &filenameWithoutStep, std::ostream &logfile, double &totalTime,
+                            bool echo = true)
+{
+    for (int step = 0; step < totalStep + 1; step++) {
+        if (step % recordStep == 0) {
+            sim.save(directoryname, filenameWithoutStep, step);
+            logfile << std::to_string(step) << "," << std::setprecision(4) << totalTime << std::endl;
+            if (echo)
+                std::cout << std::to_string(step) << " step done : total time is " << std::setprecision(4)
+                          << totalTime << std::endl;
+        }
+        sim.oneStepRK2();
+        if (sim.checkCalculationIsCrashed()) {
+            if (echo) std::cout << "Calculation stopped! : " << step << " steps" << std::endl;
+            return step;
+        }
+        totalTime += sim.dt();
+    }
+    return totalStep + 1;
+}
 
 }  // namespace rmhd2d
