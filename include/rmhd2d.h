@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RMHD2D_ABI_VERSION 1
+#define RMHD2D_ABI_VERSION 2
 #define RMHD2D_GHOST 3
 
 typedef enum {
@@ -65,6 +65,23 @@ typedef enum {
     RMHD2D_FP32_BULK = 2
 } rmhd2d_precision;
 
+typedef enum {
+    /* The single-GPU library's CT: the stage-1 corner EMF (the arithmetic
+       mean of the four numerical induction fluxes) updates the face B of
+       both stages (TP resistiveMHD_2D.cu:133-195, ct.cu:22-59). */
+    RMHD2D_CT_STAGE1 = 0,
+    /* CT-Contact: B advances by flux differences in both stages, and one CT
+       from the step input's faces ends the step, with the mean of the two
+       stages' contact EMFs -- the arithmetic mean plus corrections upwinded
+       by the signs of the mass fluxes against per-cell reference EMFs
+       u bY - v bX - eta jZ (the multi-GPU library's
+       ResistiveMHD2D_GPU/ct.cu:26-257 with the ordering of its oneStepRK2,
+       resistiveMHD2D.cu:147-221), on this library's fluxes and dt.  Runs in
+       FP64 without contraction whatever cfg.precision; no batches, adjoint
+       or rmhd2d_profile_step. */
+    RMHD2D_CT_CONTACT = 1
+} rmhd2d_ct_scheme;
+
 typedef struct {
     int nx, ny;                 /* cells per direction incl. 3 ghost layers per side; both >= 12 */
     double dx, dy;              /* cell sizes (reference const.hpp:7,12) */
@@ -80,6 +97,7 @@ typedef struct {
     int precision;              /* rmhd2d_precision */
     int device;                 /* CUDA device ordinal */
     void *stream;               /* cudaStream_t to enqueue on, or NULL for a solver-owned stream */
+    int ct_scheme;              /* rmhd2d_ct_scheme */
 } rmhd2d_config;
 
 typedef struct rmhd2d_solver rmhd2d_solver;

@@ -34,7 +34,7 @@ class _Params(ctypes.Structure):
         ("dx", ctypes.c_double), ("dy", ctypes.c_double),
         ("gamma", ctypes.c_double), ("cfl", ctypes.c_double), ("eps", ctypes.c_double),
         ("eta", ctypes.c_double), ("eta_table", ctypes.POINTER(ctypes.c_double)),
-        ("bc", ctypes.c_int), ("bc_y", ctypes.c_int),
+        ("bc", ctypes.c_int), ("bc_y", ctypes.c_int), ("ct_contact", ctypes.c_int),
     ]
 
 
@@ -129,7 +129,8 @@ class OracleLib:
             eta_keep.append(tab)
         p = _Params(setup.nx, setup.ny, setup.dx, setup.dy, setup.gamma, setup.cfl, setup.eps,
                     setup.eta, tab.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if tab is not None else None,
-                    BC[setup.bc], BC[getattr(setup, "bc_y", None) or setup.bc])
+                    BC[setup.bc], BC[getattr(setup, "bc_y", None) or setup.bc],
+                    1 if getattr(setup, "ct", "stage1") == "contact" else 0)
         return p
 
     def boundary(self, setup, state: np.ndarray) -> np.ndarray:

@@ -598,8 +598,9 @@ void orc_boundary(const orc_params *p, double *U)
 size_t orc_work_doubles(int nx, int ny)
 {
     size_t N = (size_t)nx * ny;
-    /* UBar, T, F, G, dQ, dQL, dQR (8 each) + bXOld, bYOld, tmp, Ez */
-    return N * (7 * 8 + 4);
+    /* UBar, T, F, G, dQ, dQL, dQR (8 each) + bXOld, bYOld, tmp, Ez,
+       and for CT-Contact the 12 per-cell EMF inputs of the two stages */
+    return N * (7 * 8 + 4 + 12);
 }
 
 /* resistiveMHD_2D.cu:133-195 oneStepRK2.  U is updated in place; work must
@@ -670,6 +671,150 @@ double orc_step(const orc_params *p, double *U, double *work)
     return dt;
 }
 
+/* CT-Contact inputs of one stage, per cell (ResistiveMHD_multiGPU_cuda/
+   ResistiveMHD2D_GPU/ct.cu:26-65 setFlux_kernel): the numerical induction
+   fluxes F.f5, G.f4, the mass fluxes F.f0, G.f0, and the cell's reference
+   EMF u*bY - v*bX - eta*jZ (with centred face B and the mean of the four
+   corner curls of U's face B) as the x flux and its negative as the y flux,
+   for 0 < i < nx-1, 0 < j < ny-1.  Entries outside are left NaN. */
+static void contact_set_flux(const orc_params *p, const double *F, const double *G, const double *U,
+                             double *NF5, double *NG4, double *CF5, double *CG4, double *NF0, double *NG0)
+{
+    const int nx = p->nx, ny = p->ny, N = nx * ny;
+    const double dx = p->dx, dy = p->dy;
+    for (int k = 0; k < N; ++k) NF5[k] = NG4[k] = CF5[k] = CG4[k] = NF0[k] = NG0[k] = NAN;
+    for (int i = 1; i < nx - 1; ++i) {
+        for (int j = 1; j < ny - 1; ++j) {
+            const int index = j + i * ny;
+#define BXAT(k) U[(k) * NV + BXF]
+#define BYAT(k) U[(k) * NV + BYF]
+            double rho = U[index * NV + RHO];
+            double u = U[index * NV + MX] / rho;
+            double v = U[index * NV + MY] / rho;
+            double bX = 0.5 * (BXAT(index) + BXAT(index - ny));
+            double bY = 0.5 * (BYAT(index) + BYAT(index - 1));
+            double jZ = 0.25 * (
+                (BYAT(index + ny) - BYAT(index)) / dx - (BXAT(index + 1) - BXAT(index)) / dy
+              + (BYAT(index - 1 + ny) - BYAT(index - 1)) / dx - (BXAT(index) - BXAT(index - 1)) / dy
+              + (BYAT(index - 1) - BYAT(index - 1 - ny)) / dx - (BXAT(index - ny) - BXAT(index - ny - 1)) / dy
+              + (BYAT(index) - BYAT(index - ny)) / dx - (BXAT(index + 1 - ny) - BXAT(index - ny)) / dy);
+#undef BXAT
+#undef BYAT
+            double eta = eta_at(p, i, j);
+            NF5[index] = F[index * 8 + 5];
+            NG4[index] = G[index * 8 + 4];
+            CF5[index] = u * bY - v * bX - eta * jZ;
+            CG4[index] = -(u * bY - v * bX - eta * jZ);
+            NF0[index] = F[index * 8 + 0];
+            NG0[index] = G[index * 8 + 0];
+        }
+    }
+}
+
+/* MC sign(): (x > 0) - (x < 0) as an int (sign.cu). */
+static inline int isgn(double x) { return (x > 0.0) - (x < 0.0); }
+
+/* One stage's CT-Contact corner EMF at corner (i+1/2, j+1/2) (ct.cu:147-169):
+   the arithmetic mean of the four numerical induction fluxes plus the
+   upwinded corrections selected by the signs of the mass fluxes. */
+static double contact_corner(int index, int ny, const double *NF5, const double *NG4, const double *CF5,
+                             const double *CG4, const double *NF0, const double *NG0)
+{
+    double avg = 0.25 * (-NF5[index] - NF5[index + 1] + NG4[index] + NG4[index + ny]);
+    double eS = (1.0 + isgn(NF0[index])) * (NG4[index] - CG4[index])
+              + (1.0 - isgn(NF0[index])) * (NG4[index + ny] - CG4[index + ny]);
+    double eN = (1.0 + isgn(NF0[index + 1])) * (CG4[index + 1] - NG4[index])
+              + (1.0 - isgn(NF0[index + 1])) * (CG4[index + 1 + ny] - NG4[index + ny]);
+    double eW = -(1.0 + isgn(NG0[index])) * (NF5[index] - CF5[index])
+              - (1.0 - isgn(NG0[index])) * (NF5[index + 1] - CF5[index + 1]);
+    double eE = -(1.0 + isgn(NG0[index + ny])) * (CF5[index + ny] - NF5[index])
+              - (1.0 - isgn(NG0[index + ny])) * (CF5[index + 1 + ny] - NF5[index + 1]);
+    return avg + 0.125 * (eS - eN + eW - eE);
+}
+
+/* The step with the CT-Contact EMF of the multi-GPU library
+   (ResistiveMHD2D_GPU/resistiveMHD2D.cu:147-221 oneStepRK2 ordering,
+   ct.cu:26-257): both stages update B by flux differences like every other
+   field, from the face B that shift + back-to-face left in U; the reference
+   EMFs of stage 1 are taken from U after that smoothing and those of stage 2
+   from the step's output after its boundary pass; one CT from the step
+   input's faces with the mean of the two stages' contact EMFs ends the
+   step, followed by the boundary pass.  Fluxes (HLLD, MUSCL, the resistive
+   hook), the update ranges and dt are this library's (resistiveMHD_2D.cu
+   of the single-GPU library).  Returns the dt used. */
+double orc_step_contact(const orc_params *p, double *U, double *work)
+{
+    const int nx = p->nx, ny = p->ny, N = nx * ny;
+    double *UBar = work;
+    double *T = UBar + (size_t)N * 8;
+    double *F = T + (size_t)N * 8;
+    double *G = F + (size_t)N * 8;
+    double *dQ = G + (size_t)N * 8;
+    double *dQL = dQ + (size_t)N * 8;
+    double *dQR = dQL + (size_t)N * 8;
+    double *bXOld = dQR + (size_t)N * 8;
+    double *bYOld = bXOld + N;
+    double *tmp = bYOld + N;
+    double *Ez = tmp + N;
+    double *oNF5 = Ez + N, *oNG4 = oNF5 + N, *oCF5 = oNG4 + N, *oCG4 = oCF5 + N, *oNF0 = oCG4 + N, *oNG0 = oNF0 + N;
+    double *nNF5 = oNG0 + N, *nNG4 = nNF5 + N, *nCF5 = nNG4 + N, *nCG4 = nCF5 + N, *nNF0 = nCG4 + N, *nNG0 = nNF0 + N;
+
+    for (int k = 0; k < N; ++k) { bXOld[k] = U[k * NV + BXF]; bYOld[k] = U[k * NV + BYF]; }
+    memcpy(UBar, U, (size_t)N * NV * sizeof(double));
+
+    const double dt = orc_calc_dt(p, U);
+    const double dx = p->dx, dy = p->dy;
+
+    shift_to_center(p, U, tmp);
+    flux_x(p, U, F, dQ, dQL, dQR);
+    flux_y(p, U, G, T, dQ, dQL, dQR);
+    back_to_face(p, U, tmp);
+    contact_set_flux(p, F, G, U, oNF5, oNG4, oCF5, oCG4, oNF0, oNG0);
+
+    for (int k = ny; k < N; ++k) {
+        const double *u = &U[k * NV];
+        const double *f = &F[k * 8], *fm = &F[(k - ny) * 8];
+        const double *g = &G[k * 8], *gm = &G[(k - 1) * 8];
+        double *ub = &UBar[k * NV];
+        for (int c = 0; c < 8; ++c)
+            ub[c] = u[c] - dt / dx * (f[c] - fm[c]) - dt / dy * (g[c] - gm[c]);
+    }
+    orc_boundary(p, UBar);
+
+    shift_to_center(p, UBar, tmp);
+    flux_x(p, UBar, F, dQ, dQL, dQR);
+    flux_y(p, UBar, G, T, dQ, dQL, dQR);
+    back_to_face(p, UBar, tmp);
+
+    for (int k = ny; k < N; ++k) {
+        double *u = &U[k * NV];
+        const double *ub = &UBar[k * NV];
+        const double *f = &F[k * 8], *fm = &F[(k - ny) * 8];
+        const double *g = &G[k * 8], *gm = &G[(k - 1) * 8];
+        for (int c = 0; c < 8; ++c)
+            u[c] = 0.5 * (u[c] + ub[c]
+                 - dt / dx * (f[c] - fm[c])
+                 - dt / dy * (g[c] - gm[c]));
+    }
+    orc_boundary(p, U);
+    contact_set_flux(p, F, G, U, nNF5, nNG4, nCF5, nCG4, nNF0, nNG0);
+
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const int index = j + i * ny;
+            if (i < nx - 1 && j < ny - 1) {
+                double eOld = contact_corner(index, ny, oNF5, oNG4, oCF5, oCG4, oNF0, oNG0);
+                double eNow = contact_corner(index, ny, nNF5, nNG4, nCF5, nCG4, nNF0, nNG0);
+                Ez[index] = 0.5 * (eOld + eNow);
+            } else {
+                Ez[index] = NAN;
+            }
+        }
+    ct_update(p, bXOld, bYOld, Ez, dt, U);
+    orc_boundary(p, U);
+    return dt;
+}
+
 /* Runs nsteps steps; dts (may be NULL) receives each step's dt.  Returns 0,
    or 1 + the step index at which the crash check (NaN energy) fired, after
    which no further step is taken, as the reference drivers do. */
@@ -680,7 +825,7 @@ int orc_run(const orc_params *p, double *U, int nsteps, double *dts)
     if (!work) return -1;
     int rc = 0;
     for (int s = 0; s < nsteps; ++s) {
-        double dt = orc_step(p, U, work);
+        double dt = p->ct_contact ? orc_step_contact(p, U, work) : orc_step(p, U, work);
         if (dts) dts[s] = dt;
         if (orc_is_crashed(p, U)) { rc = 1 + s; break; }
     }

@@ -25,6 +25,7 @@ typedef struct {
     const double *eta_table;  /* optional cell-centred eta, k = j + i*ny */
     int bc;                   /* x boundary: ORC_BC_PERIODIC or ORC_BC_SYMMETRIC */
     int bc_y;                 /* y boundary, or -1 for the same as bc */
+    int ct_contact;           /* 0: the step's CT with the stage-1 EMF; 1: CT-Contact EMF (orc_step_contact) */
 } orc_params;
 
 double orc_calc_dt(const orc_params *p, const double *U);
@@ -32,6 +33,7 @@ int orc_is_crashed(const orc_params *p, const double *U);
 void orc_boundary(const orc_params *p, double *U);
 size_t orc_work_doubles(int nx, int ny);
 double orc_step(const orc_params *p, double *U, double *work);
+double orc_step_contact(const orc_params *p, double *U, double *work);
 int orc_run(const orc_params *p, double *U, int nsteps, double *dts);
 
 #ifdef __cplusplus

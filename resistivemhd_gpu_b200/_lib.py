@@ -18,6 +18,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no sm_100 device"
           5: "I/O error", 6: "kernel error"}
 
 BC = {"periodic": 0, "symmetric": 1}
+CT = {"stage1": 0, "contact": 1}
 PRECISION = {"fp64_exact": 0, "exact": 0, "fp64_fast": 1, "fast": 1, "fp32_bulk": 2, "bulk32": 2}
 
 
@@ -29,7 +30,7 @@ class Config(ctypes.Structure):
         ("gamma_mhd", ctypes.c_double), ("cfl", ctypes.c_double), ("eps", ctypes.c_double),
         ("eta", ctypes.c_double),
         ("bc", ctypes.c_int), ("bc_y", ctypes.c_int), ("precision", ctypes.c_int), ("device", ctypes.c_int),
-        ("stream", ctypes.c_void_p),
+        ("stream", ctypes.c_void_p), ("ct_scheme", ctypes.c_int),
     ]
 
 

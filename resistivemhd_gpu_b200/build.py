@@ -36,6 +36,7 @@ UNITS = {
     "aux_kernels.cu": ["-fmad=false"],
     "noalloc_dt.cu": ["-fmad=false"],
     "adjoint_prep.cu": ["-fmad=false"],
+    "contact.cu": ["-fmad=false"],
     "adjoint.cu": ["-fmad=true"],
     "api.cu": ["-fmad=false"],
 }

@@ -25,6 +25,7 @@
 #include "../../include/rmhd2d.h"
 #include "adjoint.h"
 #include "aux_kernels.h"
+#include "contact.h"
 #include "noalloc_dt.h"
 #include "physics.cuh"
 #include "rmhd2d_internal.h"
@@ -56,6 +57,7 @@ struct rmhd2d_solver {
     long long steps = 0;
     cudaGraphExec_t graph2[2] = {nullptr, nullptr};
     AdjointWork *adj = nullptr;          // recorded trajectory and workspace of the discrete adjoint
+    double *contact = nullptr;           // CT-Contact workspace: C, F1, G1, F2, G2 (8 planes each), R1, R2
     std::string err;
 };
 
@@ -201,6 +203,26 @@ BatchLauncher batch_launcher(int precision)
 
 void enqueue_step(rmhd2d_solver *s, int parity)
 {
+    if (s->contact) {
+        const size_t P = (size_t)s->g.plane;
+        ContactStep c{};
+        c.g = s->g;
+        c.A = s->A;
+        c.B = s->B;
+        c.C = s->contact;
+        c.F1 = c.C + NFIELD * P;
+        c.G1 = c.F1 + NFIELD * P;
+        c.F2 = c.G1 + NFIELD * P;
+        c.G2 = c.F2 + NFIELD * P;
+        c.R1 = c.G2 + NFIELD * P;
+        c.R2 = c.R1 + P;
+        c.eta = s->eta;
+        c.row2 = s->row2;
+        c.ctl = s->ctl;
+        c.parity = parity;
+        enqueue_contact_step(c, s->stream);
+        return;
+    }
     StageArgs a{};
     a.g = s->g;
     a.eta = s->eta;
@@ -293,6 +315,7 @@ void rmhd2d_config_default(rmhd2d_config *c)
     c->precision = RMHD2D_FP64_EXACT;
     c->device = 0;
     c->stream = nullptr;
+    c->ct_scheme = RMHD2D_CT_STAGE1;
 }
 
 int rmhd2d_abi_version(void) { return RMHD2D_ABI_VERSION; }
@@ -335,6 +358,8 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
     if (cfg->precision != RMHD2D_FP64_EXACT && cfg->precision != RMHD2D_FP64_FAST &&
         cfg->precision != RMHD2D_FP32_BULK)
         return fail(s, RMHD2D_ERR_INVALID, "unknown precision");
+    if (cfg->ct_scheme != RMHD2D_CT_STAGE1 && cfg->ct_scheme != RMHD2D_CT_CONTACT)
+        return fail(s, RMHD2D_ERR_INVALID, "unknown ct_scheme");
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
@@ -382,6 +407,11 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
         cudaMalloc(&s->ctl, sizeof(Control)) != cudaSuccess ||
         cudaMallocHost(&s->ctl_host, sizeof(Control)) != cudaSuccess)
         return bail(RMHD2D_ERR_CUDA, "device allocation failed");
+    if (cfg->ct_scheme == RMHD2D_CT_CONTACT) {
+        const size_t cbytes = (size_t)g.plane * (5 * NFIELD + 2) * sizeof(double);
+        if (cudaMalloc(&s->contact, cbytes) != cudaSuccess || cudaMemset(s->contact, 0, cbytes) != cudaSuccess)
+            return bail(RMHD2D_ERR_CUDA, "device allocation failed (CT-Contact workspace)");
+    }
     // Zero the planes so padding columns hold finite values.
     if (cudaMemset(s->A, 0, state_bytes) != cudaSuccess || cudaMemset(s->B, 0, state_bytes) != cudaSuccess ||
         cudaMemset(s->row2, 0, (size_t)g.nx * sizeof(double)) != cudaSuccess ||
@@ -414,6 +444,7 @@ static int destroy_solver(rmhd2d_solver *s)
     cudaFree(s->eta);
     cudaFree(s->row2);
     cudaFree(s->ctl);
+    cudaFree(s->contact);
     free_adjoint(s->adj);
     if (s->ctl_host) cudaFreeHost(s->ctl_host);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
@@ -571,6 +602,7 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
 {
     if (!s || !ms4) return fail(s, RMHD2D_ERR_INVALID, "null argument");
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
+    if (s->contact) return fail(s, RMHD2D_ERR_STATE, "profile_step times the four launches of the stage-1-EMF step");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
     cudaEvent_t ev[5];
@@ -899,6 +931,9 @@ int rmhd2d_batch_create(const rmhd2d_config *cfgs, int nruns, rmhd2d_batch **out
     for (int r = 1; r < nruns; ++r)
         if (cfgs[r].precision != cfgs[0].precision || cfgs[r].device != cfgs[0].device)
             return bfail(b, RMHD2D_ERR_INVALID, "all runs of a batch share precision and device");
+    for (int r = 0; r < nruns; ++r)
+        if (cfgs[r].ct_scheme != RMHD2D_CT_STAGE1)
+            return bfail(b, RMHD2D_ERR_INVALID, "batched runs use the stage-1-EMF step (ct_scheme 0)");
     b = new rmhd2d_batch();
     b->device = cfgs[0].device;
     b->precision = cfgs[0].precision;
@@ -1177,6 +1212,7 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
     if (nsteps < 1) return fail(s, RMHD2D_ERR_INVALID, "nsteps must be >= 1");
     if (s->g.bc_x != BC_PERIODIC || s->g.bc_y != BC_PERIODIC)
         return fail(s, RMHD2D_ERR_INVALID, "the discrete adjoint is implemented for periodic x and y walls");
+    if (s->contact) return fail(s, RMHD2D_ERR_INVALID, "the discrete adjoint differentiates the stage-1-EMF step");
     CK(cudaSetDevice(s->device));
     int interval = checkpoint_interval;
     if (interval <= 0) interval = (int)std::ceil(std::sqrt((double)nsteps));

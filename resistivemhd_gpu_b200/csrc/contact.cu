@@ -1,0 +1,369 @@
+// contact.cu -- the step with the CT-Contact EMF (cfg.ct_scheme =
+// RMHD2D_CT_CONTACT), compiled with -fmad=false: FP64 in the reference's
+// evaluation order, bit-identical to the oracle's orc_step_contact.
+//
+// The step follows the multi-GPU library's ordering
+// (ResistiveMHD_multiGPU_cuda/ResistiveMHD2D_GPU/resistiveMHD2D.cu:147-221)
+// with its corner EMF (ct.cu:26-257), on this library's fluxes, update ranges
+// and dt:
+//   begin        dt (CFL or the fixed dt), the control block's step fields
+//   flux         F, G of the cell-centred U^n (HLLD, MUSCL, resistive hook)
+//   ref (old)    per-cell reference EMF u bY - v bX - eta jZ of U^n with the
+//                face B that shift + back-to-face leave (smoothed)
+//   update 1     U* = U^n - dt div(F, G) for all 8 fields (smoothed face B)
+//   boundary     U*
+//   flux         F, G of the cell-centred U*
+//   update 2     C = (U^n + U* - dt div(F, G)) / 2 (both with smoothed face B)
+//   boundary     C
+//   ref (now)    per-cell reference EMF of C
+//   CT           A = C with face B = U^n's faces - dt curl(Ez), Ez the mean of
+//                the two stages' contact EMFs
+//   boundary     A, then the CFL rate and NaN test of every cell
+// Flux entries whose stencil leaves the grid, and the EMF inputs outside
+// 0 < i < nx-1, 0 < j < ny-1, are NaN, as the oracle leaves them: they reach
+// only ghost cells, which the boundary passes overwrite.
+#include <cuda_runtime.h>
+
+#include "adjoint_core.cuh"
+#include "aux_kernels.h"
+#include "contact.h"
+#include "physics.cuh"
+#include "rmhd2d_internal.h"
+
+namespace rmhd2d {
+
+namespace {
+
+__device__ __forceinline__ long long at(const Grid &g, int i, int j) { return (long long)i * g.pitch + j; }
+
+__device__ __forceinline__ double qnan() { return bits_to_double(0x7FF8000000000000ull); }
+
+// shiftUToCenterForCT (resistiveMHD_2D.cu:313-368)
+__device__ __forceinline__ double bx_c(const Grid &g, const double *U, int i, int j)
+{
+    const double *b = U + BXF * g.plane;
+    return i >= 1 ? 0.5 * (b[at(g, i, j)] + b[at(g, i - 1, j)]) : b[at(g, i, j)];
+}
+__device__ __forceinline__ double by_c(const Grid &g, const double *U, int i, int j)
+{
+    const double *b = U + BYF * g.plane;
+    return j >= 1 ? 0.5 * (b[at(g, i, j)] + b[at(g, i, j - 1)]) : b[at(g, i, j)];
+}
+// then backUToCenterHalfForCT (resistiveMHD_2D.cu:371-426): the face value
+// the two leave in U
+__device__ __forceinline__ double bx_s(const Grid &g, const double *U, int i, int j)
+{
+    return i < g.nx - 1 ? 0.5 * (bx_c(g, U, i, j) + bx_c(g, U, i + 1, j)) : bx_c(g, U, i, j);
+}
+__device__ __forceinline__ double by_s(const Grid &g, const double *U, int i, int j)
+{
+    return j < g.ny - 1 ? 0.5 * (by_c(g, U, i, j) + by_c(g, U, i, j + 1)) : by_c(g, U, i, j);
+}
+
+// A cell of the cell-centred state in sweep order (hlld.cu:134-160 shuffles
+// the y sweep's cell to rho, rhoV, rhoW, rhoU, bY, bZ, bX, e).
+template <int DIR>
+__device__ __forceinline__ void sweep_cell(const Grid &g, const double *U, int i, int j, double *c)
+{
+    const long long k = at(g, i, j), P = g.plane;
+    if (DIR == 0) {
+        c[0] = U[RHO * P + k]; c[1] = U[MX * P + k]; c[2] = U[MY * P + k]; c[3] = U[MZ * P + k];
+        c[4] = bx_c(g, U, i, j); c[5] = by_c(g, U, i, j); c[6] = U[BZF * P + k]; c[7] = U[EN * P + k];
+    } else {
+        c[0] = U[RHO * P + k]; c[1] = U[MY * P + k]; c[2] = U[MZ * P + k]; c[3] = U[MX * P + k];
+        c[4] = by_c(g, U, i, j); c[5] = U[BZF * P + k]; c[6] = bx_c(g, U, i, j); c[7] = U[EN * P + k];
+    }
+}
+
+// HLLD::calculateFluxF / G (hlld.cu:110-233) + the resistive hook
+// (main_plasmoid.cu:175-290) at interface (i, j), natural field order.
+template <int DIR>
+__device__ void interface_flux(const Grid &g, const double *U, const double *eta, int i, int j, double *out)
+{
+    double cell[5][8], q[4][8];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) sweep_cell<DIR>(g, U, DIR == 0 ? i + m - 1 : i, DIR == 0 ? j : j + m - 1, cell[m]);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) adj::basic_param(cell[m], cell[m + 1][4], g.gamma, q[m]);
+    double L[8], R[8], f[8];
+    adj::muscl_states(q[0], q[1], q[2], q[3], g.eps, L, R);
+    const Prim PL{L[0], L[1], L[2], L[3], L[4], L[5], L[6], L[7]};
+    const Prim PR{R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7]};
+    hlld_flux<true>(PL, PR, g.gamma, g.eps, f);
+    if (DIR == 0) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) out[c] = f[c];
+    } else {
+        // shuffleForFluxG_kernel: the y flux from the permuted one
+        out[0] = f[0]; out[1] = f[3]; out[2] = f[1]; out[3] = f[2];
+        out[4] = f[6]; out[5] = f[4]; out[6] = f[5]; out[7] = f[7];
+    }
+    if (i < 1 || i > g.nx - 3 || j < 1 || j > g.ny - 3) return;   // the hook's 0 < i < nx-2, 0 < j < ny-2
+    const long long P = g.plane;
+    auto bz = [&](int ii, int jj) { return U[BZF * P + at(g, ii, jj)]; };
+    const double two_dx = 2.0 * g.dx, two_dy = 2.0 * g.dy;
+    if (DIR == 0) {
+        double jY, jZ, e;
+        jY = -(bz(i + 1, j) - bz(i - 1, j)) / two_dx;
+        jZ = (by_c(g, U, i + 1, j) - by_c(g, U, i - 1, j)) / two_dx - (bx_c(g, U, i, j + 1) - bx_c(g, U, i, j - 1)) / two_dy;
+        e = eta ? eta[at(g, i, j)] : g.eta;
+        const double etaJY = e * jY, etaJZ = e * jZ;
+        const double etaJYBZ = etaJY * bz(i, j), etaJZBY = etaJZ * by_c(g, U, i, j);
+        jY = -(bz(i + 2, j) - bz(i, j)) / two_dx;
+        jZ = (by_c(g, U, i + 2, j) - by_c(g, U, i, j)) / two_dx
+           - (bx_c(g, U, i + 1, j + 1) - bx_c(g, U, i + 1, j - 1)) / two_dy;
+        e = eta ? eta[at(g, i + 1, j)] : g.eta;
+        const double etaJYPlus1 = e * jY, etaJZPlus1 = e * jZ;
+        const double etaJYBZPlus1 = etaJYPlus1 * bz(i + 1, j), etaJZBYPlus1 = etaJZPlus1 * by_c(g, U, i + 1, j);
+        out[5] -= 0.5 * (etaJZ + etaJZPlus1);
+        out[6] += 0.5 * (etaJY + etaJYPlus1);
+        out[7] += 0.5 * (etaJYBZ + etaJYBZPlus1) - 0.5 * (etaJZBY + etaJZBYPlus1);
+    } else {
+        double jX, jZ, e;
+        jX = (bz(i, j + 1) - bz(i, j - 1)) / two_dy;
+        jZ = (by_c(g, U, i + 1, j) - by_c(g, U, i - 1, j)) / two_dx - (bx_c(g, U, i, j + 1) - bx_c(g, U, i, j - 1)) / two_dy;
+        e = eta ? eta[at(g, i, j)] : g.eta;
+        const double etaJX = e * jX, etaJZ = e * jZ;
+        const double etaJXBZ = etaJX * bz(i, j), etaJZBX = etaJZ * bx_c(g, U, i, j);
+        jX = (bz(i, j + 2) - bz(i, j)) / two_dy;
+        jZ = (by_c(g, U, i + 1, j + 1) - by_c(g, U, i - 1, j + 1)) / two_dx
+           - (bx_c(g, U, i, j + 2) - bx_c(g, U, i, j)) / two_dy;
+        e = eta ? eta[at(g, i, j + 1)] : g.eta;
+        const double etaJXPlus1 = e * jX, etaJZPlus1 = e * jZ;
+        const double etaJXBZPlus1 = etaJXPlus1 * bz(i, j + 1), etaJZBXPlus1 = etaJZPlus1 * bx_c(g, U, i, j + 1);
+        out[4] += 0.5 * (etaJZ + etaJZPlus1);
+        out[6] -= 0.5 * (etaJX + etaJXPlus1);
+        out[7] += 0.5 * (etaJZBX + etaJZBXPlus1) - 0.5 * (etaJXBZ + etaJXBZPlus1);
+    }
+}
+
+__global__ void contact_begin_kernel(Grid g, Control *ctl, int parity)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double dt = ctl->use_fixed_dt
+                          ? ctl->dt_fixed
+                          : step_dt(ctl->amax[parity], ctl->first_nan[parity], g.dx, g.dy, g.eps, g.eta, g.cfl);
+    ctl->dt = dt;
+    ctl->total_time = ctl->total_time + dt;
+    ctl->amax[parity ^ 1] = 0ull;
+    ctl->first_nan[parity ^ 1] = 0;
+    ctl->crashed = 0;
+}
+
+// F (grid.y = 0) or G (grid.y = 1) of every interface: the x sweep is
+// defined for 1 <= i <= nx-4, the y sweep for 1 <= j <= ny-3 (the ranges the
+// reference's buffers hold current values in), NaN elsewhere.
+__global__ void __launch_bounds__(128) contact_flux_kernel(Grid g, const double *U, const double *eta, double *F,
+                                                           double *G)
+{
+    const int dir = blockIdx.y;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)g.nx * g.ny) return;
+    const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
+    double f[8];
+    const bool ok = dir == 0 ? (i >= 1 && i <= g.nx - 4) : (j >= 1 && j <= g.ny - 3);
+    if (ok) {
+        if (dir == 0) interface_flux<0>(g, U, eta, i, j, f);
+        else interface_flux<1>(g, U, eta, i, j, f);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) f[c] = qnan();
+    }
+    double *out = (dir == 0 ? F : G) + at(g, i, j);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) out[c * g.plane] = f[c];
+}
+
+// ct.cu:45-61: reference EMF u bY - v bX - eta jZ of cell (i, j) for
+// 0 < i < nx-1, 0 < j < ny-1, from U's face B, smoothed (stage 1) or as
+// stored (stage 2).
+template <bool SMOOTHED>
+__global__ void contact_ref_kernel(Grid g, const double *U, const double *eta, double *ref)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)g.nx * g.ny) return;
+    const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
+    const long long k = at(g, i, j), P = g.plane;
+    if (!(i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1)) {
+        ref[k] = qnan();
+        return;
+    }
+    auto BX = [&](int ii, int jj) { return SMOOTHED ? bx_s(g, U, ii, jj) : U[BXF * P + at(g, ii, jj)]; };
+    auto BY = [&](int ii, int jj) { return SMOOTHED ? by_s(g, U, ii, jj) : U[BYF * P + at(g, ii, jj)]; };
+    const double dx = g.dx, dy = g.dy;
+    const double rho = U[RHO * P + k];
+    const double u = U[MX * P + k] / rho;
+    const double v = U[MY * P + k] / rho;
+    const double bX = 0.5 * (BX(i, j) + BX(i - 1, j));
+    const double bY = 0.5 * (BY(i, j) + BY(i, j - 1));
+    const double jZ = 0.25 * (
+        (BY(i + 1, j) - BY(i, j)) / dx - (BX(i, j + 1) - BX(i, j)) / dy
+      + (BY(i + 1, j - 1) - BY(i, j - 1)) / dx - (BX(i, j) - BX(i, j - 1)) / dy
+      + (BY(i, j - 1) - BY(i - 1, j - 1)) / dx - (BX(i - 1, j) - BX(i - 1, j - 1)) / dy
+      + (BY(i, j) - BY(i - 1, j)) / dx - (BX(i - 1, j + 1) - BX(i - 1, j)) / dy);
+    const double e = eta ? eta[k] : g.eta;
+    ref[k] = u * bY - v * bX - e * jZ;
+}
+
+// The stage updates (resistiveMHD_2D.cu:53-130 functors, over k >= ny), all
+// 8 fields, face B as shift + back-to-face leave it.
+template <int STAGE>
+__global__ void contact_update_kernel(Grid g, const double *Un, const double *Ub, const double *F, const double *G,
+                                      const Control *ctl, double *dst)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)g.nx * g.ny) return;
+    const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
+    const long long k = at(g, i, j), P = g.plane;
+    if (i == 0) {
+        // outside the update range: stage 1 keeps U^n (copied before the
+        // smoothing); stage 2 keeps U^n as the smoothing left it
+#pragma unroll
+        for (int c = 0; c < NFIELD; ++c) {
+            double v = Un[c * P + k];
+            if (STAGE == 2 && c == BXF) v = bx_s(g, Un, i, j);
+            if (STAGE == 2 && c == BYF) v = by_s(g, Un, i, j);
+            dst[c * P + k] = v;
+        }
+        return;
+    }
+    const double dt = ctl->dt;
+    const double rdx = dt / g.dx, rdy = dt / g.dy;
+    const long long km = at(g, i - 1, j);
+#pragma unroll
+    for (int c = 0; c < NFIELD; ++c) {
+        // the flat k - 1 neighbour of j = 0 is the previous column's last
+        // cell, whose G entry is NaN
+        const double gm = j >= 1 ? G[c * P + k - 1] : qnan();
+        const double div = rdx * (F[c * P + k] - F[c * P + km]);
+        const double dvg = rdy * (G[c * P + k] - gm);
+        double u = Un[c * P + k];
+        if (c == BXF) u = bx_s(g, Un, i, j);
+        if (c == BYF) u = by_s(g, Un, i, j);
+        if (STAGE == 1) {
+            dst[c * P + k] = u - div - dvg;
+        } else {
+            double ub = Ub[c * P + k];
+            if (c == BXF) ub = bx_s(g, Ub, i, j);
+            if (c == BYF) ub = by_s(g, Ub, i, j);
+            dst[c * P + k] = 0.5 * (u + ub - div - dvg);
+        }
+    }
+}
+
+__device__ __forceinline__ int isgn(double x) { return (x > 0.0) - (x < 0.0); }
+
+// One stage's inputs of the contact EMF (ct.cu:26-65), NaN outside
+// 0 < i < nx-1, 0 < j < ny-1.
+struct StageEmf {
+    const double *F, *G, *ref;
+    __device__ __forceinline__ bool in(const Grid &g, int i, int j) const
+    {
+        return i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1;
+    }
+    __device__ __forceinline__ double NF5(const Grid &g, int i, int j) const
+    {
+        return in(g, i, j) ? F[BYF * g.plane + at(g, i, j)] : qnan();
+    }
+    __device__ __forceinline__ double NG4(const Grid &g, int i, int j) const
+    {
+        return in(g, i, j) ? G[BXF * g.plane + at(g, i, j)] : qnan();
+    }
+    __device__ __forceinline__ double NF0(const Grid &g, int i, int j) const
+    {
+        return in(g, i, j) ? F[RHO * g.plane + at(g, i, j)] : qnan();
+    }
+    __device__ __forceinline__ double NG0(const Grid &g, int i, int j) const
+    {
+        return in(g, i, j) ? G[RHO * g.plane + at(g, i, j)] : qnan();
+    }
+    __device__ __forceinline__ double CF5(const Grid &g, int i, int j) const
+    {
+        return in(g, i, j) ? ref[at(g, i, j)] : qnan();
+    }
+    __device__ __forceinline__ double CG4(const Grid &g, int i, int j) const
+    {
+        return in(g, i, j) ? -(ref[at(g, i, j)]) : qnan();
+    }
+};
+
+// ct.cu:147-169: the corner (i+1/2, j+1/2) EMF of one stage.
+__device__ double contact_corner(const Grid &g, const StageEmf &s, int i, int j)
+{
+    const double avg = 0.25 * (-s.NF5(g, i, j) - s.NF5(g, i, j + 1) + s.NG4(g, i, j) + s.NG4(g, i + 1, j));
+    const int sF0 = isgn(s.NF0(g, i, j)), sF0n = isgn(s.NF0(g, i, j + 1));
+    const int sG0 = isgn(s.NG0(g, i, j)), sG0e = isgn(s.NG0(g, i + 1, j));
+    const double eS = (1.0 + sF0) * (s.NG4(g, i, j) - s.CG4(g, i, j))
+                    + (1.0 - sF0) * (s.NG4(g, i + 1, j) - s.CG4(g, i + 1, j));
+    const double eN = (1.0 + sF0n) * (s.CG4(g, i, j + 1) - s.NG4(g, i, j))
+                    + (1.0 - sF0n) * (s.CG4(g, i + 1, j + 1) - s.NG4(g, i + 1, j));
+    const double eW = -(1.0 + sG0) * (s.NF5(g, i, j) - s.CF5(g, i, j))
+                    - (1.0 - sG0) * (s.NF5(g, i, j + 1) - s.CF5(g, i, j + 1));
+    const double eE = -(1.0 + sG0e) * (s.CF5(g, i + 1, j) - s.NF5(g, i, j))
+                    - (1.0 - sG0e) * (s.CF5(g, i + 1, j + 1) - s.NF5(g, i, j + 1));
+    return avg + 0.125 * (eS - eN + eW - eE);
+}
+
+// ct.cu:195: the mean of the two stages' EMFs, defined for i < nx-1,
+// j < ny-1.
+__device__ __forceinline__ double corner_ez(const Grid &g, const StageEmf &o, const StageEmf &n, int i, int j)
+{
+    if (i < 0 || j < 0 || i >= g.nx - 1 || j >= g.ny - 1) return qnan();
+    return 0.5 * (contact_corner(g, o, i, j) + contact_corner(g, n, i, j));
+}
+
+// ct.cu:200-218 CT_kernel on the step input's faces (A), the rest of the
+// state from the stage-2 result C.
+__global__ void contact_ct_kernel(Grid g, StageEmf o, StageEmf n, const double *C, const Control *ctl, double *A)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)g.nx * g.ny) return;
+    const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
+    const long long k = at(g, i, j), P = g.plane;
+#pragma unroll
+    for (int c = 0; c < NFIELD; ++c)
+        if (c != BXF && c != BYF) A[c * P + k] = C[c * P + k];
+    if (i > 0 && j > 0) {
+        const double dt = ctl->dt;
+        const double ez = corner_ez(g, o, n, i, j);
+        A[BXF * P + k] = A[BXF * P + k] - dt / g.dy * (ez - corner_ez(g, o, n, i, j - 1));
+        A[BYF * P + k] = A[BYF * P + k] + dt / g.dx * (ez - corner_ez(g, o, n, i - 1, j));
+    } else {
+        A[BXF * P + k] = C[BXF * P + k];
+        A[BYF * P + k] = C[BYF * P + k];
+    }
+}
+
+int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+}  // namespace
+
+void enqueue_contact_step(const ContactStep &c, cudaStream_t st)
+{
+    const Grid &g = c.g;
+    const long long n = (long long)g.nx * g.ny;
+    const int b128 = blocks_for(n, 128), b256 = blocks_for(n, 256);
+    auto boundary = [&](double *state) {
+        if (g.bc_x == BC_SYMMETRIC) launch_snapshot_row2(g, state, c.row2, st);
+        launch_boundary(g, state, c.row2, nullptr, 0, st);
+    };
+    contact_begin_kernel<<<1, 32, 0, st>>>(g, c.ctl, c.parity);
+    // stage 1
+    contact_flux_kernel<<<dim3(b128, 2), 128, 0, st>>>(g, c.A, c.eta, c.F1, c.G1);
+    contact_ref_kernel<true><<<b256, 256, 0, st>>>(g, c.A, c.eta, c.R1);
+    contact_update_kernel<1><<<b256, 256, 0, st>>>(g, c.A, nullptr, c.F1, c.G1, c.ctl, c.B);
+    boundary(c.B);
+    // stage 2
+    contact_flux_kernel<<<dim3(b128, 2), 128, 0, st>>>(g, c.B, c.eta, c.F2, c.G2);
+    contact_update_kernel<2><<<b256, 256, 0, st>>>(g, c.A, c.B, c.F2, c.G2, c.ctl, c.C);
+    boundary(c.C);
+    contact_ref_kernel<false><<<b256, 256, 0, st>>>(g, c.C, c.eta, c.R2);
+    // CT with the two stages' mean contact EMF, then the boundary and the
+    // next step's CFL rate and crash flag
+    contact_ct_kernel<<<b256, 256, 0, st>>>(g, StageEmf{c.F1, c.G1, c.R1}, StageEmf{c.F2, c.G2, c.R2}, c.C, c.ctl,
+                                             c.A);
+    boundary(c.A);
+    launch_rate(g, c.A, c.ctl, c.parity ^ 1, 1, st);
+}
+
+}  // namespace rmhd2d

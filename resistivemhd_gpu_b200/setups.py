@@ -68,6 +68,7 @@ class Setup:
     xmin: float = 0.0
     ymin: float = 0.0
     bc_y: str | None = None      # y walls, None for the same as bc
+    ct: str = "stage1"           # "stage1": CT with the stage-1 EMF; "contact": CT-Contact EMF
 
     @property
     def nx(self) -> int:

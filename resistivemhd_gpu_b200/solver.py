@@ -34,7 +34,7 @@ class Solver:
 
     def __init__(self, nx: int, ny: int, dx: float, dy: float, *, gamma: float = 5.0 / 3.0, cfl: float = 0.4,
                  eps: float = 1e-20, eta: float = 0.0, bc: str = "periodic", bc_y: str | None = None,
-                 precision: str = "fp64_exact", device: int = 0, stream: int | None = None):
+                 precision: str = "fp64_exact", device: int = 0, stream: int | None = None, ct: str = "stage1"):
         lib = _lib.load()
         cfg = _lib.Config()
         lib.rmhd2d_config_default(ctypes.byref(cfg))
@@ -49,6 +49,9 @@ class Solver:
         cfg.precision = _lib.PRECISION[precision]
         cfg.device = int(device)
         cfg.stream = stream
+        if ct not in _lib.CT:
+            raise ValueError(f"unknown CT scheme {ct!r}")
+        cfg.ct_scheme = _lib.CT[ct]
         h = ctypes.c_void_p()
         _lib.check(lib.rmhd2d_create(ctypes.byref(cfg), ctypes.byref(h)), None)
         self._lib = lib
@@ -59,7 +62,7 @@ class Solver:
 
     @staticmethod
     def make_config(nx, ny, dx, dy, *, gamma=5.0 / 3.0, cfl=0.4, eps=1e-20, eta=0.0, bc="periodic", bc_y=None,
-                    precision="fp64_exact", device=0) -> "_lib.Config":
+                    precision="fp64_exact", device=0, ct="stage1") -> "_lib.Config":
         lib = _lib.load()
         cfg = _lib.Config()
         lib.rmhd2d_config_default(ctypes.byref(cfg))
@@ -69,6 +72,7 @@ class Solver:
         cfg.bc_y = -1 if bc_y is None else _lib.BC[bc_y]
         cfg.precision = _lib.PRECISION[precision]
         cfg.device = int(device)
+        cfg.ct_scheme = _lib.CT[ct]
         return cfg
 
     @classmethod
@@ -85,7 +89,8 @@ class Solver:
     def from_setup(cls, setup, precision: str = "fp64_exact", device: int = 0, apply_boundary: bool = True,
                    stream: int | None = None) -> "Solver":
         s = cls(setup.nx, setup.ny, setup.dx, setup.dy, gamma=setup.gamma, cfl=setup.cfl, eps=setup.eps,
-                eta=setup.eta, bc=setup.bc, bc_y=setup.bc_y, precision=precision, device=device, stream=stream)
+                eta=setup.eta, bc=setup.bc, bc_y=setup.bc_y, precision=precision, device=device, stream=stream,
+                ct=getattr(setup, "ct", "stage1"))
         if setup.eta_table is not None:
             s.set_eta_table(setup.eta_table)
         s.set_state(setup.state, apply_boundary=apply_boundary)
@@ -250,7 +255,8 @@ class Batch:
         cfgs = (_lib.Config * len(setups))()
         for r, s in enumerate(setups):
             cfgs[r] = Solver.make_config(s.nx, s.ny, s.dx, s.dy, gamma=s.gamma, cfl=s.cfl, eps=s.eps, eta=s.eta,
-                                         bc=s.bc, bc_y=s.bc_y, precision=precision, device=device)
+                                         bc=s.bc, bc_y=s.bc_y, precision=precision, device=device,
+                                         ct=getattr(s, "ct", "stage1"))
         h = ctypes.c_void_p()
         _lib.check_batch(lib.rmhd2d_batch_create(cfgs, len(setups), ctypes.byref(h)), None)
         self._lib, self._h = lib, h
@@ -345,9 +351,9 @@ class ResistiveMHD2D:
 
     def __init__(self, nx: int, ny: int, dx: float, dy: float, *, gamma_mhd: float = 5.0 / 3.0, CFL: float = 0.4,
                  EPS: float = 1e-20, eta: float = 0.0, boundary: str = "periodic", boundary_y: str | None = None,
-                 eta_table=None, precision: str = "fp64_exact", device: int = 0):
+                 eta_table=None, precision: str = "fp64_exact", device: int = 0, ct: str = "stage1"):
         self._s = Solver(nx, ny, dx, dy, gamma=gamma_mhd, cfl=CFL, eps=EPS, eta=eta, bc=boundary, bc_y=boundary_y,
-                         precision=precision, device=device)
+                         precision=precision, device=device, ct=ct)
         if eta_table is not None:
             self._s.set_eta_table(eta_table)
         self.nx, self.ny = nx, ny
