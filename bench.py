@@ -32,6 +32,8 @@ Extra blocks of the same JSON line (each can be switched off):
              forward, recorded forward and backward times and their ratios
              for the FP32-bulk and FP64 forwards, and central differences
              (h = 1e-6) through the FP64 forward on 32 seeded directions.
+  ct_contact the CT-Contact step (cfg.ct_scheme) on the headline workload
+             against the stage-1-EMF step, both in FP64 without contraction.
   ensemble   256 independent periodic runs (Orszag-Tang / Kelvin-Helmholtz,
              n^2 with n in {128..512}, eta log-uniform in [1e-4, 1e-2], 500
              steps) in one persistent batch in FP32-bulk, against the FP64
@@ -329,6 +331,8 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
             line["cpu_baseline"] = {"unavailable": str(e)[:200]}
     if world == 1 and args.precision_block:
         line["precision"] = precision_block(args, setup, label, local_rank)
+    if world == 1 and args.contact_block:
+        line["ct_contact"] = contact_block(args, setup, label, local_rank)
     if world == 1 and args.adjoint_block:
         line["adjoint"] = adjoint_block(args, local_rank)
     if args.ensemble_block:
@@ -518,6 +522,27 @@ def _fd_control(local_rank, h, n=128, nsteps=20, ndirs=16):
             "frac_le_1e-6": float((errs <= 1e-6).mean())}
 
 
+def contact_block(args, setup, label, local_rank):
+    """The CT-Contact step on the headline workload, against the
+    stage-1-EMF step in the same arithmetic (FP64 without contraction)."""
+    import dataclasses
+
+    from resistivemhd_gpu_b200 import Solver
+
+    out = {"workload": label, "steps": args.steps}
+    for ct in ("stage1", "contact"):
+        s = dataclasses.replace(setup, ct=ct)
+        with Solver.from_setup(s, precision="fp64_exact", device=local_rank) as sol:
+            sol.run(args.warmup)
+            ms = sol.run_timed(args.steps)
+            out[ct] = {"value": setup.interior_cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                       "crashed": sol.check_crashed()}
+    out["contact_over_stage1_time"] = out["contact"]["ms_per_step"] / out["stage1"]["ms_per_step"]
+    out["note"] = ("CT-Contact runs as 12 unfused launches per step (fluxes to HBM, per-cell EMF inputs, one "
+                   "CT at the end); the stage-1-EMF step is the fused 4-launch pipeline")
+    return out
+
+
 def _shard(setups_list, world):
     """Greedy largest-first assignment of runs to ranks by cell count."""
     order = sorted(range(len(setups_list)), key=lambda r: -setups_list[r].interior_cells)
@@ -595,11 +620,13 @@ def main() -> None:
     ap.add_argument("--no-baselines", dest="baselines", action="store_false")
     ap.add_argument("--no-precision", dest="precision_block", action="store_false")
     ap.add_argument("--no-adjoint", dest="adjoint_block", action="store_false")
+    ap.add_argument("--no-contact", dest="contact_block", action="store_false")
     ap.add_argument("--no-ensemble", dest="ensemble_block", action="store_false")
     ap.add_argument("--quick", action="store_true", help="headline only (no extra blocks, baselines or e2e)")
     args = ap.parse_args()
     if args.quick:
-        args.precision_block = args.adjoint_block = args.ensemble_block = args.baselines = args.e2e = False
+        args.precision_block = args.adjoint_block = args.ensemble_block = args.contact_block = False
+        args.baselines = args.e2e = False
     if args.warmup < 3:
         args.warmup = 3
 
