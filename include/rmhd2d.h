@@ -47,7 +47,15 @@ typedef enum {
 
 typedef enum {
     RMHD2D_BC_PERIODIC = 0,     /* Boundary::periodicBoundaryX2nd/Y2nd (TP boundary.cu:4-141) */
-    RMHD2D_BC_SYMMETRIC = 1     /* Boundary::symmetricBoundaryX2nd/Y2nd (TS boundary.cu:4-206) */
+    RMHD2D_BC_SYMMETRIC = 1,    /* Boundary::symmetricBoundaryX2nd/Y2nd (TS boundary.cu:4-206): mirror copies,
+                                   normal-B ghosts integrated from div B = 0 */
+    /* The multi-GPU library's walls (ResistiveMHD_multiGPU_cuda/ResistiveMHD2D_GPU/boundary.cu): */
+    RMHD2D_BC_ZERO_GRADIENT = 2,/* copies of the nearest interior cell (its symmetricBoundaryY2nd, :292-337;
+                                   the x = xmax side of its flare wall); x or y walls */
+    RMHD2D_BC_WALL = 3,         /* conducting wall (wallBoundaryY2nd, :48-119): the first interior cell's density,
+                                   pressure, normal B and bZ with zero velocity and bY; y walls only */
+    RMHD2D_BC_FLARE = 4         /* flareBoundaryX2nd (:196-245): line-tied at x = xmin (the wall state keeping v),
+                                   zero gradient at x = xmax; x walls only */
 } rmhd2d_bc;
 
 typedef enum {
@@ -90,8 +98,10 @@ typedef struct {
     double eps;                 /* EPS regulariser of the reference (const.hpp:4) */
     double eta;                 /* scalar eta: the resistive term when no eta table is set,
                                    and always the diffusive dt limit dx^2/eta (resistiveMHD_2D.cu:288) */
-    int bc;                     /* rmhd2d_bc of the x walls (and of the y walls when bc_y = -1) */
-    int bc_y;                   /* rmhd2d_bc of the y walls, or -1 for the same as bc; periodic x with
+    int bc;                     /* rmhd2d_bc of the x walls (and of the y walls when bc_y = -1);
+                                   PERIODIC, SYMMETRIC, ZERO_GRADIENT or FLARE */
+    int bc_y;                   /* rmhd2d_bc of the y walls (PERIODIC, SYMMETRIC, ZERO_GRADIENT or WALL),
+                                   or -1 for the same as bc; periodic x with
                                    symmetric y is the reference's oneStepRK2PeriodicXSymmetricY
                                    (lib_ResistiveMHD_2D_GPU_single/resistiveMHD_2D.cu:198-259) */
     int precision;              /* rmhd2d_precision */

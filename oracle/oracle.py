@@ -25,7 +25,7 @@ LIB = HERE / "liborc.so"
 TANGENT_LIB = HERE / "libtangent.so"
 REF_DIR = HERE / "_ref"
 
-BC = {"periodic": 0, "symmetric": 1}
+BC = {"periodic": 0, "symmetric": 1, "zero_gradient": 2, "wall": 3, "flare": 4}
 
 
 class _Params(ctypes.Structure):

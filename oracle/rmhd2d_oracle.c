@@ -583,16 +583,91 @@ static void symmetric_y(const orc_params *p, double *U)
 }
 #undef C
 
+/* The multi-GPU library's walls (ResistiveMHD_multiGPU_cuda/
+   ResistiveMHD2D_GPU/boundary.cu:48-355), with its 3 ghost layers. */
+
+/* The resting wall state built from cell c (boundary.cu:63-84): density,
+   normal B and bZ kept, velocity and tangential bY set to 0, energy rebuilt
+   from the cell's pressure. */
+static void mc_wall_state(const double *c, double gm, double *out)
+{
+    double rho = c[RHO];
+    double u = c[MX] / rho, v = c[MY] / rho, w = c[MZ] / rho;
+    double bX = c[BXF], bY = c[BYF], bZ = c[BZF], e = c[EN];
+    double p = (gm - 1.0) * (e - 0.5 * rho * (u * u + v * v + w * w) - 0.5 * (bX * bX + bY * bY + bZ * bZ));
+    out[RHO] = rho;
+    out[MX] = rho * 0.0; out[MY] = rho * 0.0; out[MZ] = rho * 0.0;
+    out[BXF] = bX; out[BYF] = 0.0; out[BZF] = bZ;
+    out[EN] = p / (gm - 1.0) + 0.5 * rho * (0.0 * 0.0 + 0.0 * 0.0 + 0.0 * 0.0) + 0.5 * (bX * bX + 0.0 * 0.0 + bZ * bZ);
+}
+
+/* The line-tied state of the flare's x = xmin wall (boundary.cu:212-229):
+   as the wall state but keeping the cell's v. */
+static void mc_flare_state(const double *c, double gm, double *out)
+{
+    double rho = c[RHO];
+    double u = c[MX] / rho, v = c[MY] / rho, w = c[MZ] / rho;
+    double bX = c[BXF], bY = c[BYF], bZ = c[BZF], e = c[EN];
+    double p = (gm - 1.0) * (e - 0.5 * rho * (u * u + v * v + w * w) - 0.5 * (bX * bX + bY * bY + bZ * bZ));
+    out[RHO] = rho;
+    out[MX] = rho * 0.0; out[MY] = rho * v; out[MZ] = rho * 0.0;
+    out[BXF] = bX; out[BYF] = 0.0; out[BZF] = bZ;
+    out[EN] = p / (gm - 1.0) + 0.5 * rho * (0.0 * 0.0 + v * v + 0.0 * 0.0) + 0.5 * (bX * bX + 0.0 * 0.0 + bZ * bZ);
+}
+
+/* boundary.cu:196-245 flareBoundaryX2nd_U: line-tied at x = xmin, copies of
+   the last interior column at x = xmax; every row.  With flare = 0 both
+   sides are copies (the zero-gradient wall). */
+static void mc_x_pass(const orc_params *p, double *U, int flare)
+{
+    const int nx = p->nx, ny = p->ny;
+    for (int j = 0; j < ny; ++j) {
+        double wl[NV];
+        const double *c3 = &U[(j + 3 * ny) * NV];
+        if (flare) mc_flare_state(c3, p->gamma, wl);
+        else memcpy(wl, c3, sizeof(wl));
+        for (int g = 0; g < 3; ++g) memcpy(&U[(j + g * ny) * NV], wl, sizeof(wl));
+        double wr[NV];
+        memcpy(wr, &U[(j + (nx - 4) * ny) * NV], sizeof(wr));
+        for (int g = 0; g < 3; ++g) memcpy(&U[(j + (nx - 1 - g) * ny) * NV], wr, sizeof(wr));
+    }
+}
+
+/* boundary.cu:48-119 wallBoundaryY2nd_U (wall = 1) and boundary.cu:292-337
+   symmetricBoundaryY2nd_U, the zero-gradient copy (wall = 0); every column. */
+static void mc_y_pass(const orc_params *p, double *U, int wall)
+{
+    const int nx = p->nx, ny = p->ny;
+    for (int i = 0; i < nx; ++i) {
+        double lo[NV], hi[NV];
+        const double *c3 = &U[(3 + i * ny) * NV], *cn = &U[(ny - 4 + i * ny) * NV];
+        if (wall) { mc_wall_state(c3, p->gamma, lo); mc_wall_state(cn, p->gamma, hi); }
+        else { memcpy(lo, c3, sizeof(lo)); memcpy(hi, cn, sizeof(hi)); }
+        for (int g = 0; g < 3; ++g) {
+            memcpy(&U[(g + i * ny) * NV], lo, sizeof(lo));
+            memcpy(&U[(ny - 1 - g + i * ny) * NV], hi, sizeof(hi));
+        }
+    }
+}
+
 /* The x pass then the y pass, as every oneStepRK2 variant calls them
    (TP/TS resistiveMHD_2D.cu:171-172,193-194; the periodic-x / symmetric-y
    composition is lib_ResistiveMHD_2D_GPU_single/resistiveMHD_2D.cu:229-230,252-253). */
 void orc_boundary(const orc_params *p, double *U)
 {
     const int bcy = p->bc_y < 0 ? p->bc : p->bc_y;
-    if (p->bc == ORC_BC_SYMMETRIC) symmetric_x(p, U);
-    else periodic_x(p, U);
-    if (bcy == ORC_BC_SYMMETRIC) symmetric_y(p, U);
-    else periodic_y(p, U);
+    switch (p->bc) {
+    case ORC_BC_SYMMETRIC: symmetric_x(p, U); break;
+    case ORC_BC_ZERO_GRADIENT: mc_x_pass(p, U, 0); break;
+    case ORC_BC_FLARE: mc_x_pass(p, U, 1); break;
+    default: periodic_x(p, U); break;
+    }
+    switch (bcy) {
+    case ORC_BC_SYMMETRIC: symmetric_y(p, U); break;
+    case ORC_BC_ZERO_GRADIENT: mc_y_pass(p, U, 0); break;
+    case ORC_BC_WALL: mc_y_pass(p, U, 1); break;
+    default: periodic_y(p, U); break;
+    }
 }
 
 size_t orc_work_doubles(int nx, int ny)

@@ -13,7 +13,7 @@
 extern "C" {
 #endif
 
-enum { ORC_BC_PERIODIC = 0, ORC_BC_SYMMETRIC = 1 };
+enum { ORC_BC_PERIODIC = 0, ORC_BC_SYMMETRIC = 1, ORC_BC_ZERO_GRADIENT = 2, ORC_BC_WALL = 3, ORC_BC_FLARE = 4 };
 
 typedef struct {
     int nx, ny;               /* cells per direction, 3 ghost layers per side included */
@@ -23,7 +23,7 @@ typedef struct {
     double eps;               /* EPS regulariser */
     double eta;               /* scalar eta: resistive term when eta_table is NULL, and dt limit */
     const double *eta_table;  /* optional cell-centred eta, k = j + i*ny */
-    int bc;                   /* x boundary: ORC_BC_PERIODIC or ORC_BC_SYMMETRIC */
+    int bc;                   /* x boundary: ORC_BC_PERIODIC, _SYMMETRIC, _ZERO_GRADIENT or _FLARE */
     int bc_y;                 /* y boundary, or -1 for the same as bc */
     int ct_contact;           /* 0: the step's CT with the stage-1 EMF; 1: CT-Contact EMF (orc_step_contact) */
 } orc_params;

@@ -17,7 +17,7 @@ OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no sm_100 device", 4: "invalid solver state",
           5: "I/O error", 6: "kernel error"}
 
-BC = {"periodic": 0, "symmetric": 1}
+BC = {"periodic": 0, "symmetric": 1, "zero_gradient": 2, "wall": 3, "flare": 4}
 CT = {"stage1": 0, "contact": 1}
 PRECISION = {"fp64_exact": 0, "exact": 0, "fp64_fast": 1, "fast": 1, "fp32_bulk": 2, "bulk32": 2}
 

@@ -351,10 +351,15 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
     if (!(cfg->dx > 0) || !(cfg->dy > 0)) return fail(s, RMHD2D_ERR_INVALID, "dx and dy must be positive");
     if (!(cfg->gamma_mhd > 1.0)) return fail(s, RMHD2D_ERR_INVALID, "gamma_mhd must be > 1");
     if (!(cfg->eta >= 0.0)) return fail(s, RMHD2D_ERR_INVALID, "eta must be >= 0");
-    if (cfg->bc != RMHD2D_BC_PERIODIC && cfg->bc != RMHD2D_BC_SYMMETRIC)
-        return fail(s, RMHD2D_ERR_INVALID, "unknown boundary kind");
-    if (cfg->bc_y != -1 && cfg->bc_y != RMHD2D_BC_PERIODIC && cfg->bc_y != RMHD2D_BC_SYMMETRIC)
-        return fail(s, RMHD2D_ERR_INVALID, "unknown y boundary kind");
+    {
+        const int bx = cfg->bc, by = cfg->bc_y == -1 ? cfg->bc : cfg->bc_y;
+        if (bx != RMHD2D_BC_PERIODIC && bx != RMHD2D_BC_SYMMETRIC && bx != RMHD2D_BC_ZERO_GRADIENT &&
+            bx != RMHD2D_BC_FLARE)
+            return fail(s, RMHD2D_ERR_INVALID, "unknown x boundary kind (wall walls are y walls)");
+        if (by != RMHD2D_BC_PERIODIC && by != RMHD2D_BC_SYMMETRIC && by != RMHD2D_BC_ZERO_GRADIENT &&
+            by != RMHD2D_BC_WALL)
+            return fail(s, RMHD2D_ERR_INVALID, "unknown y boundary kind (flare walls are x walls; set bc_y)");
+    }
     if (cfg->precision != RMHD2D_FP64_EXACT && cfg->precision != RMHD2D_FP64_FAST &&
         cfg->precision != RMHD2D_FP32_BULK)
         return fail(s, RMHD2D_ERR_INVALID, "unknown precision");

@@ -29,8 +29,6 @@ __device__ __forceinline__ int wrap(int c, int n)
     return c;
 }
 
-// Source index of a ghost cell along one direction: periodic wrap or mirror.
-__device__ __forceinline__ int image(int c, int n, int bc) { return bc == BC_PERIODIC ? wrap(c, n) : mirror(c, n); }
 
 // bY seen by the x-wall integration at interior column c and row r: the
 // lower-wall face row (r = 2) holds the stage's constrained-transport value
@@ -62,40 +60,112 @@ __device__ double bX_xghost(const Grid &g, const double *bX, const double *bY, c
     return b - (bY_prewall(g, bY, row2, nx - 6, r) - bY_prewall(g, bY, row2, nx - 6, r - 1)) / dy * dx;    // nx-1
 }
 
-// bX after the x pass at column c (any) and interior row r: periodic x walls
-// copy it, symmetric ones integrate it.
-__device__ __forceinline__ double bX_afterx(const Grid &g, const double *bX, const double *bY, const double *row2,
-                                            int c, int r)
+// The multi-GPU library's wall states (ResistiveMHD_multiGPU_cuda/
+// ResistiveMHD2D_GPU/boundary.cu:63-84, 212-229): from cell c, density,
+// normal B and bZ kept, tangential bY 0, velocity 0 (the conducting wall)
+// or only v kept (the flare's line-tied wall), energy rebuilt from the
+// cell's pressure (computed with its face B).
+template <bool KEEP_V>
+__device__ __forceinline__ void mc_wall_state(const double *c, double gm, double *out)
 {
-    if (c >= 3 && c < g.nx - 3) return bX[at(g, c, r)];
-    if (g.bc_x == BC_PERIODIC) return bX[at(g, wrap(c, g.nx), r)];
-    return bX_xghost(g, bX, bY, row2, c, r);
+    const double rho = c[RHO];
+    const double u = c[MX] / rho, v = c[MY] / rho, w = c[MZ] / rho;
+    const double bX = c[BXF], bY = c[BYF], bZ = c[BZF], e = c[EN];
+    const double p = (gm - 1.0) * (e - 0.5 * rho * (u * u + v * v + w * w) - 0.5 * (bX * bX + bY * bY + bZ * bZ));
+    const double vk = KEEP_V ? v : 0.0;
+    out[RHO] = rho;
+    out[MX] = rho * 0.0;
+    out[MY] = KEEP_V ? rho * v : rho * 0.0;
+    out[MZ] = rho * 0.0;
+    out[BXF] = bX;
+    out[BYF] = 0.0;
+    out[BZF] = bZ;
+    out[EN] = p / (gm - 1.0) + 0.5 * rho * (0.0 * 0.0 + vk * vk + 0.0 * 0.0) + 0.5 * (bX * bX + 0.0 * 0.0 + bZ * bZ);
 }
 
-// y-wall ghost bY at column i, ghost row j
-// (TS boundary.cu:159-188 symmetricBoundaryY2ndBY_kernel).
-__device__ double bY_yghost(const Grid &g, const double *bX, const double *bY, const double *row2, int i, int j)
+__device__ __forceinline__ void load_cell(const Grid &g, const double *s, int i, int j, double *v)
+{
+#pragma unroll
+    for (int f = 0; f < NFIELD; ++f) v[f] = s[f * g.plane + at(g, i, j)];
+}
+
+// The cell (i, j) after the x pass (any column, an interior row j): the cell
+// itself in interior columns, else the x wall's rule -- periodic copy
+// (boundary.cu:4-57), mirror copy with the integrated bX (TS
+// boundary.cu:4-104), copy of the nearest interior column (zero gradient,
+// the multi-GPU library's boundary.cu:231-243), or the flare's line-tied
+// state at x = xmin and a copy at x = xmax (boundary.cu:196-245).
+// BX is the x wall kind, or -1 to read it from g (batches of mixed walls).
+template <int BX>
+__device__ void after_x_cell(const Grid &g, const double *s, const double *row2, int i, int j, double *v)
+{
+    if (i >= 3 && i < g.nx - 3) {
+        load_cell(g, s, i, j, v);
+        return;
+    }
+    switch (BX >= 0 ? BX : g.bc_x) {
+    case BC_PERIODIC:
+        load_cell(g, s, wrap(i, g.nx), j, v);
+        return;
+    case BC_SYMMETRIC:
+        load_cell(g, s, mirror(i, g.nx), j, v);
+        v[BXF] = bX_xghost(g, s + BXF * g.plane, s + BYF * g.plane, row2, i, j);
+        return;
+    case BC_FLARE:
+        if (i < 3) {
+            double c[NFIELD];
+            load_cell(g, s, 3, j, c);
+            mc_wall_state<true>(c, g.gamma, v);
+            return;
+        }
+        load_cell(g, s, g.nx - 4, j, v);
+        return;
+    default:   // BC_ZERO_GRADIENT
+        load_cell(g, s, i < 3 ? 3 : g.nx - 4, j, v);
+        return;
+    }
+}
+
+template <int BX>
+__device__ __forceinline__ double after_x_field(const Grid &g, const double *s, const double *row2, int f, int i,
+                                                int j)
+{
+    const int kx = BX >= 0 ? BX : g.bc_x;
+    if (i >= 3 && i < g.nx - 3) return s[f * g.plane + at(g, i, j)];
+    if (kx == BC_PERIODIC) return s[f * g.plane + at(g, wrap(i, g.nx), j)];
+    if (kx == BC_SYMMETRIC)
+        return f == BXF ? bX_xghost(g, s + BXF * g.plane, s + BYF * g.plane, row2, i, j)
+                        : s[f * g.plane + at(g, mirror(i, g.nx), j)];
+    double v[NFIELD];
+    after_x_cell<BX>(g, s, row2, i, j, v);
+    return v[f];
+}
+
+// y-wall ghost bY at column i, ghost row j of the mirror wall, from the x
+// pass's result (TS boundary.cu:159-188 symmetricBoundaryY2ndBY_kernel).
+template <int BX>
+__device__ double bY_yghost(const Grid &g, const double *s, const double *row2, int i, int j)
 {
     const double dx = g.dx, dy = g.dy;
     const int ny = g.ny;
-    const int mi = image(i, g.nx, g.bc_x);   // bY of ghost columns after the x pass
+    auto bx = [&](int c, int r) { return after_x_field<BX>(g, s, row2, BXF, c, r); };
     if (j < 3) {
-        double b = bY[at(g, mi, 3)];
+        double b = after_x_field<BX>(g, s, row2, BYF, i, 3);
         if (i == 0) return b;
-        const double s3 = (bX_afterx(g, bX, bY, row2, i, 3) - bX_afterx(g, bX, bY, row2, i - 1, 3)) / dx * dy;
+        const double s3 = (bx(i, 3) - bx(i - 1, 3)) / dx * dy;
         b = b + s3;                                   // row 2
         if (j == 2) return b;
-        b = b + (bX_afterx(g, bX, bY, row2, i, 3) - bX_afterx(g, bX, bY, row2, i - 1, 3)) / dx * dy;  // row 1
+        b = b + (bx(i, 3) - bx(i - 1, 3)) / dx * dy;  // row 1
         if (j == 1) return b;
-        return b + (bX_afterx(g, bX, bY, row2, i, 4) - bX_afterx(g, bX, bY, row2, i - 1, 4)) / dx * dy;  // row 0
+        return b + (bx(i, 4) - bx(i - 1, 4)) / dx * dy;  // row 0
     }
-    double b = bY[at(g, mi, ny - 4)];
+    double b = after_x_field<BX>(g, s, row2, BYF, i, ny - 4);
     if (i == 0) return b;
-    b = b - (bX_afterx(g, bX, bY, row2, i, ny - 4) - bX_afterx(g, bX, bY, row2, i - 1, ny - 4)) / dx * dy;  // ny-3
+    b = b - (bx(i, ny - 4) - bx(i - 1, ny - 4)) / dx * dy;  // ny-3
     if (j == ny - 3) return b;
-    b = b - (bX_afterx(g, bX, bY, row2, i, ny - 5) - bX_afterx(g, bX, bY, row2, i - 1, ny - 5)) / dx * dy;  // ny-2
+    b = b - (bx(i, ny - 5) - bx(i - 1, ny - 5)) / dx * dy;  // ny-2
     if (j == ny - 2) return b;
-    return b - (bX_afterx(g, bX, bY, row2, i, ny - 6) - bX_afterx(g, bX, bY, row2, i - 1, ny - 6)) / dx * dy;  // ny-1
+    return b - (bx(i, ny - 6) - bx(i - 1, ny - 6)) / dx * dy;  // ny-1
 }
 
 // Maps a linear ghost-cell index to (i, j): first the 6 ghost columns
@@ -116,11 +186,13 @@ __device__ __forceinline__ void ghost_cell(const Grid &g, long long t, int &i, i
     }
 }
 
-// Fills ghost cell number t of `s` from its interior (and, for symmetric x
+// Fills ghost cell number t of `s` from its interior (and, for mirror x
 // walls, the CT'd lower-wall bY row), with the exact results of the
-// reference's x pass followed by its y pass, each periodic
-// (boundary.cu:4-141) or symmetric (TS boundary.cu:4-206).  Returns the
+// reference's x pass followed by its y pass.  Every ghost's value reads only
+// interior rows of the x pass's result, which reads only interior columns,
+// so no ghost cell is read and the in-place fill is race free.  Returns the
 // cell's CFL rate bits and NaN-energy flag when `rate` is set.
+template <int BX, int BY>
 __device__ __forceinline__ void fill_ghost(const Grid &g, double *s, const double *row2, long long t, bool rate,
                                            unsigned long long &bits, int &nan_e, bool &cell0_nan)
 {
@@ -129,22 +201,28 @@ __device__ __forceinline__ void fill_ghost(const Grid &g, double *s, const doubl
     const long long P = g.plane;
     const long long k = at(g, i, j);
     double v[8];
-    // hydro fields: the image of the x pass, then of the y pass
-    const int mi = image(i, g.nx, g.bc_x), mj = image(j, g.ny, g.bc_y);
-    const long long src = at(g, mi, mj);
-    const int hydro[6] = {RHO, MX, MY, MZ, BZF, EN};
-#pragma unroll
-    for (int n = 0; n < 6; ++n) v[hydro[n]] = s[hydro[n] * P + src];
-    const double *bX = s + BXF * P, *bY = s + BYF * P;
-    // bX: x pass (copy or integration), then the y pass copies rows
-    v[BXF] = bX_afterx(g, bX, bY, row2, i, mj);
-    // bY: x pass copies columns, then the y pass copies or integrates rows
-    if ((j >= 3 && j < g.ny - 3) || g.bc_y == BC_PERIODIC)
-        v[BYF] = bY[at(g, mi, mj)];
-    else
-        v[BYF] = bY_yghost(g, bX, bY, row2, i, j);
-    // all reads of this thread precede its writes; a ghost cell is never
-    // read by the boundary fill, so the in-place update is race free.
+    if (j >= 3 && j < g.ny - 3) {
+        after_x_cell<BX>(g, s, row2, i, j, v);
+    } else {
+        switch (BY >= 0 ? BY : g.bc_y) {
+        case BC_PERIODIC:                       // boundary.cu:73-141
+            after_x_cell<BX>(g, s, row2, i, wrap(j, g.ny), v);
+            break;
+        case BC_SYMMETRIC:                      // TS boundary.cu:107-205
+            after_x_cell<BX>(g, s, row2, i, mirror(j, g.ny), v);
+            v[BYF] = bY_yghost<BX>(g, s, row2, i, j);
+            break;
+        case BC_WALL: {                         // boundary.cu:48-119
+            double c[NFIELD];
+            after_x_cell<BX>(g, s, row2, i, j < 3 ? 3 : g.ny - 4, c);
+            mc_wall_state<false>(c, g.gamma, v);
+            break;
+        }
+        default:                                // BC_ZERO_GRADIENT, boundary.cu:292-337
+            after_x_cell<BX>(g, s, row2, i, j < 3 ? 3 : g.ny - 4, v);
+            break;
+        }
+    }
 #pragma unroll
     for (int f = 0; f < 8; ++f) s[f * P + k] = v[f];
     if (rate) {
@@ -174,6 +252,7 @@ __device__ __forceinline__ void reduce_ghost_rates(Control *ctl, int slot, unsig
 // Every ghost cell of one run.  With `ctl` set it also folds the ghost
 // cells' CFL rate and NaN-energy test into the reductions of the stage-2
 // kernel (slot = the next step's parity).
+template <int BX, int BY>
 __global__ void boundary_kernel(Grid g, double *s, const double *row2, Control *ctl, int slot)
 {
     const long long nghost = 6LL * g.ny + 6LL * (g.nx - 6);
@@ -181,7 +260,7 @@ __global__ void boundary_kernel(Grid g, double *s, const double *row2, Control *
     unsigned long long bits = 0ull;
     int nan_e = 0;
     bool c0 = false;
-    if (t < nghost) fill_ghost(g, s, row2, t, ctl != nullptr, bits, nan_e, c0);
+    if (t < nghost) fill_ghost<BX, BY>(g, s, row2, t, ctl != nullptr, bits, nan_e, c0);
     if (ctl) reduce_ghost_rates(ctl, slot, bits, nan_e, c0);
 }
 
@@ -200,7 +279,7 @@ __global__ void boundary_batch_kernel(const BatchRun *runs, int which, int slot)
     int nan_e = 0;
     bool c0 = false;
     const bool rate = which == 1;
-    if (t < nghost) fill_ghost(g, which == 1 ? r.A : r.B, r.row2, t, rate, bits, nan_e, c0);
+    if (t < nghost) fill_ghost<-1, -1>(g, which == 1 ? r.A : r.B, r.row2, t, rate, bits, nan_e, c0);
     if (rate) reduce_ghost_rates(r.ctl, slot, bits, nan_e, c0);
 }
 
@@ -290,7 +369,23 @@ void launch_boundary(const Grid &g, double *s, const double *row2, Control *ctl,
     const long long nghost = 6LL * g.ny + 6LL * (g.nx - 6);
     const int threads = 256;
     const int blocks = (int)((nghost + threads - 1) / threads);
-    boundary_kernel<<<blocks, threads, 0, st>>>(g, s, row2, ctl, slot);
+    // one instantiation per (x, y) wall pair; the y kind is a template
+    // argument under each x kind
+    auto launch = [&](auto kernel) { kernel<<<blocks, threads, 0, st>>>(g, s, row2, ctl, slot); };
+#define RMHD_BY(BXK)                                                                                   \
+    switch (g.bc_y) {                                                                                  \
+    case BC_PERIODIC: launch(boundary_kernel<BXK, BC_PERIODIC>); break;                                \
+    case BC_SYMMETRIC: launch(boundary_kernel<BXK, BC_SYMMETRIC>); break;                              \
+    case BC_WALL: launch(boundary_kernel<BXK, BC_WALL>); break;                                        \
+    default: launch(boundary_kernel<BXK, BC_ZERO_GRADIENT>); break;                                    \
+    }
+    switch (g.bc_x) {
+    case BC_PERIODIC: RMHD_BY(BC_PERIODIC) break;
+    case BC_SYMMETRIC: RMHD_BY(BC_SYMMETRIC) break;
+    case BC_FLARE: RMHD_BY(BC_FLARE) break;
+    default: RMHD_BY(BC_ZERO_GRADIENT) break;
+    }
+#undef RMHD_BY
 }
 
 void launch_boundary_batch(const BatchRun *runs, int nruns, long long max_ghost, int which, int slot, cudaStream_t st)

@@ -11,7 +11,10 @@ namespace rmhd2d {
 // (lib_ResistiveMHD_2D_GPU_periodicXY/conservation_parameter_struct.hpp:5-27).
 enum Field { RHO = 0, MX = 1, MY = 2, MZ = 3, BXF = 4, BYF = 5, BZF = 6, EN = 7, NFIELD = 8 };
 
-enum Bc { BC_PERIODIC = 0, BC_SYMMETRIC = 1 };
+// Wall kinds: the single-GPU libraries' periodic and mirror (symmetric)
+// walls, and the multi-GPU library's zero-gradient copy, conducting wall (y)
+// and flare wall (x).
+enum Bc { BC_PERIODIC = 0, BC_SYMMETRIC = 1, BC_ZERO_GRADIENT = 2, BC_WALL = 3, BC_FLARE = 4 };
 
 // Geometry and physics constants passed by value to every kernel.
 struct Grid {
