@@ -421,8 +421,14 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
 
     const float iSLM = rcp_nr(SL - SM + EPS), iSRM = rcp_nr(SR - SM + EPS);
     const float rho1L = rdSL * iSLM, rho1R = rdSR * iSRM;
-    const float id1L = rcp_nr(rdSL * (SL - SM) - bx2 + EPS);
-    const float id1R = rcp_nr(rdSR * (SR - SM) - bx2 + EPS);
+    // D = rho (S - u)(S - SM) - bX^2 is a difference of two terms of order
+    // bX^2.  Single precision resolves it only to about 1e-7 bX^2, so below
+    // 1e-5 bX^2 the star state keeps v, w and B_t (the degenerate case of the
+    // HLLD solver, Miyoshi & Kusano 2005 sec. 4.4) instead of dividing by a
+    // rounding residue.
+    const float DL = rdSL * (SL - SM) - bx2 + EPS, DR = rdSR * (SR - SM) - bx2 + EPS;
+    const float id1L = fabsf(DL) > 1e-5f * bx2 ? rcp_nr(DL) : 0.f;
+    const float id1R = fabsf(DR) > 1e-5f * bx2 ? rcp_nr(DR) : 0.f;
     const float tL = bX * (SM - uL) * id1L, tR = bX * (SM - uR) * id1R;
     const float v1L = vL - bYL * tL, w1L = wL - bZL * tL;
     const float v1R = vR - bYR * tR, w1R = wR - bZR * tR;

@@ -281,3 +281,30 @@ def test_orszag_tang_past_the_degenerate_fast_speed(gpu, precision):
         assert sol.total_time == pytest.approx(t_want, rel=1e-6)
     rho = np.abs(got[3:-3, 3:-3, 0] - want[3:-3, 3:-3, 0]).sum() / np.abs(want[3:-3, 3:-3, 0]).sum()
     assert rho < (1e-4 if precision == "fp32_bulk" else 1e-9)
+
+
+@pytest.mark.gpu
+def test_fp32_bulk_harris_past_the_degenerate_star_denominator(gpu):
+    """On the 2048 x 1024 Harris sheet the HLLD star denominator
+    rho (S - u)(S - SM) - bX^2 of some x-faces falls below what single
+    precision resolves (bX ~ 1, |bY| ~ 4e-5 at about step 130); dividing by
+    its rounding residue crashed the FP32-bulk run.  The run must stay
+    finite and follow the FP64 run at the same time steps."""
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.harris_sheet(2048, 1024)
+    nsteps = 200
+    with Solver.from_setup(s, precision="fp64_fast") as ref:
+        dts = []
+        for _ in range(nsteps):
+            ref.step()
+            dts.append(ref.dt)
+        assert not ref.check_crashed()
+        want = ref.get_state()
+    with Solver.from_setup(s, precision="fp32_bulk") as sol:
+        sol.run(nsteps)
+        assert not sol.check_crashed()
+        got = sol.get_state()
+        assert sol.total_time == pytest.approx(sum(dts), rel=1e-6)
+    err = rel_l1(got[3:-3, 3:-3], want[3:-3, 3:-3])
+    assert np.all(err[[0, 4, 5, 7]] < BULK_REL_L1), err
