@@ -39,6 +39,13 @@ Extra blocks of the same JSON line (each can be switched off):
              steps) in one persistent batch in FP32-bulk, against the FP64
              path looped one run at a time; with N > 1 the runs are sharded
              over the ranks (no collective on the data path).
+
+--study harris|plasmoid replaces the benchmark with the long error study of
+FP32-bulk against FP64 at the same dts, beside an FP64 run that differs from
+the reference by round-off only: Harris 2048 x 1024 for 5000 steps against
+the drop-in, or the plasmoid-unstable sheet 8192 x 4096 (half-width 0.1, eta
+1e-5, beta 0.1) for 20000 steps against fp64_fast, with the relative L1 of
+rho, p, B and J_z and max |div B| at 5 evenly spaced snapshots.
 """
 from __future__ import annotations
 
@@ -391,6 +398,106 @@ def precision_block(args, setup, label, local_rank):
     return out
 
 
+STUDIES = {
+    # name: (setup factory, label, steps, snapshots, FP64 reference precision)
+    "harris": (lambda s: s.harris_sheet(2048, 1024), "harris_2048x1024", 5000, 5, "fp64_exact"),
+    "plasmoid": (lambda s: s.plasmoid_sheet(8192, 4096), "plasmoid_8192x4096", 20000, 5, "fp64_fast"),
+}
+
+
+def _max_div_b(state, dx, dy) -> float:
+    """max |div B| over the interior cells, from the face fields."""
+    import numpy as np
+
+    div = (state[3:-3, 3:-3, 4] - state[2:-4, 3:-3, 4]) / dx + (state[3:-3, 3:-3, 5] - state[3:-3, 2:-4, 5]) / dy
+    return float(np.abs(div).max())
+
+
+def precision_study(args, local_rank):
+    """FP32-bulk against an FP64 reference run over the full length of a
+    workload, at evenly spaced snapshots, beside a "floor" run that differs
+    from the reference by round-off only: on Harris the reference is the
+    drop-in (fp64_exact) and the floor fp64_fast; on the plasmoid sheet the
+    drop-in stops at a degenerate HLLD face (see `drop_in`), so the reference
+    is fp64_fast and the floor fp64_fast from a start whose momenta are
+    scaled by 1 + 1e-15.  The runs advance in lockstep: the reference takes
+    its CFL dts segment by segment and the others replay them
+    (rmhd2d_run_fixed_dt), so every snapshot compares the same times.  The
+    floor run's error is what the flow's instability makes of round-off;
+    FP32-bulk's error is read against it."""
+    import numpy as np
+
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    make, label, nsteps, nsnap, ref_prec = STUDIES[args.study]
+    if args.study_steps:
+        nsteps = args.study_steps
+    setup = make(setups)
+    seg = [nsteps * (q + 1) // nsnap - nsteps * q // nsnap for q in range(nsnap)]
+    floor_prec = "fp64_fast"
+    floor_start = setup.state
+    floor_desc = "fp64_fast"
+    if ref_prec != "fp64_exact":
+        floor_start = setup.state.copy()
+        floor_start[3:-3, 3:-3, 1:3] *= 1.0 + 1e-15
+        floor_desc = "fp64_fast from momenta scaled by 1 + 1e-15"
+    out = {"study": label, "steps": nsteps, "snapshots": [], "reference": f"{ref_prec} (its own CFL dts)",
+           "floor": floor_desc, "unit": "relative L1 over the interior at the same dts", "data": "synthetic"}
+    if ref_prec != "fp64_exact":
+        # how far the drop-in (the reference's arithmetic) gets on its own dts
+        with Solver.from_setup(setup, precision="fp64_exact", device=local_rank) as ex:
+            crashed_at = None
+            for q in range(nsteps):
+                ex.step()
+                if (q + 1) % 50 == 0 and ex.check_crashed():
+                    crashed_at = q + 1
+                    break
+            out["drop_in"] = {"precision": "fp64_exact", "first_crash_check_failed_at_step": crashed_at,
+                              "checked_every": 50}
+    sols = {"reference": Solver.from_setup(setup, precision=ref_prec, device=local_rank),
+            "floor": Solver.from_setup(setup, precision=floor_prec, device=local_rank, apply_boundary=False),
+            "fp32_bulk": Solver.from_setup(setup, precision="fp32_bulk", device=local_rank)}
+    sols["floor"].set_state(floor_start, apply_boundary=True)
+    try:
+        done, t_wall = 0, {p: 0.0 for p in sols}
+        for n in seg:
+            dts = np.empty(n)
+            t0 = time.perf_counter()
+            for q in range(n):
+                sols["reference"].step()
+                dts[q] = sols["reference"].dt
+            t_wall["reference"] += time.perf_counter() - t0
+            for p in ("floor", "fp32_bulk"):
+                t0 = time.perf_counter()
+                sols[p].run_fixed_dt(dts)
+                sols[p].check_crashed()   # synchronises
+                t_wall[p] += time.perf_counter() - t0
+            done += n
+            ref_state = sols["reference"].get_state()
+            ref = _diagnostics(ref_state, setup.dx, setup.dy, setup.gamma)
+            snap = {"step": done, "time": sols["reference"].total_time,
+                    "max_div_b": {"reference": _max_div_b(ref_state, setup.dx, setup.dy)},
+                    "crashed": {"reference": sols["reference"].check_crashed()}}
+            del ref_state
+            for p in ("floor", "fp32_bulk"):
+                st = sols[p].get_state()
+                d = _diagnostics(st, setup.dx, setup.dy, setup.gamma)
+                snap[p] = {k: _rel_l1(d[k], ref[k]) for k in d}
+                snap["max_div_b"][p] = _max_div_b(st, setup.dx, setup.dy)
+                snap["crashed"][p] = sols[p].check_crashed()
+                del st, d
+            out["snapshots"].append(snap)
+            print(json.dumps({"progress": snap}), file=sys.stderr, flush=True)
+        out["wall_s"] = t_wall
+    finally:
+        for s in sols.values():
+            s.close()
+    last = out["snapshots"][-1]
+    out["final_bulk_over_floor"] = {k: last["fp32_bulk"][k] / max(last["floor"][k], 1e-300)
+                                    for k in last["fp32_bulk"]}
+    return out
+
+
 def adjoint_block(args, local_rank, n=512, nsteps=2000, ndirs=32, h=1e-6):
     """Cost and finite-difference agreement of the discrete adjoint."""
     import numpy as np
@@ -623,6 +730,9 @@ def main() -> None:
     ap.add_argument("--no-contact", dest="contact_block", action="store_false")
     ap.add_argument("--no-ensemble", dest="ensemble_block", action="store_false")
     ap.add_argument("--quick", action="store_true", help="headline only (no extra blocks, baselines or e2e)")
+    ap.add_argument("--study", choices=sorted(STUDIES), default=None,
+                    help="instead of the benchmark: the long FP32-bulk / FP64 error study of one workload")
+    ap.add_argument("--study-steps", type=int, default=0, help="override the study's step count")
     args = ap.parse_args()
     if args.quick:
         args.precision_block = args.adjoint_block = args.ensemble_block = args.contact_block = False
@@ -636,6 +746,10 @@ def main() -> None:
 
     if args.impl == "reference":
         reference_arm(args, rank)
+        return
+    if args.study:
+        if rank == 0:
+            print(json.dumps(precision_study(args, local_rank)), flush=True)
         return
 
     import torch

@@ -128,7 +128,10 @@ int rmhd2d_destroy(rmhd2d_solver *s);
    afterwards, as the reference drivers do at the end of initializeU. */
 int rmhd2d_set_state(rmhd2d_solver *s, const double *host_state, int apply_boundary);
 
-/* Same as rmhd2d_set_state from device memory (any CUDA-visible pointer). */
+/* Same as rmhd2d_set_state from device memory (any CUDA-visible pointer).
+   The copy is enqueued on the solver's stream, which does not wait for the
+   legacy default stream or any other: the data must be complete when the
+   call is made (synchronise the stream that produced it first). */
 int rmhd2d_set_state_device(rmhd2d_solver *s, const double *device_state, int apply_boundary);
 
 /* Replaces ResistiveMHD2D::getU() (TP resistiveMHD_2D.cu:431-434): copies

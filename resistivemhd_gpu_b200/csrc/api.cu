@@ -412,15 +412,22 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
         cudaMalloc(&s->ctl, sizeof(Control)) != cudaSuccess ||
         cudaMallocHost(&s->ctl_host, sizeof(Control)) != cudaSuccess)
         return bail(RMHD2D_ERR_CUDA, "device allocation failed");
+    // Every clear goes on the solver's stream, which does not synchronise
+    // with the legacy default stream (cudaStreamNonBlocking): a plain
+    // cudaMemset there could still be running when set_state's copy lands
+    // and zero part of it.  The stream is drained before create returns.
     if (cfg->ct_scheme == RMHD2D_CT_CONTACT) {
         const size_t cbytes = (size_t)g.plane * (5 * NFIELD + 2) * sizeof(double);
-        if (cudaMalloc(&s->contact, cbytes) != cudaSuccess || cudaMemset(s->contact, 0, cbytes) != cudaSuccess)
+        if (cudaMalloc(&s->contact, cbytes) != cudaSuccess ||
+            cudaMemsetAsync(s->contact, 0, cbytes, s->stream) != cudaSuccess)
             return bail(RMHD2D_ERR_CUDA, "device allocation failed (CT-Contact workspace)");
     }
     // Zero the planes so padding columns hold finite values.
-    if (cudaMemset(s->A, 0, state_bytes) != cudaSuccess || cudaMemset(s->B, 0, state_bytes) != cudaSuccess ||
-        cudaMemset(s->row2, 0, (size_t)g.nx * sizeof(double)) != cudaSuccess ||
-        cudaMemset(s->ctl, 0, sizeof(Control)) != cudaSuccess)
+    if (cudaMemsetAsync(s->A, 0, state_bytes, s->stream) != cudaSuccess ||
+        cudaMemsetAsync(s->B, 0, state_bytes, s->stream) != cudaSuccess ||
+        cudaMemsetAsync(s->row2, 0, (size_t)g.nx * sizeof(double), s->stream) != cudaSuccess ||
+        cudaMemsetAsync(s->ctl, 0, sizeof(Control), s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->stream) != cudaSuccess)
         return bail(RMHD2D_ERR_CUDA, "device memset failed");
     for (int sh = 0; sh < NSHAPE; ++sh)
         if (!encode_state_map(&s->mapA[sh], g, s->A, stage_ui(1, sh), shape_uj(sh)) ||
@@ -890,15 +897,20 @@ int batch_build(rmhd2d_batch *b)
     b->d_maps = nullptr;
     BCK(cudaMalloc(&b->d_runs, sizeof(BatchRun) * n));
     BCK(cudaMalloc(&b->d_maps, sizeof(CUtensorMap) * maps.size()));
-    BCK(cudaMemcpy(b->d_runs, runs.data(), sizeof(BatchRun) * n, cudaMemcpyHostToDevice));
-    BCK(cudaMemcpy(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice));
+    // On the batch stream (not the legacy default stream, which the batch
+    // stream does not wait for), drained before the host tables go away.
+    BCK(cudaMemcpyAsync(b->d_runs, runs.data(), sizeof(BatchRun) * n, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice,
+                        b->stream));
     for (int st = 0; st < 2; ++st) {
         cudaFree(b->d_tiles[st]);
         b->d_tiles[st] = nullptr;
         b->ntiles[st] = (int)tiles[st].size();
         BCK(cudaMalloc(&b->d_tiles[st], sizeof(TileRef) * tiles[st].size()));
-        BCK(cudaMemcpy(b->d_tiles[st], tiles[st].data(), sizeof(TileRef) * tiles[st].size(), cudaMemcpyHostToDevice));
+        BCK(cudaMemcpyAsync(b->d_tiles[st], tiles[st].data(), sizeof(TileRef) * tiles[st].size(),
+                            cudaMemcpyHostToDevice, b->stream));
     }
+    BCK(cudaStreamSynchronize(b->stream));
     b->dirty = false;
     return RMHD2D_OK;
 }
