@@ -75,65 +75,137 @@ __device__ __forceinline__ void sweep_cell(const Grid &g, const double *U, int i
     }
 }
 
-// HLLD::calculateFluxF / G (hlld.cu:110-233) + the resistive hook
-// (main_plasmoid.cu:175-290) at interface (i, j), natural field order.
-template <int DIR>
-__device__ void interface_flux(const Grid &g, const double *U, const double *eta, int i, int j, double *out)
+// F and G of every interface: HLLD::calculateFluxF / G (hlld.cu:110-233)
+// of the cell-centred state plus the resistive hook
+// (main_plasmoid.cu:175-290).  The x sweep is defined for 1 <= i <= nx-4,
+// the y sweep for 1 <= j <= ny-3 (the ranges the reference's buffers hold
+// current values in), NaN elsewhere.  One CTA stages the primitives of
+// (CT_TI + 3) x (CT_TJ + 3) cells in shared memory once -- the x and y
+// sweeps' pressures sum their squares in different orders, so both are
+// kept -- and forms the x and y interfaces (i, j) of its CT_TI x CT_TJ
+// cells from there, in the reference's order of operations.
+constexpr int CT_TI = 16, CT_TJ = 32, CT_THREADS = 256;
+constexpr int CT_SI = CT_TI + 3, CT_SJ = CT_TJ + 3, CT_SC = CT_SI * CT_SJ;
+enum { S_RHO = 0, S_U, S_V, S_W, S_BXC, S_BYC, S_BZ, S_PX, S_PY, S_NF };
+
+__global__ void __launch_bounds__(CT_THREADS, 2) contact_flux_tiled_kernel(Grid g, const double *U, const double *eta,
+                                                                         double *F, double *G)
 {
-    double cell[5][8], q[4][8];
-#pragma unroll
-    for (int m = 0; m < 5; ++m) sweep_cell<DIR>(g, U, DIR == 0 ? i + m - 1 : i, DIR == 0 ? j : j + m - 1, cell[m]);
-#pragma unroll
-    for (int m = 0; m < 4; ++m) adj::basic_param(cell[m], cell[m + 1][4], g.gamma, q[m]);
-    double L[8], R[8], f[8];
-    adj::muscl_states(q[0], q[1], q[2], q[3], g.eps, L, R);
-    const Prim PL{L[0], L[1], L[2], L[3], L[4], L[5], L[6], L[7]};
-    const Prim PR{R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7]};
-    hlld_flux<true>(PL, PR, g.gamma, g.eps, f);
-    if (DIR == 0) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) out[c] = f[c];
-    } else {
-        // shuffleForFluxG_kernel: the y flux from the permuted one
-        out[0] = f[0]; out[1] = f[3]; out[2] = f[1]; out[3] = f[2];
-        out[4] = f[6]; out[5] = f[4]; out[6] = f[5]; out[7] = f[7];
-    }
-    if (i < 1 || i > g.nx - 3 || j < 1 || j > g.ny - 3) return;   // the hook's 0 < i < nx-2, 0 < j < ny-2
+    __shared__ double S[S_NF][CT_SC];
+    const int i0 = blockIdx.y * CT_TI, j0 = blockIdx.x * CT_TJ;
     const long long P = g.plane;
-    auto bz = [&](int ii, int jj) { return U[BZF * P + at(g, ii, jj)]; };
+    // staged cell (si, sj) is cell (i0 - 1 + si, j0 - 1 + sj)
+    for (int c = threadIdx.x; c < CT_SC; c += CT_THREADS) {
+        const int si = c / CT_SJ, sj = c - si * CT_SJ;
+        const int i = i0 - 1 + si, j = j0 - 1 + sj;
+        if (i < 0 || j < 0 || i >= g.nx || j >= g.ny) continue;   // read by no defined interface
+        double cx[8], cy[8], qx[8], qy[8];
+        sweep_cell<0>(g, U, i, j, cx);
+        sweep_cell<1>(g, U, i, j, cy);
+        adj::basic_param(cx, 0.0, g.gamma, qx);
+        adj::basic_param(cy, 0.0, g.gamma, qy);
+        S[S_RHO][c] = qx[adj::QR];
+        S[S_U][c] = qx[adj::QU];
+        S[S_V][c] = qx[adj::QV];
+        S[S_W][c] = qx[adj::QW];
+        S[S_BXC][c] = cx[4];
+        S[S_BYC][c] = cx[5];
+        S[S_BZ][c] = cx[6];
+        S[S_PX][c] = qx[adj::QP];
+        S[S_PY][c] = qy[adj::QP];
+    }
+    __syncthreads();
+
+    auto at_s = [](int si, int sj) { return si * CT_SJ + sj; };
     const double two_dx = 2.0 * g.dx, two_dy = 2.0 * g.dy;
-    if (DIR == 0) {
-        double jY, jZ, e;
-        jY = -(bz(i + 1, j) - bz(i - 1, j)) / two_dx;
-        jZ = (by_c(g, U, i + 1, j) - by_c(g, U, i - 1, j)) / two_dx - (bx_c(g, U, i, j + 1) - bx_c(g, U, i, j - 1)) / two_dy;
-        e = eta ? eta[at(g, i, j)] : g.eta;
-        const double etaJY = e * jY, etaJZ = e * jZ;
-        const double etaJYBZ = etaJY * bz(i, j), etaJZBY = etaJZ * by_c(g, U, i, j);
-        jY = -(bz(i + 2, j) - bz(i, j)) / two_dx;
-        jZ = (by_c(g, U, i + 2, j) - by_c(g, U, i, j)) / two_dx
-           - (bx_c(g, U, i + 1, j + 1) - bx_c(g, U, i + 1, j - 1)) / two_dy;
-        e = eta ? eta[at(g, i + 1, j)] : g.eta;
-        const double etaJYPlus1 = e * jY, etaJZPlus1 = e * jZ;
-        const double etaJYBZPlus1 = etaJYPlus1 * bz(i + 1, j), etaJZBYPlus1 = etaJZPlus1 * by_c(g, U, i + 1, j);
-        out[5] -= 0.5 * (etaJZ + etaJZPlus1);
-        out[6] += 0.5 * (etaJY + etaJYPlus1);
-        out[7] += 0.5 * (etaJYBZ + etaJYBZPlus1) - 0.5 * (etaJZBY + etaJZBYPlus1);
-    } else {
-        double jX, jZ, e;
-        jX = (bz(i, j + 1) - bz(i, j - 1)) / two_dy;
-        jZ = (by_c(g, U, i + 1, j) - by_c(g, U, i - 1, j)) / two_dx - (bx_c(g, U, i, j + 1) - bx_c(g, U, i, j - 1)) / two_dy;
-        e = eta ? eta[at(g, i, j)] : g.eta;
-        const double etaJX = e * jX, etaJZ = e * jZ;
-        const double etaJXBZ = etaJX * bz(i, j), etaJZBX = etaJZ * bx_c(g, U, i, j);
-        jX = (bz(i, j + 2) - bz(i, j)) / two_dy;
-        jZ = (by_c(g, U, i + 1, j + 1) - by_c(g, U, i - 1, j + 1)) / two_dx
-           - (bx_c(g, U, i, j + 2) - bx_c(g, U, i, j)) / two_dy;
-        e = eta ? eta[at(g, i, j + 1)] : g.eta;
-        const double etaJXPlus1 = e * jX, etaJZPlus1 = e * jZ;
-        const double etaJXBZPlus1 = etaJXPlus1 * bz(i, j + 1), etaJZBXPlus1 = etaJZPlus1 * bx_c(g, U, i, j + 1);
-        out[4] += 0.5 * (etaJZ + etaJZPlus1);
-        out[6] -= 0.5 * (etaJX + etaJXPlus1);
-        out[7] += 0.5 * (etaJZBX + etaJZBXPlus1) - 0.5 * (etaJXBZ + etaJXBZPlus1);
+    for (int t = threadIdx.x; t < 2 * CT_TI * CT_TJ; t += CT_THREADS) {
+        const int dir = t >= CT_TI * CT_TJ;
+        const int r = t - dir * CT_TI * CT_TJ;
+        const int li = r / CT_TJ, lj = r - li * CT_TJ;
+        const int i = i0 + li, j = j0 + lj;
+        if (i >= g.nx || j >= g.ny) continue;
+        const int si = li + 1, sj = lj + 1;
+        double out[8];
+        const bool ok = dir == 0 ? (i >= 1 && i <= g.nx - 4) : (j >= 1 && j <= g.ny - 3);
+        if (!ok) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) out[c] = qnan();
+        } else {
+            // sweep-order primitives of the four cells along the sweep
+            double q[4][8];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int c = dir == 0 ? at_s(si - 1 + m, sj) : at_s(si, sj - 1 + m);
+                if (dir == 0) {
+                    q[m][0] = S[S_RHO][c]; q[m][1] = S[S_U][c]; q[m][2] = S[S_V][c]; q[m][3] = S[S_W][c];
+                    q[m][5] = S[S_BYC][c]; q[m][6] = S[S_BZ][c]; q[m][7] = S[S_PX][c];
+                } else {
+                    q[m][0] = S[S_RHO][c]; q[m][1] = S[S_V][c]; q[m][2] = S[S_W][c]; q[m][3] = S[S_U][c];
+                    q[m][5] = S[S_BZ][c]; q[m][6] = S[S_BXC][c]; q[m][7] = S[S_PY][c];
+                }
+                q[m][4] = 0.0;
+            }
+            // basic_param's interface-normal B of the left cell and its neighbour
+            {
+                const int nb = dir == 0 ? S_BXC : S_BYC;
+                const int c1 = at_s(si, sj), c2 = dir == 0 ? at_s(si + 1, sj) : at_s(si, sj + 1);
+                q[1][4] = XMUL(0.5, XADD(S[nb][c1], S[nb][c2]));
+            }
+            double L[8], R[8], f[8];
+            adj::muscl_states(q[0], q[1], q[2], q[3], g.eps, L, R);
+            const Prim PL{L[0], L[1], L[2], L[3], L[4], L[5], L[6], L[7]};
+            const Prim PR{R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7]};
+            hlld_flux<true>(PL, PR, g.gamma, g.eps, f);
+            if (dir == 0) {
+#pragma unroll
+                for (int c = 0; c < 8; ++c) out[c] = f[c];
+            } else {
+                out[0] = f[0]; out[1] = f[3]; out[2] = f[1]; out[3] = f[2];
+                out[4] = f[6]; out[5] = f[4]; out[6] = f[5]; out[7] = f[7];
+            }
+            // the resistive hook (the reference's 0 < i < nx-2, 0 < j < ny-2)
+            if (i >= 1 && i <= g.nx - 3 && j >= 1 && j <= g.ny - 3) {
+                auto bz = [&](int a, int b) { return S[S_BZ][at_s(a, b)]; };
+                auto byc = [&](int a, int b) { return S[S_BYC][at_s(a, b)]; };
+                auto bxc = [&](int a, int b) { return S[S_BXC][at_s(a, b)]; };
+                if (dir == 0) {
+                    double jY, jZ, e;
+                    jY = -(bz(si + 1, sj) - bz(si - 1, sj)) / two_dx;
+                    jZ = (byc(si + 1, sj) - byc(si - 1, sj)) / two_dx - (bxc(si, sj + 1) - bxc(si, sj - 1)) / two_dy;
+                    e = eta ? eta[at(g, i, j)] : g.eta;
+                    const double etaJY = e * jY, etaJZ = e * jZ;
+                    const double etaJYBZ = etaJY * bz(si, sj), etaJZBY = etaJZ * byc(si, sj);
+                    jY = -(bz(si + 2, sj) - bz(si, sj)) / two_dx;
+                    jZ = (byc(si + 2, sj) - byc(si, sj)) / two_dx
+                       - (bxc(si + 1, sj + 1) - bxc(si + 1, sj - 1)) / two_dy;
+                    e = eta ? eta[at(g, i + 1, j)] : g.eta;
+                    const double etaJYPlus1 = e * jY, etaJZPlus1 = e * jZ;
+                    const double etaJYBZPlus1 = etaJYPlus1 * bz(si + 1, sj), etaJZBYPlus1 = etaJZPlus1 * byc(si + 1, sj);
+                    out[5] -= 0.5 * (etaJZ + etaJZPlus1);
+                    out[6] += 0.5 * (etaJY + etaJYPlus1);
+                    out[7] += 0.5 * (etaJYBZ + etaJYBZPlus1) - 0.5 * (etaJZBY + etaJZBYPlus1);
+                } else {
+                    double jX, jZ, e;
+                    jX = (bz(si, sj + 1) - bz(si, sj - 1)) / two_dy;
+                    jZ = (byc(si + 1, sj) - byc(si - 1, sj)) / two_dx - (bxc(si, sj + 1) - bxc(si, sj - 1)) / two_dy;
+                    e = eta ? eta[at(g, i, j)] : g.eta;
+                    const double etaJX = e * jX, etaJZ = e * jZ;
+                    const double etaJXBZ = etaJX * bz(si, sj), etaJZBX = etaJZ * bxc(si, sj);
+                    jX = (bz(si, sj + 2) - bz(si, sj)) / two_dy;
+                    jZ = (byc(si + 1, sj + 1) - byc(si - 1, sj + 1)) / two_dx
+                       - (bxc(si, sj + 2) - bxc(si, sj)) / two_dy;
+                    e = eta ? eta[at(g, i, j + 1)] : g.eta;
+                    const double etaJXPlus1 = e * jX, etaJZPlus1 = e * jZ;
+                    const double etaJXBZPlus1 = etaJXPlus1 * bz(si, sj + 1), etaJZBXPlus1 = etaJZPlus1 * bxc(si, sj + 1);
+                    out[4] += 0.5 * (etaJZ + etaJZPlus1);
+                    out[6] -= 0.5 * (etaJX + etaJXPlus1);
+                    out[7] += 0.5 * (etaJZBX + etaJZBXPlus1) - 0.5 * (etaJXBZ + etaJXBZPlus1);
+                }
+            }
+        }
+        double *o = (dir == 0 ? F : G) + at(g, i, j);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) o[c * P] = out[c];
     }
 }
 
@@ -148,30 +220,6 @@ __global__ void contact_begin_kernel(Grid g, Control *ctl, int parity)
     ctl->amax[parity ^ 1] = 0ull;
     ctl->first_nan[parity ^ 1] = 0;
     ctl->crashed = 0;
-}
-
-// F (grid.y = 0) or G (grid.y = 1) of every interface: the x sweep is
-// defined for 1 <= i <= nx-4, the y sweep for 1 <= j <= ny-3 (the ranges the
-// reference's buffers hold current values in), NaN elsewhere.
-__global__ void __launch_bounds__(128) contact_flux_kernel(Grid g, const double *U, const double *eta, double *F,
-                                                           double *G)
-{
-    const int dir = blockIdx.y;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)g.nx * g.ny) return;
-    const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
-    double f[8];
-    const bool ok = dir == 0 ? (i >= 1 && i <= g.nx - 4) : (j >= 1 && j <= g.ny - 3);
-    if (ok) {
-        if (dir == 0) interface_flux<0>(g, U, eta, i, j, f);
-        else interface_flux<1>(g, U, eta, i, j, f);
-    } else {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) f[c] = qnan();
-    }
-    double *out = (dir == 0 ? F : G) + at(g, i, j);
-#pragma unroll
-    for (int c = 0; c < 8; ++c) out[c * g.plane] = f[c];
 }
 
 // ct.cu:45-61: reference EMF u bY - v bX - eta jZ of cell (i, j) for
@@ -342,19 +390,20 @@ void enqueue_contact_step(const ContactStep &c, cudaStream_t st)
 {
     const Grid &g = c.g;
     const long long n = (long long)g.nx * g.ny;
-    const int b128 = blocks_for(n, 128), b256 = blocks_for(n, 256);
+    const int b256 = blocks_for(n, 256);
+    const dim3 flux_grid((g.ny + CT_TJ - 1) / CT_TJ, (g.nx + CT_TI - 1) / CT_TI);
     auto boundary = [&](double *state) {
         if (g.bc_x == BC_SYMMETRIC) launch_snapshot_row2(g, state, c.row2, st);
         launch_boundary(g, state, c.row2, nullptr, 0, st);
     };
     contact_begin_kernel<<<1, 32, 0, st>>>(g, c.ctl, c.parity);
     // stage 1
-    contact_flux_kernel<<<dim3(b128, 2), 128, 0, st>>>(g, c.A, c.eta, c.F1, c.G1);
+    contact_flux_tiled_kernel<<<flux_grid, CT_THREADS, 0, st>>>(g, c.A, c.eta, c.F1, c.G1);
     contact_ref_kernel<true><<<b256, 256, 0, st>>>(g, c.A, c.eta, c.R1);
     contact_update_kernel<1><<<b256, 256, 0, st>>>(g, c.A, nullptr, c.F1, c.G1, c.ctl, c.B);
     boundary(c.B);
     // stage 2
-    contact_flux_kernel<<<dim3(b128, 2), 128, 0, st>>>(g, c.B, c.eta, c.F2, c.G2);
+    contact_flux_tiled_kernel<<<flux_grid, CT_THREADS, 0, st>>>(g, c.B, c.eta, c.F2, c.G2);
     contact_update_kernel<2><<<b256, 256, 0, st>>>(g, c.A, c.B, c.F2, c.G2, c.ctl, c.C);
     boundary(c.C);
     contact_ref_kernel<false><<<b256, 256, 0, st>>>(g, c.C, c.eta, c.R2);
