@@ -27,7 +27,9 @@ def load_golden(name: str):
     return s, z["initial"], z["final"], z["dts"], float(z["total_time"])
 
 
-GOLDEN_CASES = sorted(p.stem for p in GOLDEN.glob("*.npz"))
+# runs of the reference's own build (make_golden.py); other fixtures in the
+# folder (e.g. plasmoid_degenerate_face.npz) carry no "params" and have their own tests
+GOLDEN_CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if "params" in np.load(p).files)
 
 
 @pytest.fixture(scope="session")
