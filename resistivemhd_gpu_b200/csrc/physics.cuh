@@ -35,12 +35,17 @@ template <typename T> __device__ __forceinline__ T sgn(T x) { return x > T(0) ? 
 // 1.0 * max(min(|x|, 1.0 * y), EPS), for x < 0 the negation of
 // max(min(|x|, -y), EPS), for x == 0 (or NaN) 0.0 * max(min(|x|, 0.0 * y), EPS);
 // multiplying by +-1 is exact, so this is bit-identical for every input.
+//
+// Evaluated without branches: m = max(min(|x|, x < 0 ? -y : y), EPS), then
+// m, -m or 0 * m by the sign of x.  For x == 0 the reference's inner min
+// sees 0 * y where this sees y; min(0, y) and min(0, 0 * y) differ only for
+// y < 0 (y versus -0 or 0), and max(., EPS) turns both into EPS, so 0 * m is
+// +0 in both; a NaN x or y reaches m the same way in both forms.
 template <typename T> __device__ __forceinline__ T minmod(T x, T y, T eps)
 {
     const T ax = fabs(x);
-    if (x > T(0)) return tmax(tmin(ax, y), eps);
-    if (x < T(0)) return -tmax(tmin(ax, -y), eps);
-    return T(0) * tmax(tmin(ax, T(0) * y), eps);
+    const T m = tmax(tmin(ax, x < T(0) ? -y : y), eps);
+    return x > T(0) ? m : (x < T(0) ? -m : T(0) * m);
 }
 
 // Single-precision reciprocal and square roots of the FP32-bulk variant

@@ -44,6 +44,15 @@ struct StageArgs {
 };
 
 // One set of launchers per variant (stage_exact.cu, stage_fast.cu, stage_bulk32.cu).
+// Sweep of the stage kernel's flux phase (true: x sweep), as a compile-time
+// constant (SweepC) or a run-time value (SweepRT).
+template <bool F> struct SweepC {
+    static constexpr bool value = F;
+};
+struct SweepRT {
+    bool value;
+};
+
 namespace exact {
 void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream);

@@ -307,8 +307,14 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
 
     // ---- HLLD fluxes (hlld.cu:110-233, muscl.cu:6-126, flux_solver.cu:10-33)
     // with the resistive terms ----
-    for (int it = tid; it < T::NF + T::NG; it += STAGE_THREADS) {
-        const bool isF = it < T::NF;
+    // One interface per call.  Stage 2 of the contracted variants passes the
+    // sweep as a compile-time tag (a copy of the body per sweep, with
+    // constant plane strides); stage 1, whose larger tile spills with two
+    // copies, and the exact variant, which measured slower with them, pass
+    // it at run time.  Both sweeps share one index space, so the threads
+    // stay balanced.
+    auto flux_at = [&](const int it, const auto sweep) {
+        const bool isF = sweep.value;
         int a0, a1;   // (fi, fj) or (gi, gj)
         int ci, cj;   // the cell left of / below the interface, relative to (i0, j0)
         if (isF) {
@@ -444,6 +450,14 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
             oo[O_EN * SG] = fov[2] + (h * (eZ0 * x0 + eZ1 * x1) - h * (eX0 * z0 + eX1 * z1));
             if (STAGE == 1) oo[O_EMF * SG] = fov[1] + h * (eZ0 + eZ1);
         }
+    };
+    for (int it = tid; it < T::NF + T::NG; it += STAGE_THREADS) {
+        if (STAGE == 1 || !RMHD_FAST_MATH)
+            flux_at(it, SweepRT{it < T::NF});
+        else if (it < T::NF)
+            flux_at(it, SweepC<true>{});
+        else
+            flux_at(it, SweepC<false>{});
     }
     // Stage 2 reads U^n only in the update: issue those loads now, so their
     // latency overlaps the barrier wait of the CTA's slower warps.

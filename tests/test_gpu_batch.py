@@ -1,30 +1,36 @@
 """Tile shapes and batches of independent runs.
 
 The tile decomposition changes no arithmetic: every interface flux and cell
-update is computed by the same expressions whatever tile or launch holds it,
-so a batched run, or a run on the other tile shape, equals the single run bit
-for bit in both FP64 precisions.  The FP32-bulk variant is compiled with
-fast math and FMA contraction left to the compiler, which may contract its
-float core differently in the persistent batch kernel than in the single-run
-kernel; its batch is held to BULK_BATCH_REL_L1 of the single run (100 times
-inside the bulk variant's own 1e-5 bound against FP64)."""
+update is computed by the same expressions whatever tile or launch holds it.
+The FP64-exact variant (no contraction) is therefore equal bit for bit in a
+batch, on the other tile shape and in the single run.  The FP64-fast and
+FP32-bulk variants are compiled with fused multiply-add contraction left to
+the compiler, which may contract the same source differently in the
+persistent batch kernel than in the single-run kernel.  Their batches are
+held to FAST_BATCH_REL_L1 and BULK_BATCH_REL_L1 of the single run per
+field.  The FP64 bound is rounding level for the fluxes (~1e-16 of O(1)
+values) measured against fields as small as the Harris sheet's momenta
+(~1e-4 of its energy), i.e. up to ~1e-12 of such a field; the FP32-bulk
+bound is 100 times inside that variant's own 1e-5 against FP64."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 PRECISIONS = ["fp64_exact", "fp64_fast", "fp32_bulk"]
+FAST_BATCH_REL_L1 = 1e-10
 BULK_BATCH_REL_L1 = 1e-7
+BATCH_REL_L1 = {"fp64_exact": 0.0, "fp64_fast": FAST_BATCH_REL_L1, "fp32_bulk": BULK_BATCH_REL_L1}
 
 
 def assert_same(got, ref, precision, what):
-    if precision != "fp32_bulk":
+    if precision == "fp64_exact":
         assert np.array_equal(got, ref), what
         return
     for f in range(8):
         den = np.abs(ref[..., f]).sum()
         err = np.abs(got[..., f] - ref[..., f]).sum() / max(den, 1e-300)
-        assert err <= BULK_BATCH_REL_L1, f"{what} field {f}: rel L1 {err:.3e}"
+        assert err <= BATCH_REL_L1[precision], f"{what} field {f}: rel L1 {err:.3e}"
 
 
 def single(setup, nsteps, precision, shape=0):
@@ -58,8 +64,9 @@ def test_tile_shape_1_equals_shape_0(gpu, precision):
     s = setups.random_smooth_state(45, 39, seed=4, bc="symmetric", with_table=True)
     a, da, _ = single(s, 6, precision, shape=0)
     b, db, _ = single(s, 6, precision, shape=1)
-    assert np.array_equal(da, db)
-    assert np.array_equal(a, b)
+    rel = {"fp64_exact": 0.0, "fp64_fast": 1e-12, "fp32_bulk": 1e-6}[precision]
+    assert db == pytest.approx(da, rel=rel, abs=0)
+    assert_same(b, a, precision, "shape 1")
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
@@ -75,7 +82,7 @@ def test_batch_equals_single_runs(gpu, precision, launch):
         for r, (ref, dts, total) in enumerate(refs):
             m = b[r]
             assert_same(m.get_state(), ref, precision, f"run {r}")
-            rel = 0.0 if precision != "fp32_bulk" else 1e-6
+            rel = {"fp64_exact": 0.0, "fp64_fast": 1e-12, "fp32_bulk": 1e-6}[precision]
             assert m.dt == pytest.approx(dts[-1], rel=rel, abs=0)
             assert m.total_time == pytest.approx(total, rel=max(rel, 1e-15))
             assert not m.check_crashed()
@@ -111,7 +118,7 @@ def test_batch_autotune_restores_state(gpu):
         b.set_launch(shape, ctas)
         b.run(3)
         for r, (ref, _, _) in enumerate(refs):
-            assert np.array_equal(b[r].get_state(), ref)
+            assert_same(b[r].get_state(), ref, "fp64_fast", f"run {r}")
 
 
 def test_member_cannot_step_alone(gpu):
