@@ -128,11 +128,13 @@ __device__ __forceinline__ void add_weighted_flux(double rho, double u, double v
 // (calculateHLLDParameterFunctor), hlld.cu:469-549 (setFluxFunctor) and
 // hlld.cu:35-107 (CalculateFluxFunctor).
 //
-// ALL_CANDIDATES = true forms all six candidate fluxes and sums them with the
-// reference's 0/1 indicator weights (bit-identical to the reference for every
-// input, including non-finite ones).  ALL_CANDIDATES = false forms only the
-// candidates whose indicator is 1 and adds them in the reference's order,
-// which gives the same bits whenever all six candidates are finite.
+// ALL_CANDIDATES = true gives the bits of the reference's sum of all six
+// candidate fluxes with 0/1 indicator weights for every input, including
+// non-finite ones: it forms that sum unless exactly one candidate is selected
+// and all candidate values are bounded, where the selected flux alone has the
+// same bits.  ALL_CANDIDATES = false forms only the candidates whose
+// indicator is 1 and adds them in the reference's order, which gives the same
+// bits whenever all six candidates are finite.
 template <bool ALL_CANDIDATES>
 __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double gm, double EPS,
                                           double f[8])
@@ -224,6 +226,36 @@ __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double g
 #pragma unroll
     for (int n = 0; n < 8; ++n) f[n] = 0.0;
     if (ALL_CANDIDATES) {
+        // The weighted sum adds F * 0 = +-0 for every unselected candidate
+        // whose flux is finite, which leaves the selected candidate's flux
+        // bit for bit.  A flux component is a product of at most three of
+        // the candidate's values plus a few such products, so it is finite
+        // whenever every value is below 1e75 in magnitude; the sum of
+        // magnitudes below is NaN or infinite, and fails the test, as soon
+        // as one value is.  Then, with exactly one region selected, only
+        // that candidate is formed; otherwise all six are.
+        const int nsel = (int)bOL + (int)bML + (int)bIL + (int)bOR + (int)bMR + (int)bIR;
+        const double mag = fabs(rhoL) + fabs(uL) + fabs(vL) + fabs(wL) + fabs(bXL) + fabs(bYL) + fabs(bZL)
+                         + fabs(eL) + fabs(pTL) + fabs(rhoR) + fabs(uR) + fabs(vR) + fabs(wR) + fabs(bXR)
+                         + fabs(bYR) + fabs(bZR) + fabs(eR) + fabs(pTR) + fabs(rho1L) + fabs(rho1R) + fabs(SM)
+                         + fabs(pT1) + fabs(v1L) + fabs(w1L) + fabs(bY1L) + fabs(bZ1L) + fabs(e1L) + fabs(v1R)
+                         + fabs(w1R) + fabs(bY1R) + fabs(bZ1R) + fabs(e1R) + fabs(v2) + fabs(w2) + fabs(bY2)
+                         + fabs(bZ2) + fabs(e2L) + fabs(e2R);
+        if (nsel == 1 && mag < 1e75) {
+            const bool lft = bOL | bML | bIL;
+            const bool outer = bOL | bOR, inner = bIL | bIR;
+            const double rho = bOL ? rhoL : (bOR ? rhoR : (lft ? rho1L : rho1R));
+            const double u = bOL ? uL : (bOR ? uR : SM);
+            const double v = outer ? (bOL ? vL : vR) : (inner ? v2 : (bML ? v1L : v1R));
+            const double w = outer ? (bOL ? wL : wR) : (inner ? w2 : (bML ? w1L : w1R));
+            const double bx = lft ? bXL : bXR;
+            const double by = outer ? (bOL ? bYL : bYR) : (inner ? bY2 : (bML ? bY1L : bY1R));
+            const double bz = outer ? (bOL ? bZL : bZR) : (inner ? bZ2 : (bML ? bZ1L : bZ1R));
+            const double e = bOL ? eL : (bOR ? eR : (bML ? e1L : (bIL ? e2L : (bMR ? e1R : e2R))));
+            const double pT = bOL ? pTL : (bOR ? pTR : pT1);
+            add_one_flux(rho, u, v, w, bx, by, bz, e, pT, f);
+            return;
+        }
         // rho2L = rho1L, rho2R = rho1R, pT2 = pT1 (hlld.cu:360-378).
         add_weighted_flux(rhoL, uL, vL, wL, bXL, bYL, bZL, eL, pTL, (double)bOL, f);
         add_weighted_flux(rho1L, u1L, v1L, w1L, bXL, bY1L, bZ1L, e1L, pT1, (double)bML, f);
