@@ -57,7 +57,7 @@ struct rmhd2d_solver {
     long long steps = 0;
     cudaGraphExec_t graph2[2] = {nullptr, nullptr};
     AdjointWork *adj = nullptr;          // recorded trajectory and workspace of the discrete adjoint
-    double *contact = nullptr;           // CT-Contact workspace: C, F1, G1, F2, G2 (8 planes each), R1, R2
+    double *contact = nullptr;           // CT-Contact workspace: C, F1, G1, F2, G2 (8 planes each), R1, R2, E
     std::string err;
 };
 
@@ -216,6 +216,7 @@ void enqueue_step(rmhd2d_solver *s, int parity)
         c.G2 = c.F2 + NFIELD * P;
         c.R1 = c.G2 + NFIELD * P;
         c.R2 = c.R1 + P;
+        c.E = c.R2 + P;
         c.eta = s->eta;
         c.row2 = s->row2;
         c.ctl = s->ctl;
@@ -417,7 +418,7 @@ int rmhd2d_create(const rmhd2d_config *cfg, rmhd2d_solver **out)
     // cudaMemset there could still be running when set_state's copy lands
     // and zero part of it.  The stream is drained before create returns.
     if (cfg->ct_scheme == RMHD2D_CT_CONTACT) {
-        const size_t cbytes = (size_t)g.plane * (5 * NFIELD + 2) * sizeof(double);
+        const size_t cbytes = (size_t)g.plane * (5 * NFIELD + 3) * sizeof(double);
         if (cudaMalloc(&s->contact, cbytes) != cudaSuccess ||
             cudaMemsetAsync(s->contact, 0, cbytes, s->stream) != cudaSuccess)
             return bail(RMHD2D_ERR_CUDA, "device allocation failed (CT-Contact workspace)");

@@ -16,8 +16,8 @@
 //   update 2     C = (U^n + U* - dt div(F, G)) / 2 (both with smoothed face B)
 //   boundary     C
 //   ref (now)    per-cell reference EMF of C
-//   CT           A = C with face B = U^n's faces - dt curl(Ez), Ez the mean of
-//                the two stages' contact EMFs
+//   corners      Ez of every corner, the mean of the two stages' contact EMFs
+//   CT           A = C with face B = U^n's faces - dt curl(Ez)
 //   boundary     A, then the CFL rate and NaN test of every cell
 // Flux entries whose stencil leaves the grid, and the EMF inputs outside
 // 0 < i < nx-1, 0 < j < ny-1, are NaN, as the oracle leaves them: they reach
@@ -360,9 +360,18 @@ __device__ __forceinline__ double corner_ez(const Grid &g, const StageEmf &o, co
     return 0.5 * (contact_corner(g, o, i, j) + contact_corner(g, n, i, j));
 }
 
+// Every corner EMF once (corner_ez), NaN where it is undefined.
+__global__ void contact_corner_kernel(Grid g, StageEmf o, StageEmf n, double *E)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)g.nx * g.ny) return;
+    const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
+    E[at(g, i, j)] = corner_ez(g, o, n, i, j);
+}
+
 // ct.cu:200-218 CT_kernel on the step input's faces (A), the rest of the
-// state from the stage-2 result C.
-__global__ void contact_ct_kernel(Grid g, StageEmf o, StageEmf n, const double *C, const Control *ctl, double *A)
+// state from the stage-2 result C; E holds the corner EMFs.
+__global__ void contact_ct_kernel(Grid g, const double *E, const double *C, const Control *ctl, double *A)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)g.nx * g.ny) return;
@@ -373,9 +382,9 @@ __global__ void contact_ct_kernel(Grid g, StageEmf o, StageEmf n, const double *
         if (c != BXF && c != BYF) A[c * P + k] = C[c * P + k];
     if (i > 0 && j > 0) {
         const double dt = ctl->dt;
-        const double ez = corner_ez(g, o, n, i, j);
-        A[BXF * P + k] = A[BXF * P + k] - dt / g.dy * (ez - corner_ez(g, o, n, i, j - 1));
-        A[BYF * P + k] = A[BYF * P + k] + dt / g.dx * (ez - corner_ez(g, o, n, i - 1, j));
+        const double ez = E[k];
+        A[BXF * P + k] = A[BXF * P + k] - dt / g.dy * (ez - E[at(g, i, j - 1)]);
+        A[BYF * P + k] = A[BYF * P + k] + dt / g.dx * (ez - E[at(g, i - 1, j)]);
     } else {
         A[BXF * P + k] = C[BXF * P + k];
         A[BYF * P + k] = C[BYF * P + k];
@@ -409,8 +418,8 @@ void enqueue_contact_step(const ContactStep &c, cudaStream_t st)
     contact_ref_kernel<false><<<b256, 256, 0, st>>>(g, c.C, c.eta, c.R2);
     // CT with the two stages' mean contact EMF, then the boundary and the
     // next step's CFL rate and crash flag
-    contact_ct_kernel<<<b256, 256, 0, st>>>(g, StageEmf{c.F1, c.G1, c.R1}, StageEmf{c.F2, c.G2, c.R2}, c.C, c.ctl,
-                                             c.A);
+    contact_corner_kernel<<<b256, 256, 0, st>>>(g, StageEmf{c.F1, c.G1, c.R1}, StageEmf{c.F2, c.G2, c.R2}, c.E);
+    contact_ct_kernel<<<b256, 256, 0, st>>>(g, c.E, c.C, c.ctl, c.A);
     boundary(c.A);
     launch_rate(g, c.A, c.ctl, c.parity ^ 1, 1, st);
 }

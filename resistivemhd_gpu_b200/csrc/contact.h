@@ -15,6 +15,7 @@ struct ContactStep {
     double *F1, *G1;      // stage-1 fluxes (8 planes each)
     double *F2, *G2;      // stage-2 fluxes (8 planes each)
     double *R1, *R2;      // per-cell reference EMFs of the two stages (1 plane each)
+    double *E;            // corner EMFs, the mean of the two stages' (1 plane)
     const double *eta;    // eta plane or nullptr
     double *row2;         // the symmetric-wall boundary's row buffer
     Control *ctl;
