@@ -191,35 +191,53 @@ __global__ void __launch_bounds__(256) adj_center_kernel(AdjStageArgs a)
     }
 }
 
-// Transpose of periodicBoundaryY2nd (boundary.cu:73-141): the y pass ran
-// last, so it is undone first.
-__global__ void periodic_y_transpose(Grid g, double *Ub)
+// Transpose of the periodic boundary (periodicBoundaryX2nd then
+// periodicBoundaryY2nd, boundary.cu:4-141).  After both passes every ghost
+// cell holds the interior cell (wrap(i), wrap(j)), so its adjoint moves onto
+// that cell and the ghost's becomes 0.  One thread per interior cell of the
+// 3-wide bands along the walls and per field gathers its images -- the
+// y-wall image Jg, the x-wall image Ig and the corner (Ig, Jg) -- and zeroes
+// them, summing in the order the two passes' transposes (y first, then x)
+// would: (U(I,J) + U(I,Jg)) + (U(Ig,J) + U(Ig,Jg)).  Each ghost has one
+// image, so no two threads touch the same entry.
+__global__ void periodic_transpose_kernel(Grid g, double *Ub)
 {
+    const long long nrow = 6LL * (g.nx - 6);    // rows 3..5 and ny-6..ny-4, interior columns
+    const long long ncol = 6LL * (g.ny - 12);   // columns 3..5 and nx-6..nx-4, rows 6..ny-7
+    const long long per_field = nrow + ncol;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)g.nx * NFIELD) return;
-    const int i = (int)(t / NFIELD), f = (int)(t - (long long)i * NFIELD);
-    double *row = Ub + f * g.plane + (long long)i * g.pitch;
-    for (int q = 0; q < 3; ++q) {
-        row[g.ny - 6 + q] += row[q];
-        row[q] = 0.0;
-        row[3 + q] += row[g.ny - 3 + q];
-        row[g.ny - 3 + q] = 0.0;
+    if (t >= per_field * NFIELD) return;
+    const int f = (int)(t / per_field);
+    long long u = t - (long long)f * per_field;
+    int I, J;
+    if (u < nrow) {
+        const int r = (int)(u / (g.nx - 6));
+        I = 3 + (int)(u - (long long)r * (g.nx - 6));
+        J = r < 3 ? 3 + r : g.ny - 9 + r;
+    } else {
+        u -= nrow;
+        const int c = (int)(u / (g.ny - 12));
+        J = 6 + (int)(u - (long long)c * (g.ny - 12));
+        I = c < 3 ? 3 + c : g.nx - 9 + c;
     }
-}
-
-// Transpose of periodicBoundaryX2nd (boundary.cu:4-57).
-__global__ void periodic_x_transpose(Grid g, double *Ub)
-{
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)g.ny * NFIELD) return;
-    const int j = (int)(t / NFIELD), f = (int)(t - (long long)j * NFIELD);
-    double *col = Ub + f * g.plane + j;
-    for (int q = 0; q < 3; ++q) {
-        col[(long long)(g.nx - 6 + q) * g.pitch] += col[(long long)q * g.pitch];
-        col[(long long)q * g.pitch] = 0.0;
-        col[(long long)(3 + q) * g.pitch] += col[(long long)(g.nx - 3 + q) * g.pitch];
-        col[(long long)(g.nx - 3 + q) * g.pitch] = 0.0;
+    const int Ig = I < 6 ? I + g.nx - 6 : (I >= g.nx - 6 ? I - (g.nx - 6) : -1);
+    const int Jg = J < 6 ? J + g.ny - 6 : (J >= g.ny - 6 ? J - (g.ny - 6) : -1);
+    double *p = Ub + (long long)f * g.plane;
+    double v = p[at(g, I, J)];
+    if (Jg >= 0) {
+        v = v + p[at(g, I, Jg)];
+        p[at(g, I, Jg)] = 0.0;
     }
+    if (Ig >= 0) {
+        double w = p[at(g, Ig, J)];
+        if (Jg >= 0) {
+            w = w + p[at(g, Ig, Jg)];
+            p[at(g, Ig, Jg)] = 0.0;
+        }
+        p[at(g, Ig, J)] = 0.0;
+        v = v + w;
+    }
+    p[at(g, I, J)] = v;
 }
 
 // Pitched plane -> dense (nx, ny) table.
@@ -246,8 +264,8 @@ void launch_adjoint_stage(const AdjStageArgs &a, cudaStream_t st)
 
 void launch_boundary_transpose(const Grid &g, double *Ub, cudaStream_t st)
 {
-    periodic_y_transpose<<<blocks_for((long long)g.nx * NFIELD, 128), 128, 0, st>>>(g, Ub);
-    periodic_x_transpose<<<blocks_for((long long)g.ny * NFIELD, 128), 128, 0, st>>>(g, Ub);
+    const long long n = (6LL * (g.nx - 6) + 6LL * (g.ny - 12)) * NFIELD;
+    periodic_transpose_kernel<<<blocks_for(n, 256), 256, 0, st>>>(g, Ub);
 }
 
 void launch_plane_to_table(const Grid &g, const double *plane, double *tab, cudaStream_t st)

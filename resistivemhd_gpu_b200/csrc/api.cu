@@ -70,6 +70,7 @@ struct AdjointWork {
     double *ckpt = nullptr;          // nseg states: U at steps 0, interval, 2*interval, ...
     double *seg0 = nullptr;          // interval states: U^n of each step of a segment (recomputed)
     double *seg1 = nullptr;          // interval states: U* of each step of a segment (recomputed)
+    std::vector<CUtensorMap> map0, map1;   // stage-1 maps of the seg0 slots, stage-2 maps of the seg1 slots
     double *ub[3] = {nullptr, nullptr, nullptr};   // adjoint states
     double *Q = nullptr;             // 18 planes
     double *IF = nullptr;            // 32 planes
@@ -199,6 +200,31 @@ BatchLauncher batch_launcher(int precision)
     case RMHD2D_FP32_BULK: return bulk32::launch_stage_batch;
     default: return exact::launch_stage_batch;
     }
+}
+
+// One stage-1-EMF step from `un` (read through map_un) into `dst`, with U*
+// in `ustar` (read through map_ustar); the same launches as enqueue_step
+// without A and B.  dst may not be un.
+void enqueue_step_between(rmhd2d_solver *s, int parity, const double *un, const CUtensorMap *map_un, double *ustar,
+                          const CUtensorMap *map_ustar, double *dst)
+{
+    StageArgs a{};
+    a.g = s->g;
+    a.eta = s->eta;
+    a.row2 = s->g.bc_x == BC_SYMMETRIC ? s->row2 : nullptr;
+    a.ctl = s->ctl;
+    a.parity = parity;
+    auto launch = stage_launcher(s->cfg.precision);
+    a.src = un;
+    a.un = un;
+    a.dst = ustar;
+    launch(1, s->shape, map_un, &s->mapE1[s->shape], a, s->stream);
+    launch_boundary(s->g, ustar, s->row2, nullptr, 0, s->stream);
+    a.src = ustar;
+    a.un = un;
+    a.dst = dst;
+    launch(2, s->shape, map_ustar, &s->mapE2[s->shape], a, s->stream);
+    launch_boundary(s->g, dst, s->row2, s->ctl, parity ^ 1, s->stream);
 }
 
 void enqueue_step(rmhd2d_solver *s, int parity)
@@ -1322,20 +1348,29 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
     CK(cudaMemcpyAsync(w->aos, host_seed, naos * sizeof(double), cudaMemcpyHostToDevice, st));
     launch_aos_to_planes(g, w->aos, w->ub[0], st);
     CK(cudaMemsetAsync(w->etab, 0, (size_t)g.plane * sizeof(double), st));
+    // tensor maps of the segment slots for the solver's tile shape
+    w->map0.resize(w->interval);
+    w->map1.resize(w->interval);
+    for (int k = 0; k < w->interval; ++k)
+        if (!encode_state_map(&w->map0[k], g, w->seg0 + (size_t)k * sd, stage_ui(1, s->shape), shape_uj(s->shape)) ||
+            !encode_state_map(&w->map1[k], g, w->seg1 + (size_t)k * sd, stage_ui(2, s->shape), shape_uj(s->shape)))
+            return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint's segment states");
     int rc = set_fixed_dt_mode(s, 1);
     if (rc) return rc;
     int cur = 0;
     for (int seg = w->nseg - 1; seg >= 0; --seg) {
         const int n0 = seg * w->interval;
         const int n1 = std::min(n0 + w->interval, w->nsteps);
-        // recompute the segment from its checkpoint with the recorded dts
-        CK(cudaMemcpyAsync(s->A, w->ckpt + (size_t)seg * sd, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        // recompute the segment from its checkpoint with the recorded dts,
+        // each step reading U^n from and writing U* and U^{n+1} into the
+        // segment's slots (the last U^{n+1} is not needed: A takes it)
+        CK(cudaMemcpyAsync(w->seg0, w->ckpt + (size_t)seg * sd, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
         for (int n = n0; n < n1; ++n) {
-            const size_t o = (size_t)(n - n0) * sd;
-            CK(cudaMemcpyAsync(w->seg0 + o, s->A, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            const int k = n - n0;
+            const size_t o = (size_t)k * sd;
             CK(cudaMemcpyAsync(&s->ctl->dt_fixed, w->dts + n, sizeof(double), cudaMemcpyDeviceToDevice, st));
-            enqueue_step(s, 0);
-            CK(cudaMemcpyAsync(w->seg1 + o, s->B, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            double *next = n + 1 < n1 ? w->seg0 + o + sd : s->A;
+            enqueue_step_between(s, 0, w->seg0 + o, &w->map0[k], w->seg1 + o, &w->map1[k], next);
         }
         // reverse sweep over the segment
         for (int n = n1 - 1; n >= n0; --n) {

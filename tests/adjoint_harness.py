@@ -32,6 +32,16 @@ def misfit(final, target):
     return 0.5 * (d * d).sum()
 
 
+def misfit_difference(final_p: np.ndarray, final_m: np.ndarray, target: np.ndarray) -> float:
+    """misfit(final_p) - misfit(final_m), formed as sum (f_p - f_m) (mean -
+    target): the same number without subtracting two large misfits, whose
+    own rounding would swamp a central difference along a localized
+    direction."""
+    f = list(MISFIT_FIELDS)
+    fp, fm, t = final_p[3:-3, 3:-3, f], final_m[3:-3, 3:-3, f], target[3:-3, 3:-3, f]
+    return float(((fp - fm) * (0.5 * (fp + fm) - t)).sum())
+
+
 def misfit_seed(final: np.ndarray, target: np.ndarray) -> np.ndarray:
     seed = np.zeros_like(final)
     f = list(MISFIT_FIELDS)
