@@ -655,8 +655,8 @@ def contact_block(args, setup, label, local_rank):
             out[ct] = {"value": setup.interior_cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
                        "crashed": sol.check_crashed()}
     out["contact_over_stage1_time"] = out["contact"]["ms_per_step"] / out["stage1"]["ms_per_step"]
-    out["note"] = ("CT-Contact runs as 12 unfused launches per step (fluxes to HBM, per-cell EMF inputs, one "
-                   "CT at the end); the stage-1-EMF step is the fused 4-launch pipeline")
+    out["note"] = ("CT-Contact runs as 13 launches per step (tiled fluxes to HBM, per-cell EMF inputs, the "
+                   "corner EMFs, one CT at the end); the stage-1-EMF step is the fused 4-launch pipeline")
     return out
 
 
