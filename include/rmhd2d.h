@@ -231,7 +231,8 @@ const char *rmhd2d_batch_last_error(const rmhd2d_batch *b);
    field to the state after nsteps steps, with the dt of every step held at
    its recorded value.  Branch points (minmod's choice, the HLLD region, the
    clamped wave speeds) take the derivative of the branch the forward run
-   took.  The walls must be periodic in x and y.
+   took.  Each wall kind must be periodic or symmetric (any pairing of the
+   two); the step must use the stage-1-EMF CT.
 
    rmhd2d_run_fixed_dt: nsteps steps with the given dts (host array)
    instead of the CFL dt; the state, dt and total time advance as in
@@ -248,7 +249,10 @@ const char *rmhd2d_batch_last_error(const rmhd2d_batch *b);
    rmhd2d_adjoint_backward: given seed = dJ/dU_N (nx*ny*8 doubles, the
    state layout above; host memory), writes dJ/dU_0 into grad_state, the
    gradient with respect to the state passed to rmhd2d_set_state with
-   apply_boundary = 1 (ghost entries 0), and, when grad_eta is not NULL,
+   apply_boundary = 1 (ghost entries 0, except, with symmetric x walls, bY
+   of the lower wall face (j = 2) in columns 3, 4, nx-6, nx-5 and nx-4,
+   which the x walls' normal-B integration reads before the y pass replaces
+   it), and, when grad_eta is not NULL,
    dJ/d eta into grad_eta (nx*ny, k = j + i*ny; the cell-centred eta field,
    the table when one is set, else the uniform eta spread over the cells).
    Each segment between checkpoints is recomputed once; the solver's state

@@ -240,6 +240,148 @@ __global__ void periodic_transpose_kernel(Grid g, double *Ub)
     p[at(g, I, J)] = v;
 }
 
+// Transpose of the symmetric walls and of mixed periodic / symmetric walls.
+// The forward (TS boundary.cu:4-205, as the oracle's tangent restates it)
+// runs the x pass over every row, then the y pass over every column.  Each
+// pass copies every field but the wall-normal B from the mirror cells
+// (ghost 2 <- 3, 1 <- 4, 0 <- 5 and their upper twins) and integrates the
+// normal B into the wall from its neighbours' tangential B, e.g. at the
+// lower y wall, for column i > 0,
+//   bY(i,2) = bY(i,3) + (bX(i,3) - bX(i-1,3)) dy/dx
+//   bY(i,1) = bY(i,2) + (bX(i,2) - bX(i-1,2)) dy/dx      (bX(.,2) a copy of row 3)
+//   bY(i,0) = bY(i,1) + (bX(i,1) - bX(i-1,1)) dy/dx      (bX(.,1) a copy of row 4)
+// The transposes run in the opposite order, y then x, in gather form: a
+// thread owns one column (y) or one row (x), takes the chain adjoints of
+// its own and of the next column or row, and writes only its own entries;
+// the ghost entries it reads are zeroed by a separate launch after it.  The
+// x pass at row 3 reads the lower wall face bY(c,2) before the y pass
+// replaces it -- in the step, the stage-1 CT result (row2) -- so the x
+// transpose leaves that adjoint in the ghost entry (c,2) of the interior
+// columns, where the stage-1 reverse takes it as the CT'd face's.
+
+// Running sums of a lower and an upper chain's output adjoints: t1 = the
+// sum of all three, t2 = the outer two, t3 = the outermost.
+struct ChainAdj {
+    double t1, t2, t3;
+};
+
+__device__ __forceinline__ ChainAdj chain_adj(double inner, double middle, double outer)
+{
+    return ChainAdj{inner + middle + outer, middle + outer, outer};
+}
+
+template <int BY> __global__ void ytrans_kernel(Grid g, double *Ub)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nx) return;
+    const long long P = g.plane;
+    const int ny = g.ny;
+    auto L = [&](int f, int ii, int jj) -> double & { return Ub[f * P + at(g, ii, jj)]; };
+    if (BY == BC_PERIODIC) {
+#pragma unroll
+        for (int f = 0; f < NFIELD; ++f)
+            for (int q = 0; q < 3; ++q) {
+                L(f, i, ny - 6 + q) += L(f, i, q);
+                L(f, i, 3 + q) += L(f, i, ny - 3 + q);
+            }
+        return;
+    }
+    const double c = g.dy / g.dx;
+    auto lower = [&](int col) { return chain_adj(L(BYF, col, 2), L(BYF, col, 1), L(BYF, col, 0)); };
+    auto upper = [&](int col) { return chain_adj(L(BYF, col, ny - 3), L(BYF, col, ny - 2), L(BYF, col, ny - 1)); };
+    const ChainAdj lo = lower(i), up = upper(i);
+    // chain terms on bX: this column's (i > 0) and the next column's
+    const ChainAdj z{0.0, 0.0, 0.0};
+    const ChainAdj lo_own = i > 0 ? lo : z, up_own = i > 0 ? up : z;
+    const ChainAdj lo_nxt = i + 1 < g.nx ? lower(i + 1) : z, up_nxt = i + 1 < g.nx ? upper(i + 1) : z;
+    L(BYF, i, 3) += lo.t1;
+    L(BYF, i, ny - 4) += up.t1;
+    L(BXF, i, 3) += L(BXF, i, 2) + c * (lo_own.t1 - lo_nxt.t1) + c * (lo_own.t2 - lo_nxt.t2);
+    L(BXF, i, 4) += L(BXF, i, 1) + c * (lo_own.t3 - lo_nxt.t3);
+    L(BXF, i, 5) += L(BXF, i, 0);
+    L(BXF, i, ny - 4) += L(BXF, i, ny - 3) - c * (up_own.t1 - up_nxt.t1);
+    L(BXF, i, ny - 5) += L(BXF, i, ny - 2) - c * (up_own.t2 - up_nxt.t2);
+    L(BXF, i, ny - 6) += L(BXF, i, ny - 1) - c * (up_own.t3 - up_nxt.t3);
+#pragma unroll
+    for (int f = 0; f < NFIELD; ++f) {
+        if (f == BXF || f == BYF) continue;
+        L(f, i, 3) += L(f, i, 2);
+        L(f, i, 4) += L(f, i, 1);
+        L(f, i, 5) += L(f, i, 0);
+        L(f, i, ny - 4) += L(f, i, ny - 3);
+        L(f, i, ny - 5) += L(f, i, ny - 2);
+        L(f, i, ny - 6) += L(f, i, ny - 1);
+    }
+}
+
+// Zeroes ghost rows (ROWS) or the ghost columns of the interior rows.
+template <bool ROWS> __global__ void zero_ghosts_kernel(Grid g, double *Ub)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long per_field = ROWS ? 6LL * g.nx : 6LL * (g.ny - 6);
+    if (t >= per_field * NFIELD) return;
+    const int f = (int)(t / per_field);
+    const long long u = t - (long long)f * per_field;
+    int i, j;
+    if (ROWS) {
+        i = (int)(u / 6);
+        const int q = (int)(u - (long long)i * 6);
+        j = q < 3 ? q : g.ny - 6 + q;
+    } else {
+        j = 3 + (int)(u / 6);
+        const int q = (int)(u - (long long)(j - 3) * 6);
+        i = q < 3 ? q : g.nx - 6 + q;
+    }
+    Ub[(long long)f * g.plane + at(g, i, j)] = 0.0;
+}
+
+// x transpose for rows 2 .. ny-4 (row 2 only gathers the lower wall face's
+// adjoint from row 3's chains; every ghost row is zero by now).
+template <int BX> __global__ void xtrans_kernel(Grid g, double *Ub)
+{
+    const int j = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > g.ny - 4) return;
+    const long long P = g.plane;
+    const int nx = g.nx;
+    auto L = [&](int f, int ii, int jj) -> double & { return Ub[f * P + at(g, ii, jj)]; };
+    if (BX == BC_PERIODIC) {
+        if (j < 3) return;
+#pragma unroll
+        for (int f = 0; f < NFIELD; ++f)
+            for (int q = 0; q < 3; ++q) {
+                L(f, nx - 6 + q, j) += L(f, q, j);
+                L(f, 3 + q, j) += L(f, nx - 3 + q, j);
+            }
+        return;
+    }
+    const double c = g.dx / g.dy;
+    auto lower = [&](int row) { return chain_adj(L(BXF, 2, row), L(BXF, 1, row), L(BXF, 0, row)); };
+    auto upper = [&](int row) { return chain_adj(L(BXF, nx - 3, row), L(BXF, nx - 2, row), L(BXF, nx - 1, row)); };
+    const ChainAdj z{0.0, 0.0, 0.0};
+    const ChainAdj lo = j >= 3 ? lower(j) : z, up = j >= 3 ? upper(j) : z;
+    const ChainAdj lo_nxt = lower(j + 1), up_nxt = upper(j + 1);
+    // the chains' bY terms at this row: + from its own chain, - from the next
+    // row's (its j-1), through the copies 2 <- 3 and 1 <- 4
+    L(BYF, 3, j) += c * (lo.t1 - lo_nxt.t1) + c * (lo.t2 - lo_nxt.t2);
+    L(BYF, 4, j) += c * (lo.t3 - lo_nxt.t3);
+    L(BYF, nx - 4, j) -= c * (up.t1 - up_nxt.t1);
+    L(BYF, nx - 5, j) -= c * (up.t2 - up_nxt.t2);
+    L(BYF, nx - 6, j) -= c * (up.t3 - up_nxt.t3);
+    if (j < 3) return;
+    L(BXF, 3, j) += lo.t1;
+    L(BXF, nx - 4, j) += up.t1;
+#pragma unroll
+    for (int f = 0; f < NFIELD; ++f) {
+        if (f == BXF) continue;
+        L(f, 3, j) += L(f, 2, j);
+        L(f, 4, j) += L(f, 1, j);
+        L(f, 5, j) += L(f, 0, j);
+        L(f, nx - 4, j) += L(f, nx - 3, j);
+        L(f, nx - 5, j) += L(f, nx - 2, j);
+        L(f, nx - 6, j) += L(f, nx - 1, j);
+    }
+}
+
 // Pitched plane -> dense (nx, ny) table.
 __global__ void plane_to_table_kernel(Grid g, const double *plane, double *tab)
 {
@@ -264,8 +406,21 @@ void launch_adjoint_stage(const AdjStageArgs &a, cudaStream_t st)
 
 void launch_boundary_transpose(const Grid &g, double *Ub, cudaStream_t st)
 {
-    const long long n = (6LL * (g.nx - 6) + 6LL * (g.ny - 12)) * NFIELD;
-    periodic_transpose_kernel<<<blocks_for(n, 256), 256, 0, st>>>(g, Ub);
+    if (g.bc_x == BC_PERIODIC && g.bc_y == BC_PERIODIC) {
+        const long long n = (6LL * (g.nx - 6) + 6LL * (g.ny - 12)) * NFIELD;
+        periodic_transpose_kernel<<<blocks_for(n, 256), 256, 0, st>>>(g, Ub);
+        return;
+    }
+    if (g.bc_y == BC_PERIODIC)
+        ytrans_kernel<BC_PERIODIC><<<blocks_for(g.nx, 128), 128, 0, st>>>(g, Ub);
+    else
+        ytrans_kernel<BC_SYMMETRIC><<<blocks_for(g.nx, 128), 128, 0, st>>>(g, Ub);
+    zero_ghosts_kernel<true><<<blocks_for(6LL * g.nx * NFIELD, 256), 256, 0, st>>>(g, Ub);
+    if (g.bc_x == BC_PERIODIC)
+        xtrans_kernel<BC_PERIODIC><<<blocks_for(g.ny - 5, 128), 128, 0, st>>>(g, Ub);
+    else
+        xtrans_kernel<BC_SYMMETRIC><<<blocks_for(g.ny - 5, 128), 128, 0, st>>>(g, Ub);
+    zero_ghosts_kernel<false><<<blocks_for(6LL * (g.ny - 6) * NFIELD, 256), 256, 0, st>>>(g, Ub);
 }
 
 void launch_plane_to_table(const Grid &g, const double *plane, double *tab, cudaStream_t st)

@@ -1254,8 +1254,8 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     if (nsteps < 1) return fail(s, RMHD2D_ERR_INVALID, "nsteps must be >= 1");
-    if (s->g.bc_x != BC_PERIODIC || s->g.bc_y != BC_PERIODIC)
-        return fail(s, RMHD2D_ERR_INVALID, "the discrete adjoint is implemented for periodic x and y walls");
+    if ((s->g.bc_x != BC_PERIODIC && s->g.bc_x != BC_SYMMETRIC) || (s->g.bc_y != BC_PERIODIC && s->g.bc_y != BC_SYMMETRIC))
+        return fail(s, RMHD2D_ERR_INVALID, "the discrete adjoint is implemented for periodic and symmetric walls");
     if (s->contact) return fail(s, RMHD2D_ERR_INVALID, "the discrete adjoint differentiates the stage-1-EMF step");
     CK(cudaSetDevice(s->device));
     int interval = checkpoint_interval;

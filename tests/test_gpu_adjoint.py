@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 
 ADJ_REL = 1e-10
 FD_REL = 1e-6
+HARRIS_REL = 1e-5
 
 
 def _dirs(setup, seed):
@@ -29,15 +30,32 @@ def _eta_field(setup):
     return setup.eta_table if setup.eta_table is not None else np.full((setup.nx, setup.ny), setup.eta)
 
 
-@pytest.mark.parametrize("with_table,shape,nsteps,interval", [
-    (False, (20, 18), 5, 2),
-    (True, (26, 21), 6, 0),
-    (True, (16, 16), 4, 4),
+def _ghost_gradient_is_zero(gs, nx, bc):
+    """Ghost entries of dJ/dU_0 are 0 (set_state's boundary overwrites them),
+    except, with symmetric x walls, the lower wall face bY(c, 2) that the x
+    walls' normal-B integration reads (c = 3, 4, nx-6, nx-5, nx-4)."""
+    ghost = np.ones(gs.shape[:2], bool)
+    ghost[3:-3, 3:-3] = False
+    mask = np.repeat(ghost[..., None], 8, axis=2)
+    if bc == "symmetric":
+        for c in (3, 4, nx - 6, nx - 5, nx - 4):
+            mask[c, 2, 5] = False
+    return np.all(gs[mask] == 0)
+
+
+@pytest.mark.parametrize("with_table,shape,nsteps,interval,bc,bc_y", [
+    (False, (20, 18), 5, 2, "periodic", None),
+    (True, (26, 21), 6, 0, "periodic", None),
+    (True, (16, 16), 4, 4, "periodic", None),
+    (False, (20, 18), 5, 2, "symmetric", None),
+    (True, (23, 26), 6, 0, "symmetric", None),
+    (True, (18, 21), 4, 2, "periodic", "symmetric"),
+    (False, (21, 17), 5, 0, "symmetric", "periodic"),
 ])
-def test_adjoint_matches_oracle_tangent(gpu, oracle, tangent, with_table, shape, nsteps, interval):
+def test_adjoint_matches_oracle_tangent(gpu, oracle, tangent, with_table, shape, nsteps, interval, bc, bc_y):
     from resistivemhd_gpu_b200 import Solver, setups
 
-    s = setups.random_smooth_state(*shape, seed=21, bc="periodic", with_table=with_table)
+    s = setups.random_smooth_state(*shape, seed=21, bc=bc, bc_y=bc_y, with_table=with_table)
     ref, ref_dts, crashed = oracle.run(s, s.state, nsteps)
     assert crashed == -1
     w = np.random.default_rng(5).standard_normal(s.state.shape)
@@ -47,7 +65,7 @@ def test_adjoint_matches_oracle_tangent(gpu, oracle, tangent, with_table, shape,
         assert np.array_equal(dts, ref_dts)
         assert np.array_equal(sol.get_state(), ref)
         gs, ge = sol.adjoint_backward(w)
-    assert np.all(gs[:3] == 0) and np.all(gs[-3:] == 0) and np.all(gs[:, :3] == 0) and np.all(gs[:, -3:] == 0)
+    assert _ghost_gradient_is_zero(gs, s.nx, bc)
     for k in range(3):
         d, deta = _dirs(s, 100 + k)
         _, dU = tangent.tangent(s, s.state, d, dts, deta=deta)
@@ -163,10 +181,36 @@ def test_adjoint_against_central_differences(gpu):
         sol.close()
 
 
-def test_adjoint_rejects_symmetric_walls(gpu):
+def test_adjoint_rejects_other_walls(gpu):
     from resistivemhd_gpu_b200 import Solver, _lib, setups
 
-    s = setups.harris_sheet(64, 32)
+    s = setups.random_smooth_state(20, 18, seed=1, bc="periodic", bc_y="zero_gradient")
     with Solver.from_setup(s, precision="fp64_exact") as sol:
         with pytest.raises(_lib.RMHDError):
             sol.adjoint_forward(2)
+
+
+def test_adjoint_on_the_harris_sheet(gpu, tangent):
+    """Symmetric walls and the eta table of the Harris workload (64 x 32):
+    the gradient along seeded directions against the oracle's tangent.
+
+    The sheet reverses B_x, so many interfaces sit near the HLLD's degenerate
+    star state (tangential B -> 0), where the flux derivatives grow like the
+    inverse square of a small denominator, and the start is exactly uniform
+    along x and mirror symmetric, so some sit on branch ties.  There the
+    reverse sweep (reciprocals) and the dual-number tangent (divisions) do
+    not round alike; they agree to HARRIS_REL instead of ADJ_REL."""
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = setups.harris_sheet(64, 32)
+    w = np.random.default_rng(3).standard_normal(s.state.shape)
+    with Solver.from_setup(s, precision="fp64_exact") as sol:
+        sol.adjoint_forward(6, 0)
+        dts = sol.adjoint_dts()
+        gs, ge = sol.adjoint_backward(w)
+    assert _ghost_gradient_is_zero(gs, s.nx, "symmetric")
+    for k in range(2):
+        d, deta = _dirs(s, 200 + k)
+        _, dU = tangent.tangent(s, s.state, d, dts, deta=deta)
+        assert float((gs * d).sum() + (ge * deta).sum()) == pytest.approx(float((w * dU).sum()), rel=HARRIS_REL,
+                                                                            abs=1e-14)

@@ -82,6 +82,31 @@ def test_exact_bitwise_vs_oracle(gpu, oracle, bc, table, shape):
     assert np.array_equal(out, ref, equal_nan=True)
 
 
+@pytest.mark.parametrize("case", ["huge", "nan"])
+def test_exact_bitwise_vs_oracle_on_extreme_values(gpu, oracle, case):
+    """The exact HLLD forms the selected candidate alone only where all six
+    candidates are provably finite (every candidate value below 1e75), and
+    the reference's full weighted sum elsewhere.  A patch scaled by 1e80
+    (candidate fluxes overflow) and a NaN energy (propagated through the
+    weighted sum's 0 * NaN) take the second path; both must still give the
+    reference's bits, NaNs included, dt and all (both crash in their first
+    step, as the reference does)."""
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(40, 36, seed=11, bc="periodic")
+    st = s.state.copy()
+    if case == "huge":
+        st[18:21, 15:19, :] *= 1e80
+    else:
+        st[18, 15, 7] = np.nan
+    s.state = st
+    ref, rdts, crashed_at = oracle.run(s, st, 3)
+    n = 3 if crashed_at < 0 else crashed_at + 1
+    out, cdts, _, _ = run_cuda(s, n)
+    assert np.array_equal(cdts, rdts[:n], equal_nan=True)
+    assert np.array_equal(out, ref, equal_nan=True)
+
+
 @pytest.mark.parametrize("bc,bc_y,table,shape", [
     ("periodic", "symmetric", False, (40, 33)),   # oneStepRK2PeriodicXSymmetricY
     ("periodic", "symmetric", True, (17, 70)),
