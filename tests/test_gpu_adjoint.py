@@ -194,12 +194,12 @@ def test_adjoint_on_the_harris_sheet(gpu, tangent):
     """Symmetric walls and the eta table of the Harris workload (64 x 32):
     the gradient along seeded directions against the oracle's tangent.
 
-    The sheet reverses B_x, so many interfaces sit near the HLLD's degenerate
-    star state (tangential B -> 0), where the flux derivatives grow like the
-    inverse square of a small denominator, and the start is exactly uniform
-    along x and mirror symmetric, so some sit on branch ties.  There the
-    reverse sweep (reciprocals) and the dual-number tangent (divisions) do
-    not round alike; they agree to HARRIS_REL instead of ADJ_REL."""
+    The start is exactly uniform along x and mirror symmetric, so some
+    branch decisions sit exactly on ties and the frozen-dt map has kinks at
+    the base point itself (one-sided finite differences of the oracle
+    disagree there); the reverse sweep and the dual-number tangent then take
+    slightly different one-sided derivatives at a few components, and agree
+    to HARRIS_REL instead of ADJ_REL."""
     from resistivemhd_gpu_b200 import Solver, setups
 
     s = setups.harris_sheet(64, 32)
