@@ -65,7 +65,6 @@ sys.path.insert(0, str(ROOT))
 METRIC = "cell-updates/s"
 MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
-B200_FP64_TFLOPS_NOMINAL = 37.0
 
 
 def workload(name: str):
@@ -94,6 +93,22 @@ def hbm_peak():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+B200_FP64_TFLOPS_NOMINAL_PIPE = 148 * 64 * 2 * 1.965e9 / 1e12   # SMs x FP64 FMA lanes x 2 x max clock
+
+
+def flops_from_profile(label: str):
+    """Floating-point operations per cell-update of the algorithm, from the
+    committed count (profiles/flops_<label>.md, line
+    'flops_per_cell_update:')."""
+    p = ROOT / "profiles" / f"flops_{label}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("flops_per_cell_update:"):
+            return float(line.split(":", 1)[1])
+    return None
 
 
 def traffic_from_profile(label: str):
@@ -310,9 +325,18 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
         }
         if e2e:
             line["e2e"] = e2e
-        # FP64 issue bound: executed FP64 instruction rate is in the ncu summary.
-        line["fp64"] = {"peak_nominal_tflops": B200_FP64_TFLOPS_NOMINAL,
-                        "see": f"profiles/stage_kernel_{label}_{args.precision}.md"}
+        # The FP64 roofline beside the HBM one: the algorithm's flops per
+        # cell-update (counted on the oracle's operation-counting scalar,
+        # profiles/flops_<label>.md) times the measured rate, against the
+        # nominal FP64 pipe rate (the measured peaks file has no FP64 figure).
+        fpc = flops_from_profile(label)
+        achieved_tf = None if fpc is None else fpc * value / world / 1e12   # per GPU
+        line["fp64"] = {"bound": "fp64", "flops_per_cell_update": fpc, "achieved_tflops": achieved_tf,
+                        "peak_tflops": B200_FP64_TFLOPS_NOMINAL_PIPE,
+                        "peak_kind": "nominal: 148 SMs x 64 FP64 FMA lanes x 2 x 1.965 GHz",
+                        "frac": None if achieved_tf is None else achieved_tf / B200_FP64_TFLOPS_NOMINAL_PIPE,
+                        "flops_source": f"profiles/flops_{label}.md",
+                        "pipe_counters": f"profiles/stage_kernel_{label}_{args.precision}.md"}
     sol.close()
 
     if rank == 0 and world == 1 and args.baselines:

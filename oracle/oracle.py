@@ -75,6 +75,7 @@ class TangentLib:
         self.lib.orc_run_fixed_dt.argtypes = [P, D, ctypes.c_int, D, ctypes.c_int]
         self.lib.orc_tangent_run.argtypes = [P, D, D, D, ctypes.c_int, D]
         self.lib.orc_hlld_jvp.argtypes = [D, D, D, D, ctypes.c_double, ctypes.c_double, D, D]
+        self.lib.orc_count_ops.argtypes = [P, D, ctypes.c_int, D, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong)]
 
     @staticmethod
     def _d(a):
@@ -100,6 +101,18 @@ class TangentLib:
         self.lib.orc_tangent_run(ctypes.byref(p), self._d(s), self._d(ds), None if de is None else self._d(de),
                                  len(d), self._d(d))
         return s, ds
+
+    def count_ops(self, setup, state, dts, apply_boundary=True):
+        """(U_N, counts) of the run on the operation-counting scalar; counts
+        maps add (incl. sub), mul, div, sqrt, abs, cmp to totals over the
+        whole array and all steps."""
+        keep = []
+        p = OracleLib._params(setup, keep)
+        s = np.ascontiguousarray(state, dtype=np.float64).copy()
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        c = (ctypes.c_ulonglong * 6)()
+        self.lib.orc_count_ops(ctypes.byref(p), self._d(s), len(d), self._d(d), int(bool(apply_boundary)), c)
+        return s, dict(zip(("add", "mul", "div", "sqrt", "abs", "cmp"), (int(v) for v in c)))
 
     def hlld_jvp(self, L, R, dL, dR, gamma, eps):
         f, df = np.zeros(8), np.zeros(8)

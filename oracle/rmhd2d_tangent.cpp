@@ -14,13 +14,17 @@
  * from the state, since the adjoint differentiates the step with its dt
  * held fixed.  Branches (minmod's choice, thrust::min/max, the HLLD region
  * indicators) follow the value, so the derivative is the one-sided one of
- * the branch taken, which is the subgradient the adjoint uses.
+ * the branch taken, which is the subgradient the adjoint uses.  Instantiated
+ * on an operation-counting scalar it gives the step's floating-point
+ * operation count (the algorithm's flops per cell-update).
  *
  * Build: g++ -O2 -ffp-contract=off -fno-fast-math -fopenmp -shared -fPIC.
  */
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+
+#include <omp.h>
 
 #include <vector>
 
@@ -60,14 +64,42 @@ inline Dual sqrt(Dual a)
 }
 inline Dual fabs(Dual a) { return a.v < 0.0 ? -a : (a.v > 0.0 ? a : Dual(0.0, 0.0)); }
 
+/* Operation-counting scalar: a double that counts the floating-point
+   operations applied to it (into g_ops; run single-threaded).  Instantiated
+   on it, the step is the oracle's arithmetic with its operation count. */
+struct OpCounts {
+    unsigned long long add, mul, div, sqrt, abs, cmp;
+};
+OpCounts g_ops;
+
+struct Counted {
+    double v;
+    Counted() : v(0.0) {}
+    Counted(double x) : v(x) {}
+};
+inline Counted operator+(Counted a, Counted b) { ++g_ops.add; return Counted(a.v + b.v); }
+inline Counted operator-(Counted a, Counted b) { ++g_ops.add; return Counted(a.v - b.v); }
+inline Counted operator-(Counted a) { return Counted(-a.v); }
+inline Counted operator*(Counted a, Counted b) { ++g_ops.mul; return Counted(a.v * b.v); }
+inline Counted operator/(Counted a, Counted b) { ++g_ops.div; return Counted(a.v / b.v); }
+inline Counted &operator+=(Counted &a, Counted b) { a = a + b; return a; }
+inline Counted &operator-=(Counted &a, Counted b) { a = a - b; return a; }
+inline bool operator<(Counted a, Counted b) { ++g_ops.cmp; return a.v < b.v; }
+inline bool operator>(Counted a, Counted b) { ++g_ops.cmp; return a.v > b.v; }
+inline bool operator<=(Counted a, Counted b) { ++g_ops.cmp; return a.v <= b.v; }
+inline Counted sqrt(Counted a) { ++g_ops.sqrt; return Counted(::sqrt(a.v)); }
+inline Counted fabs(Counted a) { ++g_ops.abs; return Counted(::fabs(a.v)); }
+
 inline double val(double x) { return x; }
 inline double val(Dual x) { return x.v; }
+inline double val(Counted x) { return x.v; }
 
 /* F * I for an HLLD indicator I in {0, 1}: the value is the reference's
    product; a candidate that is not selected contributes no derivative even
    where its own derivative is not finite. */
 inline double weigh(double f, double i) { return f * i; }
 inline Dual weigh(Dual f, double i) { return Dual(f.v * i, i != 0.0 ? f.d * i : 0.0); }
+inline Counted weigh(Counted f, double i) { return f * Counted(i); }
 
 enum { RHO = 0, MX = 1, MY = 2, MZ = 3, BXF = 4, BYF = 5, BZF = 6, EN = 7, NV = 8 };
 enum { QR = 0, QU = 1, QV = 2, QW = 3, QBX = 4, QBY = 5, QBZ = 6, QP = 7 };
@@ -616,6 +648,33 @@ int orc_tangent_run(const orc_params *p, double *U, double *dU, const double *de
     st.boundary(S.data());
     for (int s = 0; s < nsteps; ++s) st.step(S.data(), dts[s]);
     for (size_t k = 0; k < N * NV; ++k) { U[k] = S[k].v; dU[k] = S[k].d; }
+    return 0;
+}
+
+/* nsteps steps with the given dts from U (boundary applied first when
+   apply_boundary != 0), on the operation-counting scalar, single-threaded:
+   U_N is written back into U and the operation counts into counts[6] =
+   {add/sub, mul, div, sqrt, abs, compare}, summed over the whole array
+   (ghost cells included) and all steps. */
+int orc_count_ops(const orc_params *p, double *U, int nsteps, const double *dts, int apply_boundary,
+                  unsigned long long *counts)
+{
+    const size_t N = (size_t)p->nx * p->ny;
+    const int threads = omp_get_max_threads();
+    omp_set_num_threads(1);
+    std::vector<Counted> eta(N), S(N * NV);
+    for (size_t k = 0; k < N; ++k) eta[k] = Counted(p->eta_table ? p->eta_table[k] : p->eta);
+    for (size_t k = 0; k < N * NV; ++k) S[k] = Counted(U[k]);
+    g_ops = OpCounts{0, 0, 0, 0, 0, 0};
+    {
+        Step<Counted> st(p, eta.data());
+        if (apply_boundary) st.boundary(S.data());
+        for (int s = 0; s < nsteps; ++s) st.step(S.data(), dts[s]);
+    }
+    for (size_t k = 0; k < N * NV; ++k) U[k] = S[k].v;
+    counts[0] = g_ops.add; counts[1] = g_ops.mul; counts[2] = g_ops.div;
+    counts[3] = g_ops.sqrt; counts[4] = g_ops.abs; counts[5] = g_ops.cmp;
+    omp_set_num_threads(threads);
     return 0;
 }
 

@@ -57,3 +57,19 @@ def test_tangent_matches_central_differences(oracle, tangent, with_table):
     h = 1e-6
     fd = (J(h) - J(-h)) / (2 * h)
     assert abs(fd - jvp) <= 1e-6 * max(abs(jvp), 1e-12), (fd, jvp)
+
+
+def test_operation_count_runs_the_same_arithmetic(oracle, tangent):
+    """The operation-counting instantiation of the template gives the double
+    run's bits, and a count per cell-update of the size the reference's
+    algorithm implies (each interface's HLLD with all six candidates)."""
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.orszag_tang(32)
+    _, dts, _ = oracle.run(s, s.state, 2)
+    ref = tangent.run_fixed_dt(s, s.state, dts)
+    out, c = tangent.count_ops(s, s.state, dts)
+    assert np.array_equal(out, ref)
+    per_cell = (c["add"] + c["mul"] + c["div"] + c["sqrt"]) / (s.interior_cells * len(dts))
+    assert 3000 < per_cell < 6000, c
+    assert c["div"] > 0 and c["sqrt"] > 0
