@@ -56,6 +56,7 @@ struct rmhd2d_solver {
     bool has_state = false;
     long long steps = 0;
     cudaGraphExec_t graph2[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph1[2] = {nullptr, nullptr};   // one step per parity (rmhd2d_step_rk2)
     AdjointWork *adj = nullptr;          // recorded trajectory and workspace of the discrete adjoint
     double *contact = nullptr;           // CT-Contact workspace: C, F1, G1, F2, G2 (8 planes each), R1, R2, E
     std::string err;
@@ -321,6 +322,10 @@ void destroy_graphs(rmhd2d_solver *s)
         if (gx) cudaGraphExecDestroy(gx);
         gx = nullptr;
     }
+    for (auto &gx : s->graph1) {
+        if (gx) cudaGraphExecDestroy(gx);
+        gx = nullptr;
+    }
 }
 
 }  // namespace
@@ -580,8 +585,32 @@ int rmhd2d_step_rk2(rmhd2d_solver *s)
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
-    enqueue_step(s, s->parity);
-    CK(cudaGetLastError());
+    // One step replayed from a captured graph: a single launch instead of
+    // the step's kernels one by one, which is what a driver loop that
+    // synchronises after every step (crash check, dt) waits on.  Under a
+    // caller's own stream capture the kernels are enqueued directly.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(s->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        enqueue_step(s, s->parity);
+        CK(cudaGetLastError());
+    } else {
+        cudaGraphExec_t &ge = s->graph1[s->parity];
+        if (!ge) {
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_step(s, s->parity);
+            cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+            if (e != cudaSuccess) return fail(s, RMHD2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&ge, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                ge = nullptr;
+                return fail(s, RMHD2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            }
+        }
+        CK(cudaGraphLaunch(ge, s->stream));
+    }
     s->parity ^= 1;
     s->steps += 1;
     return RMHD2D_OK;
