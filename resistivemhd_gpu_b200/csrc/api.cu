@@ -154,8 +154,9 @@ bool encode_eta_map(CUtensorMap *map, const Grid &g, double *base, int ui, int u
 
 int sync_and_check(rmhd2d_solver *s)
 {
+    // The control block is read behind the stream's work: one wait covers both.
+    CK(cudaMemcpyAsync(s->ctl_host, s->ctl, sizeof(Control), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    CK(cudaMemcpy(s->ctl_host, s->ctl, sizeof(Control), cudaMemcpyDeviceToHost));
     if (s->ctl_host->error != KERR_NONE)
         return fail(s, RMHD2D_ERR_KERNEL, "a stage kernel's bounded wait for its staged tile expired");
     return RMHD2D_OK;
