@@ -83,6 +83,7 @@ struct AdjointWork {
     double *final_state = nullptr;   // U at the end of the forward run
     double *aos = nullptr;           // nx*ny*8 staging for seeds and gradients
     Control ctl_final{};
+    bool recorded = false;           // the last forward run completed (nsteps, dts_host, final_state valid)
 };
 
 namespace {
@@ -315,6 +316,31 @@ int set_fixed_dt_mode(rmhd2d_solver *s, int on)
 struct DeviceBuffer {
     double *p = nullptr;
     ~DeviceBuffer() { cudaFree(p); }
+};
+
+// A CUDA event destroyed on scope exit.
+struct ScopedEvent {
+    cudaEvent_t e = nullptr;
+    ScopedEvent() = default;
+    ScopedEvent(const ScopedEvent &) = delete;
+    ScopedEvent &operator=(const ScopedEvent &) = delete;
+    ~ScopedEvent()
+    {
+        if (e) cudaEventDestroy(e);
+    }
+};
+
+// Turns Control::use_fixed_dt back off when a frozen-dt run returns early, so
+// that later steps take the CFL dt again.  The error already reported is kept.
+struct FixedDtScope {
+    rmhd2d_solver *s = nullptr;
+    bool armed = false;
+    ~FixedDtScope()
+    {
+        static const int kOff = 0;
+        if (armed)
+            cudaMemcpyAsync(&s->ctl->use_fixed_dt, &kOff, sizeof(int), cudaMemcpyHostToDevice, s->stream);
+    }
 };
 
 void destroy_graphs(rmhd2d_solver *s)
@@ -653,17 +679,15 @@ int rmhd2d_run_timed(rmhd2d_solver *s, int nsteps, float *ms)
     if (!s || !ms) return fail(s, RMHD2D_ERR_INVALID, "null argument");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventRecord(e0, s->stream));
+    ScopedEvent e0, e1;
+    CK(cudaEventCreate(&e0.e));
+    CK(cudaEventCreate(&e1.e));
+    CK(cudaEventRecord(e0.e, s->stream));
     int rc = rmhd2d_run(s, nsteps);
-    CK(cudaEventRecord(e1, s->stream));
-    CK(cudaEventSynchronize(e1));
-    CK(cudaEventElapsedTime(ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (rc) return rc;
+    CK(cudaEventRecord(e1.e, s->stream));
+    CK(cudaEventSynchronize(e1.e));
+    CK(cudaEventElapsedTime(ms, e0.e, e1.e));
     return sync_and_check(s);
 }
 
@@ -674,8 +698,12 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
     if (s->contact) return fail(s, RMHD2D_ERR_STATE, "profile_step times the four launches of the stage-1-EMF step");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
+    ScopedEvent sev[5];
     cudaEvent_t ev[5];
-    for (auto &e : ev) CK(cudaEventCreate(&e));
+    for (int n = 0; n < 5; ++n) {
+        CK(cudaEventCreate(&sev[n].e));
+        ev[n] = sev[n].e;
+    }
     const int parity = s->parity;
     StageArgs a{};
     a.g = s->g;
@@ -698,7 +726,6 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(ev[4]));
     for (int n = 0; n < 4; ++n) CK(cudaEventElapsedTime(&ms4[n], ev[n], ev[n + 1]));
-    for (auto &e : ev) cudaEventDestroy(e);
     s->parity ^= 1;
     s->steps += 1;
     return sync_and_check(s);
@@ -804,10 +831,14 @@ int rmhd2d_get_tile_shape(const rmhd2d_solver *s, int *shape)
 // Saves the user-visible state (A and the control block) of a solver so that
 // trial steps can be undone.
 struct Snapshot {
-    double *A = nullptr;
+    double *A = nullptr;   // owned: freed on restore or on scope exit
     Control ctl{};
     int parity = 0;
     long long steps = 0;
+    Snapshot() = default;
+    Snapshot(const Snapshot &) = delete;
+    Snapshot &operator=(const Snapshot &) = delete;
+    ~Snapshot() { cudaFree(A); }
 };
 
 static int snapshot_take(rmhd2d_solver *s, Snapshot &sn)
@@ -1138,17 +1169,15 @@ int rmhd2d_batch_run_timed(rmhd2d_batch *b, int nsteps, float *ms)
     BCK(cudaSetDevice(b->device));
     int rc = batch_build(b);
     if (rc) return rc;
-    cudaEvent_t e0, e1;
-    BCK(cudaEventCreate(&e0));
-    BCK(cudaEventCreate(&e1));
-    BCK(cudaEventRecord(e0, b->stream));
+    ScopedEvent e0, e1;
+    BCK(cudaEventCreate(&e0.e));
+    BCK(cudaEventCreate(&e1.e));
+    BCK(cudaEventRecord(e0.e, b->stream));
     rc = rmhd2d_batch_run(b, nsteps);
-    BCK(cudaEventRecord(e1, b->stream));
-    BCK(cudaEventSynchronize(e1));
-    BCK(cudaEventElapsedTime(ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (rc) return rc;
+    BCK(cudaEventRecord(e1.e, b->stream));
+    BCK(cudaEventSynchronize(e1.e));
+    BCK(cudaEventElapsedTime(ms, e0.e, e1.e));
     for (auto *s : b->runs) {
         const int r2 = sync_and_check(s);
         if (r2) return bfail(b, r2, rmhd2d_last_error(s));
@@ -1183,10 +1212,15 @@ int rmhd2d_batch_autotune(rmhd2d_batch *b, int trial_steps, int *best_shape, int
                 bc = c;
             }
         }
-    for (size_t r = 0; r < b->runs.size(); ++r) snapshot_restore(b->runs[r], sn[r]);
+    int rc_restore = RMHD2D_OK;
+    for (size_t r = 0; r < b->runs.size(); ++r) {
+        const int r2 = snapshot_restore(b->runs[r], sn[r]);
+        if (r2 && !rc_restore) rc_restore = bfail(b, r2, rmhd2d_last_error(b->runs[r]));
+    }
     b->parity = par0;
     b->steps = steps0;
     if (rc) return rc;
+    if (rc_restore) return rc_restore;
     rc = rmhd2d_batch_set_launch(b, bs, bc);
     if (best_shape) *best_shape = bs;
     if (best_ctas_per_sm) *best_ctas_per_sm = bc;
@@ -1266,12 +1300,14 @@ extern "C" int rmhd2d_run_fixed_dt(rmhd2d_solver *s, int nsteps, const double *h
     CK(cudaMemcpyAsync(d.p, host_dts, (size_t)nsteps * sizeof(double), cudaMemcpyHostToDevice, s->stream));
     int rc = set_fixed_dt_mode(s, 1);
     if (rc) return rc;
+    FixedDtScope fixed{s, true};
     for (int n = 0; n < nsteps; ++n) {
         CK(cudaMemcpyAsync(&s->ctl->dt_fixed, d.p + n, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
         enqueue_step(s, s->parity);
         s->parity ^= 1;
         s->steps += 1;
     }
+    fixed.armed = false;
     rc = set_fixed_dt_mode(s, 0);
     if (rc) return rc;
     CK(cudaGetLastError());
@@ -1335,6 +1371,7 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
         w->cap_steps = nsteps;
         s->adj = w;
     }
+    w->recorded = false;
     w->nsteps = nsteps;
     w->interval = interval;
     w->nseg = nseg;
@@ -1354,13 +1391,15 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
     w->dts_host.resize(nsteps);
     CK(cudaMemcpy(w->dts_host.data(), w->dts, (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost));
     w->ctl_final = *s->ctl_host;
+    w->recorded = true;
     return RMHD2D_OK;
 }
 
 extern "C" int rmhd2d_adjoint_dts(rmhd2d_solver *s, double *host_dts)
 {
     if (!s || !host_dts) return fail(s, RMHD2D_ERR_INVALID, "null argument");
-    if (!s->adj) return fail(s, RMHD2D_ERR_STATE, "no recorded forward run (rmhd2d_adjoint_forward)");
+    if (!s->adj || !s->adj->recorded)
+        return fail(s, RMHD2D_ERR_STATE, "no recorded forward run (rmhd2d_adjoint_forward)");
     std::memcpy(host_dts, s->adj->dts_host.data(), s->adj->dts_host.size() * sizeof(double));
     return RMHD2D_OK;
 }
@@ -1369,7 +1408,8 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
                                        double *host_grad_eta)
 {
     if (!s || !host_seed || !host_grad_state) return fail(s, RMHD2D_ERR_INVALID, "null argument");
-    if (!s->adj) return fail(s, RMHD2D_ERR_STATE, "no recorded forward run (rmhd2d_adjoint_forward)");
+    if (!s->adj || !s->adj->recorded)
+        return fail(s, RMHD2D_ERR_STATE, "no recorded forward run (rmhd2d_adjoint_forward)");
     CK(cudaSetDevice(s->device));
     AdjointWork *w = s->adj;
     const Grid &g = s->g;
@@ -1387,6 +1427,7 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
             return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint's segment states");
     int rc = set_fixed_dt_mode(s, 1);
     if (rc) return rc;
+    FixedDtScope fixed{s, true};
     int cur = 0;
     for (int seg = w->nseg - 1; seg >= 0; --seg) {
         const int n0 = seg * w->interval;
@@ -1446,9 +1487,10 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(host_grad_eta, w->aos, (size_t)g.nx * g.ny * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
-    // back to the end of the forward run
+    // back to the end of the forward run (its control block has use_fixed_dt off)
     CK(cudaMemcpyAsync(s->A, w->final_state, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s->ctl, &w->ctl_final, sizeof(Control), cudaMemcpyHostToDevice, st));
+    fixed.armed = false;
     return sync_and_check(s);
 }
 

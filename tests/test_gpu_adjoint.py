@@ -190,6 +190,31 @@ def test_adjoint_rejects_other_walls(gpu):
             sol.adjoint_forward(2)
 
 
+def test_adjoint_needs_a_recorded_run(gpu):
+    """backward and adjoint_dts are refused before a forward run and after
+    adjoint_release, and a refused call leaves the solver stepping with the
+    CFL dt."""
+    from resistivemhd_gpu_b200 import Solver, _lib, setups
+
+    s = setups.random_smooth_state(20, 18, seed=2, bc="periodic")
+    with Solver.from_setup(s, precision="fp64_exact") as sol, \
+            Solver.from_setup(s, precision="fp64_exact") as ref:
+        seed = np.zeros_like(s.state)
+        with pytest.raises(_lib.RMHDError):
+            sol.adjoint_backward(seed)
+        sol.adjoint_forward(2)
+        sol.adjoint_release()
+        with pytest.raises(_lib.RMHDError):
+            sol.adjoint_backward(seed)
+        with pytest.raises(_lib.RMHDError):
+            sol.adjoint_dts()
+        ref.run(2)
+        sol.run(3)
+        ref.run(3)
+        assert sol.dt == ref.dt
+        assert np.array_equal(sol.get_state(), ref.get_state())
+
+
 def test_adjoint_on_the_harris_sheet(gpu, tangent):
     """Symmetric walls and the eta table of the Harris workload (64 x 32):
     the gradient along seeded directions against the oracle's tangent.
