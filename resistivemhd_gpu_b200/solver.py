@@ -27,10 +27,14 @@ def _as_f64(a: np.ndarray) -> np.ndarray:
 class Solver:
     """One solver instance on one CUDA device.
 
-    ``nx``, ``ny`` include 3 ghost layers per side.  ``bc`` is "periodic" or
-    "symmetric" (both directions).  ``precision`` is "fp64_exact" (bit-for-bit
-    the reference's IEEE binary64 arithmetic) or "fp64_fast" (FMA contraction).
-    ``stream`` may be a CUDA stream handle (int) to enqueue on."""
+    ``nx``, ``ny`` include 3 ghost layers per side.  ``bc`` names the x walls
+    and, unless ``bc_y`` is given, the y walls too: "periodic", "symmetric",
+    "zero_gradient", "flare" (x only) or "wall" (y only).  ``precision`` is
+    "fp64_exact" (bit-for-bit the reference's IEEE binary64 arithmetic),
+    "fp64_fast" (FMA contraction) or "fp32_bulk" (FP32 reconstruction and
+    fan, FP64 stresses, update and dt).  ``ct`` is "stage1" (the single-GPU
+    library's stage-1 EMF) or "contact" (CT-Contact).  ``stream`` may be a
+    CUDA stream handle (int) to enqueue on."""
 
     def __init__(self, nx: int, ny: int, dx: float, dy: float, *, gamma: float = 5.0 / 3.0, cfl: float = 0.4,
                  eps: float = 1e-20, eta: float = 0.0, bc: str = "periodic", bc_y: str | None = None,
@@ -364,6 +368,16 @@ class ResistiveMHD2D:
     @property
     def solver(self) -> Solver:
         return self._s
+
+    def close(self) -> None:
+        """Releases the device state now (the reference frees it in its destructor)."""
+        self._s.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def initializeU(self) -> None:
         """Override: fill self.U.  The default uploads self.U as it is."""
