@@ -155,10 +155,15 @@ int rmhd2d_calculate_dt(rmhd2d_solver *s, double *dt);
 
 /* Replaces ResistiveMHD2D::oneStepRK2() (TP resistiveMHD_2D.cu:133-195,
    TS resistiveMHD_2D.cu:133-195): one Heun RK2 step with constrained
-   transport.  Enqueued asynchronously. */
+   transport.  Enqueued asynchronously, as one launch of a CUDA graph of the
+   step captured on first use; while the caller is capturing the solver's
+   stream, the step's kernels are enqueued into that capture instead.
+   Graphs are captured again after rmhd2d_set_tile_shape and
+   rmhd2d_set_eta_table. */
 int rmhd2d_step_rk2(rmhd2d_solver *s);
 
-/* nsteps calls of rmhd2d_step_rk2, replayed from a captured CUDA graph. */
+/* nsteps calls of rmhd2d_step_rk2, replayed from a captured CUDA graph of
+   two steps. */
 int rmhd2d_run(rmhd2d_solver *s, int nsteps);
 
 /* Measurement hooks (the reference has no timers).
