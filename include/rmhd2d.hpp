@@ -58,6 +58,8 @@ public:
     void initialize()
     {
         initializeU();
+        if (hU_.size() != (size_t)cfg_.nx * cfg_.ny * 8)
+            throw Error(RMHD2D_ERR_INVALID, "hostU() must hold nx*ny*8 doubles");
         check(rmhd2d_set_state(s_, hU_.data(), 1), s_);
     }
 
@@ -99,7 +101,13 @@ public:
         check(rmhd2d_get_state(s_, u.data()), s_);
         return u;
     }
-    void setEtaTable(const std::vector<double> &eta) { check(rmhd2d_set_eta_table(s_, eta.data()), s_); }
+    // eta at the nx*ny cell centres (k = j + i*ny); an empty vector returns to the uniform cfg.eta.
+    void setEtaTable(const std::vector<double> &eta)
+    {
+        if (!eta.empty() && eta.size() != (size_t)cfg_.nx * cfg_.ny)
+            throw Error(RMHD2D_ERR_INVALID, "the eta table must hold nx*ny doubles");
+        check(rmhd2d_set_eta_table(s_, eta.empty() ? nullptr : eta.data()), s_);
+    }
     void applyBoundary() { check(rmhd2d_apply_boundary(s_), s_); }
 
     std::vector<double> &hostU() { return hU_; }
