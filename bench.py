@@ -96,6 +96,8 @@ def hbm_peak():
 
 
 B200_FP64_TFLOPS_NOMINAL_PIPE = 148 * 64 * 2 * 1.965e9 / 1e12   # SMs x FP64 FMA lanes x 2 x max clock
+# sizeof(rmhd2d::Control): the control block each synchronising query (crash flag, dt) reads back
+CONTROL_BLOCK_BYTES = 64
 
 
 def flops_from_profile(label: str):
@@ -297,10 +299,9 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
         if dist:
             dist.all_reduce(el, op=dist.ReduceOp.MAX)
         state_bytes = setup.state.nbytes
-        ctl_bytes = 48  # control block read back by each synchronising query
         e2e = {"value": world * cells * args.steps / float(el.item()), "unit": METRIC,
                "h2d_bytes_per_step": state_bytes / args.steps,
-               "d2h_bytes_per_step": state_bytes / args.steps + 2 * ctl_bytes,
+               "d2h_bytes_per_step": state_bytes / args.steps + 2 * CONTROL_BLOCK_BYTES,
                "note": "set_state(pinned) + K x (step_rk2 + check_crashed + get_dt) + get_state(pinned), wall clock"}
         e2e_sol.close()
 

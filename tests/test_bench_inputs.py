@@ -1,7 +1,8 @@
 """CPU checks of what bench.py reads besides the GPU: the committed profile
 summaries it takes the DRAM traffic and the flop count from, its misfit
-difference, and the synthetic set-ups every benchmark and parity run starts
-from (divergence-free to round-off, positive density and pressure)."""
+difference, the control-block size its e2e byte count uses, and the
+synthetic set-ups every benchmark and parity run starts from
+(divergence-free to round-off, positive density and pressure)."""
 import sys
 from pathlib import Path
 
@@ -79,3 +80,20 @@ def test_setups_are_divergence_free_and_positive(make):
     assert _pressure(s).min() > 0
     if s.eta_table is not None:
         assert s.eta_table.min() >= 0 and s.eta >= s.eta_table.max()
+
+
+def test_control_block_size_matches_the_library(tmp_path):
+    """The e2e line counts the control block each synchronising query reads
+    back; that count is sizeof(rmhd2d::Control) of the library's own header."""
+    import subprocess
+
+    import bench
+
+    src = tmp_path / "size.cpp"
+    src.write_text('#include <cstdio>\n#include "rmhd2d_internal.h"\n'
+                   'int main() { std::printf("%zu\\n", sizeof(rmhd2d::Control)); return 0; }\n')
+    exe = tmp_path / "size"
+    subprocess.run(["g++", "-std=c++17", str(src), "-I", str(ROOT / "resistivemhd_gpu_b200" / "csrc"), "-o", str(exe)],
+                   check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    assert int(out) == bench.CONTROL_BLOCK_BYTES
