@@ -133,6 +133,8 @@ class OracleLib:
         self.lib.orc_boundary.argtypes = [P, D]
         self.lib.orc_run.argtypes = [P, D, ctypes.c_int, D]
         self.lib.orc_run.restype = ctypes.c_int
+        self.lib.orc_run_keep_stages.argtypes = [P, D, ctypes.c_int, D, D, D]
+        self.lib.orc_run_keep_stages.restype = ctypes.c_int
 
     @staticmethod
     def _params(setup, eta_keep):
@@ -173,6 +175,29 @@ class OracleLib:
             raise MemoryError("oracle work allocation failed")
         crashed_at = rc - 1 if rc > 0 else -1
         return s, dts[:nsteps], crashed_at
+
+
+    def run_keep_stages(self, setup, state: np.ndarray, nsteps: int, apply_boundary: bool = True):
+        """As run, plus the trajectory a discrete adjoint reverses: (final_state,
+        dts, crashed_at, Un, Ustar), Un[s] the state step s starts from and
+        Ustar[s] its stage-1 state after the boundary pass."""
+        keep = []
+        p = self._params(setup, keep)
+        s = np.ascontiguousarray(state, dtype=np.float64).copy()
+        D = ctypes.POINTER(ctypes.c_double)
+        dp = s.ctypes.data_as(D)
+        if apply_boundary:
+            self.lib.orc_boundary(ctypes.byref(p), dp)
+        n = max(nsteps, 1)
+        dts = np.zeros(n, dtype=np.float64)
+        un = np.zeros((n,) + s.shape, dtype=np.float64)
+        us = np.zeros((n,) + s.shape, dtype=np.float64)
+        rc = self.lib.orc_run_keep_stages(ctypes.byref(p), dp, nsteps, dts.ctypes.data_as(D), un.ctypes.data_as(D),
+                                          us.ctypes.data_as(D))
+        if rc < 0:
+            raise MemoryError("oracle work allocation failed")
+        crashed_at = rc - 1 if rc > 0 else -1
+        return s, dts[:nsteps], crashed_at, un[:nsteps], us[:nsteps]
 
 
 def reference_binary(kind: str, bc: str) -> Path:

@@ -679,8 +679,10 @@ size_t orc_work_doubles(int nx, int ny)
 }
 
 /* resistiveMHD_2D.cu:133-195 oneStepRK2.  U is updated in place; work must
-   hold orc_work_doubles(nx, ny) doubles.  Returns the dt used. */
-double orc_step(const orc_params *p, double *U, double *work)
+   hold orc_work_doubles(nx, ny) doubles.  Ustar (may be NULL) receives the
+   stage-1 state after its boundary pass, the state stage 2 reads.  Returns
+   the dt used. */
+static double step_impl(const orc_params *p, double *U, double *work, double *Ustar)
 {
     const int nx = p->nx, ny = p->ny, N = nx * ny;
     double *UBar = work;
@@ -720,6 +722,7 @@ double orc_step(const orc_params *p, double *U, double *work)
     corner_ez(p, F, G, Ez);
     ct_update(p, bXOld, bYOld, Ez, dt, UBar);
     orc_boundary(p, UBar);
+    if (Ustar) memcpy(Ustar, UBar, (size_t)N * NV * sizeof(double));
 
     shift_to_center(p, UBar, tmp);
     flux_x(p, UBar, F, dQ, dQL, dQR);
@@ -744,6 +747,11 @@ double orc_step(const orc_params *p, double *U, double *work)
     ct_update(p, bXOld, bYOld, Ez, dt, U);
     orc_boundary(p, U);
     return dt;
+}
+
+double orc_step(const orc_params *p, double *U, double *work)
+{
+    return step_impl(p, U, work, NULL);
 }
 
 /* CT-Contact inputs of one stage, per cell (ResistiveMHD_multiGPU_cuda/
@@ -893,6 +901,26 @@ double orc_step_contact(const orc_params *p, double *U, double *work)
 /* Runs nsteps steps; dts (may be NULL) receives each step's dt.  Returns 0,
    or 1 + the step index at which the crash check (NaN energy) fired, after
    which no further step is taken, as the reference drivers do. */
+/* nsteps stage-1-EMF steps as orc_run takes them, keeping the trajectory a
+   discrete adjoint of the steps reverses: Un + s*nx*ny*8 receives the state
+   step s starts from and Ustar + s*nx*ny*8 its stage-1 state after the
+   boundary pass.  dts receives each step's dt.  Returns as orc_run. */
+int orc_run_keep_stages(const orc_params *p, double *U, int nsteps, double *dts, double *Un, double *Ustar)
+{
+    const size_t sd = (size_t)p->nx * p->ny * NV;
+    size_t nw = orc_work_doubles(p->nx, p->ny);
+    double *work = (double *)malloc(nw * sizeof(double));
+    if (!work) return -1;
+    int rc = 0;
+    for (int s = 0; s < nsteps; ++s) {
+        memcpy(Un + (size_t)s * sd, U, sd * sizeof(double));
+        dts[s] = step_impl(p, U, work, Ustar + (size_t)s * sd);
+        if (orc_is_crashed(p, U)) { rc = 1 + s; break; }
+    }
+    free(work);
+    return rc;
+}
+
 int orc_run(const orc_params *p, double *U, int nsteps, double *dts)
 {
     size_t nw = orc_work_doubles(p->nx, p->ny);

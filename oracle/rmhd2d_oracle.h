@@ -35,6 +35,7 @@ size_t orc_work_doubles(int nx, int ny);
 double orc_step(const orc_params *p, double *U, double *work);
 double orc_step_contact(const orc_params *p, double *U, double *work);
 int orc_run(const orc_params *p, double *U, int nsteps, double *dts);
+int orc_run_keep_stages(const orc_params *p, double *U, int nsteps, double *dts, double *Un, double *Ustar);
 
 #ifdef __cplusplus
 }

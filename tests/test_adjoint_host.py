@@ -1,0 +1,192 @@
+"""The discrete adjoint's kernels on the CPU: adjoint.cu and adjoint_prep.cu
+compiled for the host (tests/cuda_host_shim.h, each kernel launch rewritten
+into a loop over its blocks and threads) and driven by the reverse loop of
+rmhd2d_adjoint_backward (tests/adjoint_host.cpp) over the oracle's forward
+trajectory.  The gradient is checked against the oracle's dual-number
+tangent as the GPU tests check the CUDA run (tests/test_gpu_adjoint.py), so
+changes to the adjoint's arithmetic, transposes and stage wiring are caught
+without a GPU."""
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE.parent / "resistivemhd_gpu_b200" / "csrc"
+ADJ_REL = 1e-10
+
+
+def _split_top_level(s: str) -> list[str]:
+    parts, depth, cur = [], 0, []
+    for ch in s:
+        if ch in "([{":
+            depth += 1
+        elif ch in ")]}":
+            depth -= 1
+        if ch == "," and depth == 0:
+            parts.append("".join(cur).strip())
+            cur = []
+        else:
+            cur.append(ch)
+    parts.append("".join(cur).strip())
+    return parts
+
+
+def rewrite_launches(src: str) -> str:
+    """`kernel<T><<<grid, block, smem, stream>>>(args)` -> host_launch(grid,
+    block, [&]() { kernel<T>(args); })."""
+    out, pos = [], 0
+    while True:
+        k = src.find("<<<", pos)
+        if k < 0:
+            break
+        e = src.find(">>>", k)
+        j, depth = k, 0                      # the kernel expression before <<<
+        while j > 0:
+            ch = src[j - 1]
+            if ch == ">":
+                depth += 1
+            elif ch == "<":
+                if depth == 0:
+                    break
+                depth -= 1
+            elif depth == 0 and not (ch.isalnum() or ch in "_:"):
+                break
+            j -= 1
+        kernel = src[j:k]
+        assert src[e + 3] == "(", src[k:e + 10]
+        m, d = e + 3, 0                      # the call's argument list
+        while True:
+            if src[m] == "(":
+                d += 1
+            elif src[m] == ")":
+                d -= 1
+                if d == 0:
+                    break
+            m += 1
+        cfg = _split_top_level(src[k + 3:e])
+        out.append(src[pos:j])
+        out.append(f"host_launch({cfg[0]}, {cfg[1]}, [&]() {{ {kernel}({src[e + 4:m]}); }})")
+        pos = m + 1
+    out.append(src[pos:])
+    return "".join(out)
+
+
+@pytest.fixture(scope="module")
+def host_adjoint(tmp_path_factory):
+    d = tmp_path_factory.mktemp("adjhost")
+    (d / "cuda_runtime.h").write_text(f'#include "{HERE / "cuda_host_shim.h"}"\n')
+    srcs = []
+    for name in ("adjoint.cu", "adjoint_prep.cu"):
+        text = rewrite_launches((CSRC / name).read_text())
+        assert "<<<" not in text
+        out = d / (name + ".cpp")
+        out.write_text(f"#line 1 \"{CSRC / name}\"\n" + text)
+        srcs.append(str(out))
+    so = d / "libadjhost.so"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-Wno-unknown-pragmas", "-shared", "-fPIC",
+                    "-I", str(d), "-I", str(CSRC), *srcs, str(HERE / "adjoint_host.cpp"), "-o", str(so)],
+                   check=True, capture_output=True)
+    lib = ctypes.CDLL(str(so))
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.host_adjoint_backward.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                          ctypes.c_int, D, ctypes.c_int, D, D, D, D, D, D]
+    lib.host_adjoint_backward.restype = ctypes.c_int
+    return lib
+
+
+BC = {"periodic": 0, "symmetric": 1}
+
+
+def backward(lib, s, un, us, dts, seed):
+    D = ctypes.POINTER(ctypes.c_double)
+
+    def p(a):
+        return None if a is None else a.ctypes.data_as(D)
+
+    tab = None if s.eta_table is None else np.ascontiguousarray(s.eta_table, dtype=np.float64)
+    gs = np.zeros_like(s.state)
+    ge = np.zeros((s.nx, s.ny))
+    un, us, dts, seed = (np.ascontiguousarray(x, dtype=np.float64) for x in (un, us, dts, seed))
+    rc = lib.host_adjoint_backward(s.nx, s.ny, s.dx, s.dy, s.gamma, s.eps, s.eta, BC[s.bc],
+                                   BC[s.bc_y] if s.bc_y else -1, p(tab), len(dts), p(un), p(us), p(dts), p(seed),
+                                   p(gs), p(ge))
+    assert rc == 0
+    return gs, ge
+
+
+def _dirs(setup, seed):
+    rng = np.random.default_rng(seed)
+    d = rng.standard_normal(setup.state.shape)
+    d[..., (1, 2, 3)] *= 1e-2
+    d[..., (0, 4, 5, 6, 7)] *= 1e-3
+    deta = rng.standard_normal((setup.nx, setup.ny)) * 1e-4
+    return d, deta
+
+
+def test_launch_rewrite_keeps_template_kernels_and_nested_arguments():
+    src = ("  k1<<<dim3(f(n, 2), 2), T, 0, st>>>(a);\n"
+           "  ytrans_kernel<BC_PERIODIC><<<g(x), 128, 0, st>>>(g, h(u, v));\n")
+    out = rewrite_launches(src)
+    assert out == ("  host_launch(dim3(f(n, 2), 2), T, [&]() { k1(a); });\n"
+                   "  host_launch(g(x), 128, [&]() { ytrans_kernel<BC_PERIODIC>(g, h(u, v)); });\n")
+
+
+@pytest.mark.parametrize("with_table,shape,nsteps,bc,bc_y", [
+    (False, (20, 18), 5, "periodic", None),
+    (True, (26, 21), 6, "periodic", None),
+    (False, (20, 18), 5, "symmetric", None),
+    (True, (23, 26), 6, "symmetric", None),
+    (True, (18, 21), 4, "periodic", "symmetric"),
+    (False, (21, 17), 5, "symmetric", "periodic"),
+])
+def test_host_adjoint_matches_oracle_tangent(host_adjoint, oracle, tangent, with_table, shape, nsteps, bc, bc_y):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(*shape, seed=21, bc=bc, bc_y=bc_y, with_table=with_table)
+    _, dts, crashed, un, us = oracle.run_keep_stages(s, s.state, nsteps)
+    assert crashed == -1
+    w = np.random.default_rng(5).standard_normal(s.state.shape)
+    gs, ge = backward(host_adjoint, s, un, us, dts, w)
+    ghost = np.ones(gs.shape[:2], bool)
+    ghost[3:-3, 3:-3] = False
+    mask = np.repeat(ghost[..., None], 8, axis=2)
+    if bc == "symmetric":
+        for c in (3, 4, s.nx - 6, s.nx - 5, s.nx - 4):
+            mask[c, 2, 5] = False
+    assert np.all(gs[mask] == 0)
+    for k in range(3):
+        d, deta = _dirs(s, 100 + k)
+        _, dU = tangent.tangent(s, s.state, d, dts, deta=deta)
+        jvp = float((w * dU).sum())
+        vjp = float((gs * d).sum()) + float((ge * deta).sum())
+        assert vjp == pytest.approx(jvp, rel=ADJ_REL, abs=1e-14)
+
+
+def test_host_adjoint_unit_directions(host_adjoint, oracle, tangent):
+    """Single components of dJ/dU_0 and dJ/d eta on a 12 x 12 interior with
+    an eta table, against the tangent along unit directions."""
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(12, 12, seed=8, bc="periodic", with_table=True)
+    _, dts, crashed, un, us = oracle.run_keep_stages(s, s.state, 3)
+    assert crashed == -1
+    w = np.random.default_rng(9).standard_normal(s.state.shape)
+    gs, ge = backward(host_adjoint, s, un, us, dts, w)
+    rng = np.random.default_rng(10)
+    cells = [(i, j) for i in range(3, s.nx - 3) for j in range(3, s.ny - 3)]
+    for t in rng.choice(len(cells), 6, replace=False):
+        i, j = cells[t]
+        for f in range(8):
+            d = np.zeros_like(s.state)
+            d[i, j, f] = 1.0
+            _, dU = tangent.tangent(s, s.state, d, dts)
+            assert gs[i, j, f] == pytest.approx(float((w * dU).sum()), rel=1e-9, abs=1e-12), (i, j, f)
+        de = np.zeros((s.nx, s.ny))
+        de[i, j] = 1.0
+        _, dU = tangent.tangent(s, s.state, np.zeros_like(s.state), dts, deta=de)
+        assert ge[i, j] == pytest.approx(float((w * dU).sum()), rel=1e-9, abs=1e-12), (i, j)
