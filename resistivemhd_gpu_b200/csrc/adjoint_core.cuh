@@ -25,8 +25,10 @@
 #define ADJ_FN inline
 #endif
 
-// Correctly rounded single operations, kept out of any contraction.
-#if defined(__CUDA_ARCH__)
+// Correctly rounded single operations, kept out of any contraction.  A host
+// build that models the device's rounding (contracting everything else)
+// defines RMHD_ADJ_HOST_RN and supplies __dadd_rn and the others.
+#if defined(__CUDA_ARCH__) || defined(RMHD_ADJ_HOST_RN)
 #define XADD(a, b) __dadd_rn((a), (b))
 #define XSUB(a, b) __dsub_rn((a), (b))
 #define XMUL(a, b) __dmul_rn((a), (b))
@@ -325,8 +327,12 @@ ADJ_FN void hlld_flux_adj(const double *L, const double *R, double gm, double EP
     l.idS = adj_rcp(dSL);
     r.idS = adj_rcp(dSR);
     auto star = [&](Side &x) {
-        x.iD = adj_rcp(x.rho * x.a * (x.S - SM) - x.bX * x.bX + EPS);
-        x.N = x.rho * x.a * x.a - x.bX * x.bX;
+        // D and N in the forward's rounding: where the fast and Alfven waves
+        // meet, both are differences of nearly equal terms, and the ratios
+        // N / D and (SM - u) / D linearised at contracted values differ
+        // from the forward's at the 1e-6 level.
+        x.iD = adj_rcp(XADD(XSUB(XMUL(XMUL(x.rho, x.a), XSUB(x.S, SM)), XMUL(x.bX, x.bX)), EPS));
+        x.N = XSUB(XMUL(XMUL(x.rho, x.a), x.a), XMUL(x.bX, x.bX));
         const double q = (SM - x.u) * x.iD;
         x.v1 = x.v - x.bX * x.bY * q;
         x.w1 = x.w - x.bX * x.bZ * q;

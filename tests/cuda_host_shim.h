@@ -8,9 +8,9 @@
 // launch's blocks and threads (host_launch; the test rewrites each
 // `k<<<grid, block, smem, stream>>>(args)` into a host_launch call).  The
 // correctly rounded device operations map to the host's IEEE binary64
-// operations (built with -ffp-contract=off); the reverse sweep's reciprocals
-// are host divisions (adjoint_core.cuh: adj_rcp), so results agree with the
-// GPU's to rounding.
+// operations; the reverse sweep's reciprocals are host divisions
+// (adjoint_core.cuh: adj_rcp), so results agree with the GPU's to
+// rounding.
 #pragma once
 
 #include <cmath>
@@ -48,11 +48,21 @@ template <class F> void host_launch(dim3 grid, dim3 block, F &&kernel_call)
                         }
 }
 
-inline double __dadd_rn(double a, double b) { return a + b; }
-inline double __dsub_rn(double a, double b) { return a - b; }
-inline double __dmul_rn(double a, double b) { return a * b; }
-inline double __ddiv_rn(double a, double b) { return a / b; }
-inline double __dsqrt_rn(double a) { return std::sqrt(a); }
+// The device's __dadd_rn and the others are single correctly rounded
+// operations that are never fused with a neighbouring one.  The empty asm
+// statements make their operands and results opaque to the host compiler,
+// so that holds here too when the rest of a file is built with contraction
+// (-ffp-contract=fast), the way nvcc builds the adjoint kernels.
+#if defined(__x86_64__)
+#define RN_OPAQUE(v) asm("" : "+x"(v))
+#else
+#define RN_OPAQUE(v) ((void)0)
+#endif
+inline double __dadd_rn(double a, double b) { RN_OPAQUE(a); RN_OPAQUE(b); double r = a + b; RN_OPAQUE(r); return r; }
+inline double __dsub_rn(double a, double b) { RN_OPAQUE(a); RN_OPAQUE(b); double r = a - b; RN_OPAQUE(r); return r; }
+inline double __dmul_rn(double a, double b) { RN_OPAQUE(a); RN_OPAQUE(b); double r = a * b; RN_OPAQUE(r); return r; }
+inline double __ddiv_rn(double a, double b) { RN_OPAQUE(a); RN_OPAQUE(b); double r = a / b; RN_OPAQUE(r); return r; }
+inline double __dsqrt_rn(double a) { RN_OPAQUE(a); double r = std::sqrt(a); RN_OPAQUE(r); return r; }
 
 inline long long __double_as_longlong(double x)
 {

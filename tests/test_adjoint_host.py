@@ -75,21 +75,29 @@ def rewrite_launches(src: str) -> str:
     return "".join(out)
 
 
-@pytest.fixture(scope="module")
-def host_adjoint(tmp_path_factory):
-    d = tmp_path_factory.mktemp("adjhost")
+def _build(d: Path, contracted: bool):
+    """The adjoint kernels and the reverse loop as a host library.  With
+    `contracted`, adjoint.cu is built the way nvcc builds it for the device
+    (fused multiply-add wherever the compiler finds one; the explicitly
+    rounded operations kept apart, RMHD_ADJ_HOST_RN) and adjoint_prep.cu
+    without contraction (-fmad=false on the device)."""
     (d / "cuda_runtime.h").write_text(f'#include "{HERE / "cuda_host_shim.h"}"\n')
-    srcs = []
+    objs = []
     for name in ("adjoint.cu", "adjoint_prep.cu"):
         text = rewrite_launches((CSRC / name).read_text())
         assert "<<<" not in text
-        out = d / (name + ".cpp")
-        out.write_text(f"#line 1 \"{CSRC / name}\"\n" + text)
-        srcs.append(str(out))
+        src = d / (name + ".cpp")
+        src.write_text(f"#line 1 \"{CSRC / name}\"\n" + text)
+        fl = ["-ffp-contract=fast", "-mfma", "-DRMHD_ADJ_HOST_RN"] if contracted and name == "adjoint.cu" \
+            else ["-ffp-contract=off"]
+        obj = d / (name + ".o")
+        subprocess.run(["g++", "-std=c++17", "-O2", *fl, "-Wno-unknown-pragmas", "-fPIC", "-c", "-I", str(d),
+                        "-I", str(CSRC), str(src), "-o", str(obj)], check=True, capture_output=True)
+        objs.append(str(obj))
     so = d / "libadjhost.so"
-    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-Wno-unknown-pragmas", "-shared", "-fPIC",
-                    "-I", str(d), "-I", str(CSRC), *srcs, str(HERE / "adjoint_host.cpp"), "-o", str(so)],
-                   check=True, capture_output=True)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I", str(d), "-I", str(CSRC),
+                    *objs,
+                    str(HERE / "adjoint_host.cpp"), "-o", str(so)], check=True, capture_output=True)
     lib = ctypes.CDLL(str(so))
     D = ctypes.POINTER(ctypes.c_double)
     lib.host_adjoint_backward.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
@@ -97,6 +105,25 @@ def host_adjoint(tmp_path_factory):
                                           ctypes.c_int, D, ctypes.c_int, D, D, D, D, D, D]
     lib.host_adjoint_backward.restype = ctypes.c_int
     return lib
+
+
+@pytest.fixture(scope="module")
+def host_adjoint(tmp_path_factory):
+    return _build(tmp_path_factory.mktemp("adjhost"), contracted=False)
+
+
+def _has_fma() -> bool:
+    try:
+        return " fma " in open("/proc/cpuinfo").read().replace("\n", " ")
+    except OSError:
+        return False
+
+
+@pytest.fixture(scope="module")
+def host_adjoint_contracted(tmp_path_factory):
+    if not _has_fma():
+        pytest.skip("the host has no fused multiply-add to model the device build with")
+    return _build(tmp_path_factory.mktemp("adjhost_fma"), contracted=True)
 
 
 BC = {"periodic": 0, "symmetric": 1}
@@ -190,3 +217,27 @@ def test_host_adjoint_unit_directions(host_adjoint, oracle, tangent):
         de[i, j] = 1.0
         _, dU = tangent.tangent(s, s.state, np.zeros_like(s.state), dts, deta=de)
         assert ge[i, j] == pytest.approx(float((w * dU).sum()), rel=1e-9, abs=1e-12), (i, j)
+
+
+@pytest.mark.parametrize("build", ["plain", "contracted"])
+def test_host_adjoint_on_the_harris_sheet(request, oracle, tangent, build):
+    """Symmetric walls and the eta table of the Harris workload (64 x 32),
+    where the fast and Alfven waves meet and the star states' N and D are
+    differences of nearly equal terms.  The reverse recomputes them exactly
+    rounded, as the forward does, so the gradient holds the tangent's 1e-10
+    also when the rest of the reverse is contracted into fused multiply-adds
+    as on the device (built that way, with N and D contracted too, this case
+    was 6e-7 and 2e-6 off)."""
+    from resistivemhd_gpu_b200 import setups
+
+    lib = request.getfixturevalue("host_adjoint" if build == "plain" else "host_adjoint_contracted")
+    s = setups.harris_sheet(64, 32)
+    _, dts, crashed, un, us = oracle.run_keep_stages(s, s.state, 6)
+    assert crashed == -1
+    w = np.random.default_rng(3).standard_normal(s.state.shape)
+    gs, ge = backward(lib, s, un, us, dts, w)
+    for k in range(2):
+        d, deta = _dirs(s, 200 + k)
+        _, dU = tangent.tangent(s, s.state, d, dts, deta=deta)
+        vjp = float((gs * d).sum() + (ge * deta).sum())
+        assert vjp == pytest.approx(float((w * dU).sum()), rel=ADJ_REL, abs=1e-14)
