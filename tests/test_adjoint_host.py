@@ -163,6 +163,7 @@ def test_launch_rewrite_keeps_template_kernels_and_nested_arguments():
                    "  host_launch(g(x), 128, [&]() { ytrans_kernel<BC_PERIODIC>(g, h(u, v)); });\n")
 
 
+@pytest.mark.parametrize("build", ["plain", "contracted"])
 @pytest.mark.parametrize("with_table,shape,nsteps,bc,bc_y", [
     (False, (20, 18), 5, "periodic", None),
     (True, (26, 21), 6, "periodic", None),
@@ -171,14 +172,15 @@ def test_launch_rewrite_keeps_template_kernels_and_nested_arguments():
     (True, (18, 21), 4, "periodic", "symmetric"),
     (False, (21, 17), 5, "symmetric", "periodic"),
 ])
-def test_host_adjoint_matches_oracle_tangent(host_adjoint, oracle, tangent, with_table, shape, nsteps, bc, bc_y):
+def test_host_adjoint_matches_oracle_tangent(request, oracle, tangent, with_table, shape, nsteps, bc, bc_y, build):
     from resistivemhd_gpu_b200 import setups
 
+    lib = request.getfixturevalue("host_adjoint" if build == "plain" else "host_adjoint_contracted")
     s = setups.random_smooth_state(*shape, seed=21, bc=bc, bc_y=bc_y, with_table=with_table)
     _, dts, crashed, un, us = oracle.run_keep_stages(s, s.state, nsteps)
     assert crashed == -1
     w = np.random.default_rng(5).standard_normal(s.state.shape)
-    gs, ge = backward(host_adjoint, s, un, us, dts, w)
+    gs, ge = backward(lib, s, un, us, dts, w)
     ghost = np.ones(gs.shape[:2], bool)
     ghost[3:-3, 3:-3] = False
     mask = np.repeat(ghost[..., None], 8, axis=2)
