@@ -243,3 +243,42 @@ def test_host_adjoint_on_the_harris_sheet(request, oracle, tangent, build):
         _, dU = tangent.tangent(s, s.state, d, dts, deta=deta)
         vjp = float((gs * d).sum() + (ge * deta).sum())
         assert vjp == pytest.approx(float((w * dU).sum()), rel=ADJ_REL, abs=1e-14)
+
+
+def test_host_adjoint_against_central_differences(host_adjoint, oracle, tangent):
+    """The misfit gradient of the host build against central differences
+    (h = 1e-6 and 1e-7, the better one held to 1e-6) of the oracle's
+    frozen-dt forward along localized directions of momentum and eta, as
+    tests/test_gpu_adjoint.py checks the CUDA adjoint through the CUDA
+    forward."""
+    import copy
+
+    from adjoint_harness import misfit_difference, misfit_seed
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(48, 48, seed=3, bc="periodic", with_table=True)
+    eta0 = s.eta_table.copy()
+    target = s.state.copy()
+    final, dts, crashed, un, us = oracle.run_keep_stages(s, s.state, 10)
+    assert crashed == -1
+    gs, ge = backward(host_adjoint, s, un, us, dts, misfit_seed(final, target))
+
+    def final_of(state, eta):
+        s2 = copy.copy(s)
+        s2.eta_table = eta
+        return tangent.run_fixed_dt(s2, state, dts)
+
+    rng = np.random.default_rng(7)
+    for _ in range(4):
+        d = np.zeros_like(s.state)
+        de = np.zeros_like(eta0)
+        i0, j0 = rng.integers(3, s.nx - 6), rng.integers(3, s.ny - 6)
+        d[i0:i0 + 3, j0:j0 + 3, 1:3] = rng.standard_normal((3, 3, 2))
+        de[i0:i0 + 3, j0:j0 + 3] = rng.standard_normal((3, 3)) * eta0[i0:i0 + 3, j0:j0 + 3]
+        ad = float((gs * d).sum() + (ge * de).sum())
+        errs = []
+        for h in (1e-6, 1e-7):
+            fd = misfit_difference(final_of(s.state + h * d, eta0 + h * de),
+                                   final_of(s.state - h * d, eta0 - h * de), target) / (2 * h)
+            errs.append(abs(fd - ad) / abs(ad))
+        assert min(errs) <= 1e-6, (errs, ad)
