@@ -7,72 +7,15 @@ tangent as the GPU tests check the CUDA run (tests/test_gpu_adjoint.py), so
 changes to the adjoint's arithmetic, transposes and stage wiring are caught
 without a GPU."""
 import ctypes
-import re
-import subprocess
 from pathlib import Path
 
 import numpy as np
 import pytest
 
+from host_build import compile_unit, link, rewrite_launches, shim_dir
+
 HERE = Path(__file__).resolve().parent
-CSRC = HERE.parent / "resistivemhd_gpu_b200" / "csrc"
 ADJ_REL = 1e-10
-
-
-def _split_top_level(s: str) -> list[str]:
-    parts, depth, cur = [], 0, []
-    for ch in s:
-        if ch in "([{":
-            depth += 1
-        elif ch in ")]}":
-            depth -= 1
-        if ch == "," and depth == 0:
-            parts.append("".join(cur).strip())
-            cur = []
-        else:
-            cur.append(ch)
-    parts.append("".join(cur).strip())
-    return parts
-
-
-def rewrite_launches(src: str) -> str:
-    """`kernel<T><<<grid, block, smem, stream>>>(args)` -> host_launch(grid,
-    block, [&]() { kernel<T>(args); })."""
-    out, pos = [], 0
-    while True:
-        k = src.find("<<<", pos)
-        if k < 0:
-            break
-        e = src.find(">>>", k)
-        j, depth = k, 0                      # the kernel expression before <<<
-        while j > 0:
-            ch = src[j - 1]
-            if ch == ">":
-                depth += 1
-            elif ch == "<":
-                if depth == 0:
-                    break
-                depth -= 1
-            elif depth == 0 and not (ch.isalnum() or ch in "_:"):
-                break
-            j -= 1
-        kernel = src[j:k]
-        assert src[e + 3] == "(", src[k:e + 10]
-        m, d = e + 3, 0                      # the call's argument list
-        while True:
-            if src[m] == "(":
-                d += 1
-            elif src[m] == ")":
-                d -= 1
-                if d == 0:
-                    break
-            m += 1
-        cfg = _split_top_level(src[k + 3:e])
-        out.append(src[pos:j])
-        out.append(f"host_launch({cfg[0]}, {cfg[1]}, [&]() {{ {kernel}({src[e + 4:m]}); }})")
-        pos = m + 1
-    out.append(src[pos:])
-    return "".join(out)
 
 
 def _build(d: Path, contracted: bool):
@@ -81,24 +24,11 @@ def _build(d: Path, contracted: bool):
     (fused multiply-add wherever the compiler finds one; the explicitly
     rounded operations kept apart, RMHD_ADJ_HOST_RN) and adjoint_prep.cu
     without contraction (-fmad=false on the device)."""
-    (d / "cuda_runtime.h").write_text(f'#include "{HERE / "cuda_host_shim.h"}"\n')
-    objs = []
-    for name in ("adjoint.cu", "adjoint_prep.cu"):
-        text = rewrite_launches((CSRC / name).read_text())
-        assert "<<<" not in text
-        src = d / (name + ".cpp")
-        src.write_text(f"#line 1 \"{CSRC / name}\"\n" + text)
-        fl = ["-ffp-contract=fast", "-mfma", "-DRMHD_ADJ_HOST_RN"] if contracted and name == "adjoint.cu" \
-            else ["-ffp-contract=off"]
-        obj = d / (name + ".o")
-        subprocess.run(["g++", "-std=c++17", "-O2", *fl, "-Wno-unknown-pragmas", "-fPIC", "-c", "-I", str(d),
-                        "-I", str(CSRC), str(src), "-o", str(obj)], check=True, capture_output=True)
-        objs.append(str(obj))
-    so = d / "libadjhost.so"
-    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I", str(d), "-I", str(CSRC),
-                    *objs,
-                    str(HERE / "adjoint_host.cpp"), "-o", str(so)], check=True, capture_output=True)
-    lib = ctypes.CDLL(str(so))
+    shim_dir(d)
+    objs = [compile_unit(d, "adjoint.cu", ["-ffp-contract=fast", "-mfma", "-DRMHD_ADJ_HOST_RN"] if contracted
+                         else ["-ffp-contract=off"]),
+            compile_unit(d, "adjoint_prep.cu", ["-ffp-contract=off"])]
+    lib = link(d, objs, [HERE / "adjoint_host.cpp"], "libadjhost.so")
     D = ctypes.POINTER(ctypes.c_double)
     lib.host_adjoint_backward.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
