@@ -76,6 +76,9 @@ def rewrite_launches(src: str, threaded: tuple[str, ...] = ()) -> str:
     return "".join(out)
 
 
+SANITIZE = ["-fsanitize=address,undefined", "-fno-omit-frame-pointer", "-fno-sanitize-recover=all"]
+
+
 def compile_unit(d: Path, name: str, flags: list[str], threaded: tuple[str, ...] = ()) -> str:
     """Rewrites csrc/<name> into d and compiles it to an object; returns its path."""
     text = rewrite_launches((CSRC / name).read_text(), threaded)
@@ -94,9 +97,9 @@ def shim_dir(d: Path) -> Path:
     return d
 
 
-def link(d: Path, objs: list[str], sources: list[Path], name: str) -> ctypes.CDLL:
+def link(d: Path, objs: list[str], sources: list[Path], name: str, flags: tuple[str, ...] = ()) -> ctypes.CDLL:
     so = d / name
-    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-I", str(d), "-I", str(CSRC),
-                    "-I", str(ORACLE), *objs, *[str(s) for s in sources], "-o", str(so), "-lpthread"],
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", *flags, "-shared", "-fPIC", "-I", str(d),
+                    "-I", str(CSRC), "-I", str(ORACLE), *objs, *[str(s) for s in sources], "-o", str(so), "-lpthread"],
                    check=True, capture_output=True)
     return ctypes.CDLL(str(so))

@@ -1,0 +1,52 @@
+"""TEST INFRASTRUCTURE, run by tests/test_host_memory_safety.py in a child
+process with the address sanitizer's runtime preloaded: the host builds of
+the adjoint kernels (adjoint.cu, adjoint_prep.cu) and of the CT-Contact
+kernels (contact.cu) compiled with -fsanitize=address,undefined and run on
+small ragged grids of every wall pairing they support.  Any read or write
+outside an allocation, and any undefined behaviour, aborts the child: the
+kernels' index arithmetic is checked against their buffers on the CPU.
+Prints "ok" at the end."""
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+sys.path.insert(0, str(HERE.parent))
+
+from host_build import SANITIZE  # noqa: E402
+
+
+def main() -> None:
+    import test_adjoint_host as A
+    import test_contact_host as C
+    from oracle.oracle import OracleLib
+    from resistivemhd_gpu_b200 import setups
+
+    oracle = OracleLib()
+    tmp = Path(tempfile.mkdtemp())
+    (tmp / "adj").mkdir()
+    adj = A._build(tmp / "adj", contracted=False, extra=tuple(SANITIZE))
+    for shape, bc, bc_y, table in [((13, 11), "periodic", None, True), ((12, 15), "symmetric", None, False),
+                                   ((14, 12), "periodic", "symmetric", True), ((11, 13), "symmetric", "periodic", False)]:
+        s = setups.random_smooth_state(*shape, seed=3, bc=bc, bc_y=bc_y, with_table=table)
+        _, dts, crashed, un, us = oracle.run_keep_stages(s, s.state, 2)
+        assert crashed == -1
+        gs, ge = A.backward(adj, s, un, us, dts, np.random.default_rng(1).standard_normal(s.state.shape))
+        assert np.isfinite(gs).all() and np.isfinite(ge).all()
+    (tmp / "ct").mkdir()
+    ct = C.build_contact(tmp / "ct", tuple(SANITIZE))
+    for shape, bc, bc_y, table in [((13, 11), "periodic", None, True), ((12, 15), "symmetric", None, False),
+                                   ((14, 12), "flare", "wall", True), ((11, 13), "zero_gradient", "periodic", False)]:
+        s = setups.random_smooth_state(*shape, seed=3, bc=bc, bc_y=bc_y, with_table=table)
+        s.ct = "contact"
+        want, want_dts, _ = oracle.run(s, s.state, 2)
+        got, got_dts, _ = C.run_host(ct, s, 2)
+        assert np.array_equal(got, want, equal_nan=True) and np.array_equal(got_dts, want_dts)
+    print("ok", flush=True)
+
+
+if __name__ == "__main__":
+    main()

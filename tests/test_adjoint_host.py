@@ -18,17 +18,17 @@ HERE = Path(__file__).resolve().parent
 ADJ_REL = 1e-10
 
 
-def _build(d: Path, contracted: bool):
+def _build(d: Path, contracted: bool, extra: tuple[str, ...] = ()):
     """The adjoint kernels and the reverse loop as a host library.  With
     `contracted`, adjoint.cu is built the way nvcc builds it for the device
     (fused multiply-add wherever the compiler finds one; the explicitly
     rounded operations kept apart, RMHD_ADJ_HOST_RN) and adjoint_prep.cu
     without contraction (-fmad=false on the device)."""
     shim_dir(d)
-    objs = [compile_unit(d, "adjoint.cu", ["-ffp-contract=fast", "-mfma", "-DRMHD_ADJ_HOST_RN"] if contracted
-                         else ["-ffp-contract=off"]),
-            compile_unit(d, "adjoint_prep.cu", ["-ffp-contract=off"])]
-    lib = link(d, objs, [HERE / "adjoint_host.cpp"], "libadjhost.so")
+    objs = [compile_unit(d, "adjoint.cu", [*(["-ffp-contract=fast", "-mfma", "-DRMHD_ADJ_HOST_RN"] if contracted
+                                            else ["-ffp-contract=off"]), *extra]),
+            compile_unit(d, "adjoint_prep.cu", ["-ffp-contract=off", *extra])]
+    lib = link(d, objs, [HERE / "adjoint_host.cpp"], "libadjhost.so", extra)
     D = ctypes.POINTER(ctypes.c_double)
     lib.host_adjoint_backward.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,

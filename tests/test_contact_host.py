@@ -18,21 +18,27 @@ HERE = Path(__file__).resolve().parent
 BC = {"periodic": 0, "symmetric": 1, "zero_gradient": 2, "wall": 3, "flare": 4}
 
 
-@pytest.fixture(scope="module")
-def host_contact(tmp_path_factory):
-    d = shim_dir(tmp_path_factory.mktemp("contacthost"))
-    objs = [compile_unit(d, "contact.cu", ["-ffp-contract=off"], threaded=("contact_flux_tiled_kernel",))]
+def build_contact(d: Path, extra: tuple[str, ...] = ()):
+    """contact.cu, the oracle and the step driver as a host library; `extra`
+    adds compiler flags to every unit (e.g. sanitizers)."""
+    shim_dir(d)
+    objs = [compile_unit(d, "contact.cu", ["-ffp-contract=off", *extra], threaded=("contact_flux_tiled_kernel",))]
     orc = d / "oracle.o"
-    subprocess.run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fPIC", "-c", str(ORACLE / "rmhd2d_oracle.c"),
-                    "-o", str(orc)], check=True, capture_output=True)
+    subprocess.run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", *extra, "-fPIC", "-c",
+                    str(ORACLE / "rmhd2d_oracle.c"), "-o", str(orc)], check=True, capture_output=True)
     objs.append(str(orc))
-    lib = link(d, objs, [HERE / "contact_host.cpp"], "libcontacthost.so")
+    lib = link(d, objs, [HERE / "contact_host.cpp"], "libcontacthost.so", extra)
     D = ctypes.POINTER(ctypes.c_double)
     lib.host_contact_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, D,
                                      D, ctypes.c_int, D]
     lib.host_contact_run.restype = ctypes.c_int
     return lib
+
+
+@pytest.fixture(scope="module")
+def host_contact(tmp_path_factory):
+    return build_contact(tmp_path_factory.mktemp("contacthost"))
 
 
 def run_host(lib, s, nsteps):
