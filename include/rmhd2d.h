@@ -247,7 +247,11 @@ const char *rmhd2d_batch_last_error(const rmhd2d_batch *b);
    rmhd2d_adjoint_forward: nsteps steps from the current state (as
    rmhd2d_run), recording each step's dt and keeping the state every
    checkpoint_interval steps (0: ceil(sqrt(nsteps))).  Memory: about
-   (nsteps / interval + 2 * interval + 6) states of nx*ny*8 doubles.
+   (nsteps / interval + 2 * interval + 6) states of nx*ny*8 doubles.  A
+   negative checkpoint_interval keeps the whole trajectory instead, U^n and
+   the stage-1 state of every step (about 2 * nsteps + 7 states), and
+   rmhd2d_adjoint_backward then recomputes no step; the gradient is the same
+   bit for bit.
 
    rmhd2d_adjoint_dts: the nsteps dts recorded by the last forward run.
 
@@ -260,9 +264,9 @@ const char *rmhd2d_batch_last_error(const rmhd2d_batch *b);
    it), and, when grad_eta is not NULL,
    dJ/d eta into grad_eta (nx*ny, k = j + i*ny; the cell-centred eta field,
    the table when one is set, else the uniform eta spread over the cells).
-   Each segment between checkpoints is recomputed once; the solver's state
-   is restored to U_N afterwards, so backward may be called again with
-   another seed.
+   Each segment between checkpoints is recomputed once (not at all for a
+   kept trajectory); the solver's state is restored to U_N afterwards, so
+   backward may be called again with another seed.
 
    rmhd2d_adjoint_release: frees the recorded trajectory and workspace. */
 int rmhd2d_run_fixed_dt(rmhd2d_solver *s, int nsteps, const double *host_dts);

@@ -67,6 +67,7 @@ struct rmhd2d_solver {
 struct AdjointWork {
     int nsteps = 0, interval = 0, nseg = 0;
     int cap_steps = 0, cap_interval = 0, cap_seg = 0;   // sizes the buffers were allocated for
+    bool tape = false;               // the forward run filled the segment slots with every step (no recompute)
     size_t state_doubles = 0;
     double *ckpt = nullptr;          // nseg states: U at steps 0, interval, 2*interval, ...
     double *seg0 = nullptr;          // interval states: U^n of each step of a segment (recomputed)
@@ -1324,7 +1325,10 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
         return fail(s, RMHD2D_ERR_INVALID, "the discrete adjoint is implemented for periodic and symmetric walls");
     if (s->contact) return fail(s, RMHD2D_ERR_INVALID, "the discrete adjoint differentiates the stage-1-EMF step");
     CK(cudaSetDevice(s->device));
-    int interval = checkpoint_interval;
+    // checkpoint_interval < 0: one segment holding every step's U^n and U*,
+    // written by the forward run itself, so backward recomputes nothing
+    const bool tape = checkpoint_interval < 0;
+    int interval = tape ? nsteps : checkpoint_interval;
     if (interval <= 0) interval = (int)std::ceil(std::sqrt((double)nsteps));
     if (interval > nsteps) interval = nsteps;
     const int nseg = (nsteps + interval - 1) / interval;
@@ -1375,14 +1379,35 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
     w->nsteps = nsteps;
     w->interval = interval;
     w->nseg = nseg;
-    for (int n = 0; n < nsteps; ++n) {
-        if (n % interval == 0)
-            CK(cudaMemcpyAsync(w->ckpt + (size_t)(n / interval) * sd, s->A, sd * sizeof(double),
-                               cudaMemcpyDeviceToDevice, s->stream));
-        enqueue_step(s, s->parity);
-        s->parity ^= 1;
-        s->steps += 1;
-        CK(cudaMemcpyAsync(w->dts + n, &s->ctl->dt, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+    w->tape = tape;
+    if (tape) {
+        // every step reads U^n from and writes U* and U^{n+1} into the
+        // segment slots, through each slot's own tensor maps
+        w->map0.resize(nsteps);
+        w->map1.resize(nsteps);
+        for (int k = 0; k < nsteps; ++k)
+            if (!encode_state_map(&w->map0[k], g, w->seg0 + (size_t)k * sd, stage_ui(1, s->shape), shape_uj(s->shape)) ||
+                !encode_state_map(&w->map1[k], g, w->seg1 + (size_t)k * sd, stage_ui(2, s->shape), shape_uj(s->shape)))
+                return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint's trajectory slots");
+        CK(cudaMemcpyAsync(w->seg0, s->A, sd * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        for (int n = 0; n < nsteps; ++n) {
+            const size_t o = (size_t)n * sd;
+            double *next = n + 1 < nsteps ? w->seg0 + o + sd : s->A;
+            enqueue_step_between(s, s->parity, w->seg0 + o, &w->map0[n], w->seg1 + o, &w->map1[n], next);
+            s->parity ^= 1;
+            s->steps += 1;
+            CK(cudaMemcpyAsync(w->dts + n, &s->ctl->dt, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        }
+    } else {
+        for (int n = 0; n < nsteps; ++n) {
+            if (n % interval == 0)
+                CK(cudaMemcpyAsync(w->ckpt + (size_t)(n / interval) * sd, s->A, sd * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, s->stream));
+            enqueue_step(s, s->parity);
+            s->parity ^= 1;
+            s->steps += 1;
+            CK(cudaMemcpyAsync(w->dts + n, &s->ctl->dt, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        }
     }
     CK(cudaMemcpyAsync(w->final_state, s->A, sd * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
     CK(cudaGetLastError());
@@ -1418,13 +1443,16 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
     CK(cudaMemcpyAsync(w->aos, host_seed, naos * sizeof(double), cudaMemcpyHostToDevice, st));
     launch_aos_to_planes(g, w->aos, w->ub[0], st);
     CK(cudaMemsetAsync(w->etab, 0, (size_t)g.plane * sizeof(double), st));
-    // tensor maps of the segment slots for the solver's tile shape
-    w->map0.resize(w->interval);
-    w->map1.resize(w->interval);
-    for (int k = 0; k < w->interval; ++k)
-        if (!encode_state_map(&w->map0[k], g, w->seg0 + (size_t)k * sd, stage_ui(1, s->shape), shape_uj(s->shape)) ||
-            !encode_state_map(&w->map1[k], g, w->seg1 + (size_t)k * sd, stage_ui(2, s->shape), shape_uj(s->shape)))
-            return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint's segment states");
+    // tensor maps of the segment slots for the solver's tile shape (a kept
+    // trajectory is read as it is: nothing is recomputed)
+    if (!w->tape) {
+        w->map0.resize(w->interval);
+        w->map1.resize(w->interval);
+        for (int k = 0; k < w->interval; ++k)
+            if (!encode_state_map(&w->map0[k], g, w->seg0 + (size_t)k * sd, stage_ui(1, s->shape), shape_uj(s->shape)) ||
+                !encode_state_map(&w->map1[k], g, w->seg1 + (size_t)k * sd, stage_ui(2, s->shape), shape_uj(s->shape)))
+                return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint's segment states");
+    }
     int rc = set_fixed_dt_mode(s, 1);
     if (rc) return rc;
     FixedDtScope fixed{s, true};
@@ -1435,13 +1463,16 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
         // recompute the segment from its checkpoint with the recorded dts,
         // each step reading U^n from and writing U* and U^{n+1} into the
         // segment's slots (the last U^{n+1} is not needed: A takes it)
-        CK(cudaMemcpyAsync(w->seg0, w->ckpt + (size_t)seg * sd, sd * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        for (int n = n0; n < n1; ++n) {
-            const int k = n - n0;
-            const size_t o = (size_t)k * sd;
-            CK(cudaMemcpyAsync(&s->ctl->dt_fixed, w->dts + n, sizeof(double), cudaMemcpyDeviceToDevice, st));
-            double *next = n + 1 < n1 ? w->seg0 + o + sd : s->A;
-            enqueue_step_between(s, 0, w->seg0 + o, &w->map0[k], w->seg1 + o, &w->map1[k], next);
+        if (!w->tape) {
+            CK(cudaMemcpyAsync(w->seg0, w->ckpt + (size_t)seg * sd, sd * sizeof(double), cudaMemcpyDeviceToDevice,
+                               st));
+            for (int n = n0; n < n1; ++n) {
+                const int k = n - n0;
+                const size_t o = (size_t)k * sd;
+                CK(cudaMemcpyAsync(&s->ctl->dt_fixed, w->dts + n, sizeof(double), cudaMemcpyDeviceToDevice, st));
+                double *next = n + 1 < n1 ? w->seg0 + o + sd : s->A;
+                enqueue_step_between(s, 0, w->seg0 + o, &w->map0[k], w->seg1 + o, &w->map1[k], next);
+            }
         }
         // reverse sweep over the segment
         for (int n = n1 - 1; n >= n0; --n) {

@@ -171,7 +171,8 @@ class Solver:
         self._ck(self._lib.rmhd2d_run_fixed_dt(self._h, len(d), d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
 
     def adjoint_forward(self, nsteps: int, checkpoint_interval: int = 0) -> None:
-        """nsteps steps, recording the dts and sqrt(N) checkpoints for adjoint_backward."""
+        """nsteps steps, recording the dts and sqrt(N) checkpoints for adjoint_backward
+        (checkpoint_interval 0; a negative one keeps every step's states, and backward recomputes nothing)."""
         self._ck(self._lib.rmhd2d_adjoint_forward(self._h, int(nsteps), int(checkpoint_interval)))
         self._adj_steps = int(nsteps)
 

@@ -6,7 +6,8 @@
 * Against central finite differences (h = 1e-6) of the CUDA fixed-dt
   forward: FD_REL, the agreement the adjoint is specified to reach.
 * The checkpoint interval changes nothing (segments are recomputed bit for
-  bit), and backward leaves the solver at the end of the forward run."""
+  bit; a kept whole trajectory gives the same gradient with no recompute),
+  and backward leaves the solver at the end of the forward run."""
 import numpy as np
 import pytest
 
@@ -51,6 +52,7 @@ def _ghost_gradient_is_zero(gs, nx, bc):
     (True, (23, 26), 6, 0, "symmetric", None),
     (True, (18, 21), 4, 2, "periodic", "symmetric"),
     (False, (21, 17), 5, 0, "symmetric", "periodic"),
+    (True, (22, 19), 5, -1, "symmetric", None),        # the whole trajectory kept
 ])
 def test_adjoint_matches_oracle_tangent(gpu, oracle, tangent, with_table, shape, nsteps, interval, bc, bc_y):
     from resistivemhd_gpu_b200 import Solver, setups
@@ -110,7 +112,7 @@ def test_checkpoint_interval_changes_nothing_and_state_is_restored(gpu):
     s = setups.orszag_tang(48)
     w = np.random.default_rng(1).standard_normal(s.state.shape)
     grads = []
-    for interval in (1, 3, 0, 10):
+    for interval in (1, 3, 0, 10, -1):   # -1: the whole trajectory kept, nothing recomputed
         with Solver.from_setup(s, precision="fp64_exact") as sol:
             sol.adjoint_forward(10, interval)
             end = sol.get_state().copy()
