@@ -594,7 +594,7 @@ def adjoint_block(args, local_rank, n=512, nsteps=2000, ndirs=32, h=1e-6):
             out["fp64_exact_whole_trajectory"] = {
                 "recorded_forward_ms": 1e3 * t_rec, "backward_ms": 1e3 * t_bwd,
                 "adjoint_over_forward": 1e3 * (t_rec + t_bwd) / ms_fwd,
-                "trajectory_bytes": 2 * nsteps * s.state.nbytes,
+                "trajectory_states": 2 * nsteps,
                 "gradient_equals_checkpointed": bool(np.array_equal(gs, grads["fp64_exact"][0])
                                                      and np.array_equal(ge, grads["fp64_exact"][1]))}
     except Exception as e:  # reported, never fatal
