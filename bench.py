@@ -268,7 +268,7 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
         "traffic": (traffic["stage1"] + traffic["stage2"]) / 2 if traffic else None,
         "algorithmic_bytes_per_launch": (ab["stage1"] + ab["stage2"]) / 2,
         "launch_ms": {"stage1": st1, "boundary1": bn1, "stage2": st2, "boundary2_cfl": bn2},
-        "note": "FP64-issue bound: see fp64 and DESIGN.md",
+        "note": "FP64-issue bound: the fp64 object carries the FP64 roofline",
     }
 
     # ---- end-to-end through the public API with pinned host buffers ----
