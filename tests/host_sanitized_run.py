@@ -2,7 +2,8 @@
 process with the address sanitizer's runtime preloaded: the host builds of
 the adjoint kernels (adjoint.cu, adjoint_prep.cu) and of the CT-Contact
 kernels (contact.cu) compiled with -fsanitize=address,undefined and run on
-small ragged grids of every wall pairing they support.  Any read or write
+small ragged grids, down to the smallest legal 6 x 6 interior, of every
+wall pairing they support.  Any read or write
 outside an allocation, and any undefined behaviour, aborts the child: the
 kernels' index arithmetic is checked against their buffers on the CPU.
 Prints "ok" at the end."""
@@ -30,16 +31,22 @@ def main() -> None:
     (tmp / "adj").mkdir()
     adj = A._build(tmp / "adj", contracted=False, extra=tuple(SANITIZE))
     for shape, bc, bc_y, table in [((13, 11), "periodic", None, True), ((12, 15), "symmetric", None, False),
-                                   ((14, 12), "periodic", "symmetric", True), ((11, 13), "symmetric", "periodic", False)]:
+                                   ((14, 12), "periodic", "symmetric", True), ((11, 13), "symmetric", "periodic", False),
+                                   ((6, 6), "periodic", None, True), ((6, 7), "symmetric", None, False),
+                                   ((7, 6), "periodic", "symmetric", False)]:
         s = setups.random_smooth_state(*shape, seed=3, bc=bc, bc_y=bc_y, with_table=table)
         _, dts, crashed, un, us = oracle.run_keep_stages(s, s.state, 2)
-        assert crashed == -1
-        gs, ge = A.backward(adj, s, un, us, dts, np.random.default_rng(1).standard_normal(s.state.shape))
-        assert np.isfinite(gs).all() and np.isfinite(ge).all()
+        # the smallest symmetric boxes crash in the reference's arithmetic;
+        # their trajectory up to and including the crashing step still runs
+        n = 2 if crashed < 0 else crashed + 1
+        gs, ge = A.backward(adj, s, un[:n], us[:n], dts[:n], np.random.default_rng(1).standard_normal(s.state.shape))
+        if crashed < 0:
+            assert np.isfinite(gs).all() and np.isfinite(ge).all()
     (tmp / "ct").mkdir()
     ct = C.build_contact(tmp / "ct", tuple(SANITIZE))
     for shape, bc, bc_y, table in [((13, 11), "periodic", None, True), ((12, 15), "symmetric", None, False),
-                                   ((14, 12), "flare", "wall", True), ((11, 13), "zero_gradient", "periodic", False)]:
+                                   ((14, 12), "flare", "wall", True), ((11, 13), "zero_gradient", "periodic", False),
+                                   ((6, 6), "periodic", None, False), ((6, 7), "symmetric", "wall", True)]:
         s = setups.random_smooth_state(*shape, seed=3, bc=bc, bc_y=bc_y, with_table=table)
         s.ct = "contact"
         want, want_dts, _ = oracle.run(s, s.state, 2)
