@@ -16,6 +16,7 @@
 // rounding.
 #pragma once
 
+#include <atomic>
 #include <cmath>
 #include <condition_variable>
 #include <cstdint>
@@ -31,6 +32,7 @@
 #define __forceinline__ inline
 #define __launch_bounds__(...)
 #define __shared__ static
+#define __align__(n) __attribute__((aligned(n)))
 
 struct dim3 {
     unsigned x, y, z;
@@ -58,13 +60,19 @@ template <class F> void host_launch(dim3 grid, dim3 block, F &&kernel_call)
                         }
 }
 
-// The barrier of the block that host_launch_threaded runs.  A thread that
-// returns leaves it, as an exited thread does on the device.
+// A barrier of the threads that host_launch_threaded runs (a block, or one
+// warp of it).  A thread that returns leaves it, as an exited thread does on
+// the device.
 struct ShimBarrier {
     std::mutex m;
     std::condition_variable cv;
     unsigned expected = 0, arrived = 0;
     unsigned long generation = 0;
+    void reset(unsigned n)
+    {
+        expected = n;
+        arrived = 0;
+    }
     void release()
     {
         arrived = 0;
@@ -89,8 +97,64 @@ struct ShimBarrier {
     }
 };
 inline ShimBarrier g_block_barrier;
+inline ShimBarrier g_warp_barrier[32];        // one per warp of the running block (at most 1024 threads)
+inline unsigned long long g_warp_lanes[32][32];
 
 inline void __syncthreads() { g_block_barrier.arrive_and_wait(); }
+
+inline unsigned shim_flat_thread() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+
+// Warp exchanges of the threaded launch: each lane posts its value, the warp
+// meets, each lane reads its partner's, the warp meets again.  Only full
+// warps (mask 0xffffffff) are modelled, which is how the kernels call them.
+inline unsigned long long __shfl_xor_sync(unsigned, unsigned long long v, int lane_mask)
+{
+    const unsigned t = shim_flat_thread(), w = t >> 5, lane = t & 31u;
+    g_warp_lanes[w][lane] = v;
+    g_warp_barrier[w].arrive_and_wait();
+    const unsigned long long r = g_warp_lanes[w][lane ^ (unsigned)lane_mask];
+    g_warp_barrier[w].arrive_and_wait();
+    return r;
+}
+inline int __any_sync(unsigned, int pred)
+{
+    const unsigned t = shim_flat_thread(), w = t >> 5, lane = t & 31u;
+    g_warp_lanes[w][lane] = pred ? 1ull : 0ull;
+    g_warp_barrier[w].arrive_and_wait();
+    int any = 0;
+    for (unsigned l = 0; l < 32; ++l) any |= g_warp_lanes[w][l] != 0ull;
+    g_warp_barrier[w].arrive_and_wait();
+    return any;
+}
+
+inline std::mutex g_atomic_mutex;
+inline unsigned long long atomicMax(unsigned long long *p, unsigned long long v)
+{
+    std::lock_guard<std::mutex> lk(g_atomic_mutex);
+    const unsigned long long old = *p;
+    if (v > old) *p = v;
+    return old;
+}
+inline unsigned long long atomicAdd(unsigned long long *p, unsigned long long v)
+{
+    std::lock_guard<std::mutex> lk(g_atomic_mutex);
+    const unsigned long long old = *p;
+    *p = old + v;
+    return old;
+}
+inline int atomicExch(int *p, int v)
+{
+    std::lock_guard<std::mutex> lk(g_atomic_mutex);
+    const int old = *p;
+    *p = v;
+    return old;
+}
+inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
+template <class T> inline T __ldcg(const T *p)
+{
+    std::lock_guard<std::mutex> lk(g_atomic_mutex);
+    return *p;
+}
 
 template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_call)
 {
@@ -100,8 +164,8 @@ template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_c
     for (unsigned bz = 0; bz < grid.z; ++bz)
         for (unsigned by = 0; by < grid.y; ++by)
             for (unsigned bx = 0; bx < grid.x; ++bx) {
-                g_block_barrier.expected = n;
-                g_block_barrier.arrived = 0;
+                g_block_barrier.reset(n);
+                for (unsigned w = 0; w < (n + 31) / 32; ++w) g_warp_barrier[w].reset(n - 32 * w < 32 ? n - 32 * w : 32);
                 std::vector<std::thread> threads;
                 threads.reserve(n);
                 for (unsigned t = 0; t < n; ++t)
@@ -109,10 +173,33 @@ template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_c
                         blockIdx = dim3(bx, by, bz);
                         threadIdx = dim3(t % block.x, (t / block.x) % block.y, t / (block.x * block.y));
                         kernel_call();
+                        g_warp_barrier[t >> 5].drop();
                         g_block_barrier.drop();
                     });
                 for (auto &th : threads) th.join();
             }
+}
+
+// The runtime calls the kernels' host launchers make.
+typedef int cudaError_t;
+enum { cudaSuccess = 0, cudaErrorInvalidValue = 1, cudaErrorInvalidDevice = 101 };
+enum cudaMemcpyKind { cudaMemcpyHostToHost, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice };
+inline cudaError_t cudaGetLastError() { return cudaSuccess; }
+inline cudaError_t cudaMemsetAsync(void *p, int v, size_t n, cudaStream_t = nullptr)
+{
+    std::memset(p, v, n);
+    return cudaSuccess;
+}
+inline cudaError_t cudaMemcpyAsync(void *d, const void *s, size_t n, cudaMemcpyKind, cudaStream_t = nullptr)
+{
+    std::memcpy(d, s, n);
+    return cudaSuccess;
+}
+inline cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
+template <class T> inline cudaError_t cudaGetSymbolAddress(void **p, T &symbol)
+{
+    *p = static_cast<void *>(&symbol);
+    return cudaSuccess;
 }
 
 // The device's __dadd_rn and the others are single correctly rounded

@@ -1,12 +1,13 @@
 """TEST INFRASTRUCTURE, run by tests/test_host_memory_safety.py in a child
-process with the address sanitizer's runtime preloaded: the host builds of
-the adjoint kernels (adjoint.cu, adjoint_prep.cu) and of the CT-Contact
-kernels (contact.cu) compiled with -fsanitize=address,undefined and run on
-small ragged grids, down to the smallest legal 6 x 6 interior, of every
-wall pairing they support.  Any read or write
-outside an allocation, and any undefined behaviour, aborts the child: the
-kernels' index arithmetic is checked against their buffers on the CPU.
-Prints "ok" at the end."""
+process with the address sanitizer's runtime preloaded.  The host builds of
+the adjoint kernels (adjoint.cu, adjoint_prep.cu), the CT-Contact kernels
+(contact.cu), the ghost fill and CFL reduction (aux_kernels.cu) and the
+allocation-free dt (noalloc_dt.cu) are compiled with
+-fsanitize=address,undefined and run on small ragged grids, down to the
+smallest legal 6 x 6 interior, with every wall pairing they support.  Any
+read or write outside an allocation, and any undefined behaviour, aborts
+the child: the kernels' index arithmetic is checked against their buffers on
+the CPU.  Prints "ok" at the end."""
 import sys
 import tempfile
 from pathlib import Path
@@ -52,6 +53,16 @@ def main() -> None:
         want, want_dts, _ = oracle.run(s, s.state, 2)
         got, got_dts, _ = C.run_host(ct, s, 2)
         assert np.array_equal(got, want, equal_nan=True) and np.array_equal(got_dts, want_dts)
+    import test_aux_host as X
+
+    (tmp / "aux").mkdir()
+    aux = X.build_aux(tmp / "aux", tuple(SANITIZE))
+    for bcx in ("periodic", "symmetric", "zero_gradient", "flare"):
+        for bcy in ("periodic", "symmetric", "zero_gradient", "wall"):
+            s = setups.random_smooth_state(6, 7, seed=4, bc=bcx, bc_y=bcy)
+            got, dt, _, _ = X.set_state_dt(aux, s, s.state, ghost_rates=True)
+            assert np.array_equal(got, oracle.boundary(s, s.state), equal_nan=True)
+            assert X.same(X.dt_noalloc(aux, s, got), dt)
     print("ok", flush=True)
 
 

@@ -1,6 +1,6 @@
 """Memory safety of kernel index arithmetic, checked on the CPU: the host
-builds of the adjoint and CT-Contact kernels run under the address and
-undefined-behaviour sanitizers (tests/host_sanitized_run.py) in a child
+builds of the adjoint, CT-Contact, ghost-fill/CFL and allocation-free dt
+kernels run under the address and undefined-behaviour sanitizers (tests/host_sanitized_run.py) in a child
 process that preloads the sanitizer runtime."""
 import os
 import subprocess
@@ -18,7 +18,7 @@ def _asan_runtime() -> str | None:
     return path if r.returncode == 0 and os.path.isabs(path) and os.path.exists(path) else None
 
 
-def test_adjoint_and_contact_kernels_stay_in_bounds():
+def test_host_built_kernels_stay_in_bounds():
     rt = _asan_runtime()
     if rt is None:
         pytest.skip("no address-sanitizer runtime on this host")
