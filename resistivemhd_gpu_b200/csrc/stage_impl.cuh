@@ -4,6 +4,7 @@
 #pragma once
 
 #include "stage.cuh"
+#include "tma_ptx.cuh"
 
 #ifndef RMHD_FAST_MATH
 #define RMHD_FAST_MATH 0
@@ -108,27 +109,12 @@ __device__ __forceinline__ void muscl_dev(double qm, double q0, double qp, doubl
     qR = qp - (double)(0.5f * mR);
 }
 
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
 // Waits for phase `phase` of the mbarrier with a bounded number of tries
 // (each try suspends for at most 20 us); false when the bound expired.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase)
 {
-    const uint32_t a = smem_addr(bar);
-    for (int tries = 0; tries < 50000; ++tries) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(a), "r"(phase), "r"(20000u)
-            : "memory");
-        if (ok) return true;
-    }
+    for (int tries = 0; tries < 50000; ++tries)
+        if (mbar_try_wait(bar, phase)) return true;
     return false;
 }
 
@@ -167,24 +153,12 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
     // (and one 2-D load of the eta table) ----
     if (tid == 0) {
         // order this CTA's earlier shared-memory accesses before the async copy
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                     ::"r"(smem_addr(bar)), "r"(T::U_BYTES + (has_eta ? T::E_BYTES : 0u)) : "memory");
+        fence_proxy_async();
+        mbar_expect_tx(bar, T::U_BYTES + (has_eta ? T::E_BYTES : 0u));
         // x coordinate (j) = j0 - 3 = tj * TJ: a multiple of TJ (even), so
         // 16-byte aligned in the global tensor as TMA requires.
-        asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-            " [%0], [%1, {%3, %4, %5}], [%2];"
-            ::"r"(smem_addr(Ut)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(smem_addr(bar)),
-              "r"(j0 - HALO), "r"(i0 - HALO), "r"(0)
-            : "memory");
-        if (has_eta)
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-                " [%0], [%1, {%3, %4}], [%2];"
-                ::"r"(smem_addr(Et)), "l"(reinterpret_cast<uint64_t>(emap)), "r"(smem_addr(bar)),
-                  "r"(j0 - HALO), "r"(i0 - HALO)
-                : "memory");
+        tma_load_3d(Ut, tmap, bar, j0 - HALO, i0 - HALO, 0);
+        if (has_eta) tma_load_2d(Et, emap, bar, j0 - HALO, i0 - HALO);
     }
 
     // own cell of this thread in the update phase
@@ -198,7 +172,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
 #pragma unroll
         for (int f = 0; f < NFIELD; ++f)
             if (f != BXF && f != BYF)
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(a.un + f * PL + k)));
+                prefetch_l2(a.un + f * PL + k);
     }
 
     // dt of this step from the CFL reduction of the previous state
@@ -574,11 +548,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
 
 __device__ __forceinline__ void init_tile_barrier(uint64_t *bar)
 {
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
+    if (threadIdx.x == 0) mbar_init_tile(bar);
     __syncthreads();
 }
 
