@@ -31,6 +31,7 @@
 #define __host__
 #define __forceinline__ inline
 #define __launch_bounds__(...)
+#define __grid_constant__
 #define __shared__ static
 #define __align__(n) __attribute__((aligned(n)))
 
@@ -43,6 +44,12 @@ inline thread_local dim3 blockIdx, threadIdx;
 inline dim3 blockDim, gridDim;
 
 typedef struct CUstream_st *cudaStream_t;
+
+// The driver's opaque 128-byte tensor-map type; host builds fill it with
+// tests/host_tma.h's HostMap.
+typedef struct CUtensorMap_st {
+    alignas(64) unsigned long long opaque[16];
+} CUtensorMap;
 
 template <class F> void host_launch(dim3 grid, dim3 block, F &&kernel_call)
 {
@@ -102,7 +109,31 @@ inline unsigned long long g_warp_lanes[32][32];
 
 inline void __syncthreads() { g_block_barrier.arrive_and_wait(); }
 
+inline std::atomic<int> g_block_or{0};
+inline int shim_flat_thread_id();
+// Block-wide OR of pred, returned to every thread (three meetings: gather,
+// read, clear).
+inline int __syncthreads_or(int pred)
+{
+    if (pred) g_block_or.fetch_or(1);
+    __syncthreads();
+    const int r = g_block_or.load();
+    __syncthreads();
+    if (shim_flat_thread_id() == 0) g_block_or.store(0);
+    __syncthreads();
+    return r;
+}
+
+// Dynamic shared memory of the running block (host_launch_threaded's
+// `smem_bytes`), filled with NaN bytes at each block's start so that a read
+// of a word the block did not write shows up in the results.
+// It is allocated at exactly the launch's size, so that a sanitizer sees an
+// access past its end.
+inline unsigned char *g_dynamic_smem = nullptr;
+inline unsigned char *shim_dynamic_smem() { return g_dynamic_smem; }
+
 inline unsigned shim_flat_thread() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+inline int shim_flat_thread_id() { return (int)shim_flat_thread(); }
 
 // Warp exchanges of the threaded launch: each lane posts its value, the warp
 // meets, each lane reads its partner's, the warp meets again.  Only full
@@ -156,7 +187,7 @@ template <class T> inline T __ldcg(const T *p)
     return *p;
 }
 
-template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_call)
+template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_call, size_t smem_bytes = 0)
 {
     gridDim = grid;
     blockDim = block;
@@ -164,6 +195,11 @@ template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_c
     for (unsigned bz = 0; bz < grid.z; ++bz)
         for (unsigned by = 0; by < grid.y; ++by)
             for (unsigned bx = 0; bx < grid.x; ++bx) {
+                void *smem = nullptr;
+                if (smem_bytes && posix_memalign(&smem, 1024, smem_bytes) != 0) std::abort();
+                if (smem) std::memset(smem, 0xFF, smem_bytes);
+                g_dynamic_smem = static_cast<unsigned char *>(smem);
+                g_block_or.store(0);
                 g_block_barrier.reset(n);
                 for (unsigned w = 0; w < (n + 31) / 32; ++w) g_warp_barrier[w].reset(n - 32 * w < 32 ? n - 32 * w : 32);
                 std::vector<std::thread> threads;
@@ -177,6 +213,8 @@ template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_c
                         g_block_barrier.drop();
                     });
                 for (auto &th : threads) th.join();
+                std::free(smem);
+                g_dynamic_smem = nullptr;
             }
 }
 
@@ -196,6 +234,12 @@ inline cudaError_t cudaMemcpyAsync(void *d, const void *s, size_t n, cudaMemcpyK
     return cudaSuccess;
 }
 inline cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
+enum cudaFuncAttribute { cudaFuncAttributeMaxDynamicSharedMemorySize = 8 };
+struct cudaFuncAttributes {
+    int numRegs = 0;
+};
+template <class F> inline cudaError_t cudaFuncSetAttribute(F, cudaFuncAttribute, int) { return cudaSuccess; }
+inline cudaError_t cudaFuncGetAttributes(cudaFuncAttributes *, const void *) { return cudaSuccess; }
 template <class T> inline cudaError_t cudaGetSymbolAddress(void **p, T &symbol)
 {
     *p = static_cast<void *>(&symbol);

@@ -68,9 +68,12 @@ def rewrite_launches(src: str, threaded: tuple[str, ...] = ()) -> str:
             m += 1
         cfg = _split_top_level(src[k + 3:e])
         name = kernel.split("<")[0]
-        launcher = "host_launch_threaded" if name in threaded else "host_launch"
         out.append(src[pos:j])
-        out.append(f"{launcher}({cfg[0]}, {cfg[1]}, [&]() {{ {kernel}({src[e + 4:m]}); }})")
+        if name in threaded:
+            smem = cfg[2] if len(cfg) > 2 else "0"
+            out.append(f"host_launch_threaded({cfg[0]}, {cfg[1]}, [&]() {{ {kernel}({src[e + 4:m]}); }}, {smem})")
+        else:
+            out.append(f"host_launch({cfg[0]}, {cfg[1]}, [&]() {{ {kernel}({src[e + 4:m]}); }})")
         pos = m + 1
     out.append(src[pos:])
     return "".join(out)
@@ -79,12 +82,24 @@ def rewrite_launches(src: str, threaded: tuple[str, ...] = ()) -> str:
 SANITIZE = ["-fsanitize=address,undefined", "-fno-omit-frame-pointer", "-fno-sanitize-recover=all"]
 
 
-def compile_unit(d: Path, name: str, flags: list[str], threaded: tuple[str, ...] = ()) -> str:
-    """Rewrites csrc/<name> into d and compiles it to an object; returns its path."""
+def _rewrite(name: str, threaded: tuple[str, ...]) -> str:
     text = rewrite_launches((CSRC / name).read_text(), threaded)
-    assert "<<<" not in text
+    # dynamic shared memory: the running block's buffer of the threaded launch
+    text = text.replace("extern __shared__ __align__(1024) unsigned char smem_raw[];",
+                        "unsigned char *smem_raw = shim_dynamic_smem();")
+    assert "<<<" not in text and "extern __shared__" not in text
+    return f"#line 1 \"{CSRC / name}\"\n" + text
+
+
+def compile_unit(d: Path, name: str, flags: list[str], threaded: tuple[str, ...] = (),
+                 headers: tuple[str, ...] = ()) -> str:
+    """Rewrites csrc/<name> into d and compiles it to an object; returns its
+    path.  `headers` are csrc headers holding kernels the unit includes:
+    rewritten into d too, where the unit's #include finds them first."""
+    for h in headers:
+        (d / h).write_text(_rewrite(h, threaded))
     src = d / (name + ".cpp")
-    src.write_text(f"#line 1 \"{CSRC / name}\"\n" + text)
+    src.write_text(_rewrite(name, threaded))
     obj = d / (name + ".o")
     subprocess.run(["g++", "-std=c++17", "-O2", *flags, "-Wno-unknown-pragmas", "-fPIC", "-c", "-I", str(d),
                     "-I", str(CSRC), "-I", str(ORACLE), str(src), "-o", str(obj)], check=True, capture_output=True)
@@ -92,8 +107,9 @@ def compile_unit(d: Path, name: str, flags: list[str], threaded: tuple[str, ...]
 
 
 def shim_dir(d: Path) -> Path:
-    """A directory whose cuda_runtime.h is the host shim."""
+    """A directory whose cuda_runtime.h and cuda.h are the host shim."""
     (d / "cuda_runtime.h").write_text(f'#include "{HERE / "cuda_host_shim.h"}"\n')
+    (d / "cuda.h").write_text(f'#include "{HERE / "cuda_host_shim.h"}"\n')
     return d
 
 

@@ -1,7 +1,7 @@
 """TEST INFRASTRUCTURE, run by tests/test_host_memory_safety.py in a child
 process with the address sanitizer's runtime preloaded.  The host builds of
-the adjoint kernels (adjoint.cu, adjoint_prep.cu), the CT-Contact kernels
-(contact.cu), the ghost fill and CFL reduction (aux_kernels.cu) and the
+the fused stage kernel (stage_exact.cu), the adjoint kernels (adjoint.cu,
+adjoint_prep.cu), the CT-Contact kernels (contact.cu), the ghost fill and CFL reduction (aux_kernels.cu) and the
 allocation-free dt (noalloc_dt.cu) are compiled with
 -fsanitize=address,undefined and run on small ragged grids, down to the
 smallest legal 6 x 6 interior, with every wall pairing they support.  Any
@@ -63,6 +63,17 @@ def main() -> None:
             got, dt, _, _ = X.set_state_dt(aux, s, s.state, ghost_rates=True)
             assert np.array_equal(got, oracle.boundary(s, s.state), equal_nan=True)
             assert X.same(X.dt_noalloc(aux, s, got), dt)
+    import test_stage_host as S
+
+    (tmp / "stage").mkdir()
+    stage = S.build_stage(tmp / "stage", tuple(SANITIZE))
+    for shape in (0, 1):
+        for dims, bc, bc_y, table in [((6, 6), "periodic", None, True), ((19, 13), "symmetric", None, False),
+                                      ((9, 7), "flare", "wall", True), ((14, 11), "periodic", "symmetric", False)]:
+            s = setups.random_smooth_state(*dims, seed=5, bc=bc, bc_y=bc_y, with_table=table)
+            want, want_dts, _ = oracle.run(s, s.state, 1)
+            got, got_dts, _ = S.run_host(stage, s, 1, shape)
+            assert np.array_equal(got, want, equal_nan=True) and np.array_equal(got_dts, want_dts, equal_nan=True)
     print("ok", flush=True)
 
 

@@ -1,0 +1,73 @@
+"""The fused stage kernel on the CPU: the exact variant (stage_exact.cu) and
+the ghost-fill / CFL kernels compiled for the host (tests/host_build.py,
+RMHD_HOST_TMA_EMULATION with tests/host_tma.cpp for the tile staging; the
+kernels run one host thread per CUDA thread) and driven as enqueue_step
+drives them (tests/stage_host.cpp).  Built without contraction, as nvcc
+builds the exact variant (-fmad=false), states and dts must equal the
+oracle's bit for bit, as tests/test_gpu_parity.py requires of the CUDA run.
+Shared memory starts each block as NaN bytes, so a read of a word the
+kernel did not stage or compute would show in the results."""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from host_build import compile_unit, link, shim_dir
+
+HERE = Path(__file__).resolve().parent
+BC = {"periodic": 0, "symmetric": 1, "zero_gradient": 2, "wall": 3, "flare": 4}
+EMU = "-DRMHD_HOST_TMA_EMULATION"
+
+
+def build_stage(d: Path, extra: tuple[str, ...] = ()):
+    """stage_exact.cu, aux_kernels.cu, the staging emulation and the step
+    driver as a host library; `extra` adds compiler flags to every unit."""
+    shim_dir(d)
+    objs = [compile_unit(d, "stage_exact.cu", ["-ffp-contract=off", EMU, *extra],
+                         threaded=("stage_kernel", "stage_batch_kernel"), headers=("stage_impl.cuh",)),
+            compile_unit(d, "aux_kernels.cu", ["-ffp-contract=off", *extra],
+                         threaded=("kernel", "rate_kernel", "boundary_batch_kernel"))]
+    lib = link(d, objs, [HERE / "host_tma.cpp", HERE / "stage_host.cpp"], "libstagehost.so", (EMU, *extra))
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.host_stage_run.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 6 + [
+        ctypes.c_int, ctypes.c_int, D, ctypes.c_int, D, ctypes.c_int, D]
+    lib.host_stage_run.restype = ctypes.c_int
+    return lib
+
+
+@pytest.fixture(scope="module")
+def host_stage(tmp_path_factory):
+    return build_stage(tmp_path_factory.mktemp("stagehost"))
+
+
+def run_host(lib, s, nsteps, shape):
+    D = ctypes.POINTER(ctypes.c_double)
+    tab = None if s.eta_table is None else np.ascontiguousarray(s.eta_table, dtype=np.float64)
+    state = np.ascontiguousarray(s.state, dtype=np.float64).copy()
+    dts = np.zeros(max(nsteps, 1))
+    rc = lib.host_stage_run(s.nx, s.ny, s.dx, s.dy, s.gamma, s.cfl, s.eps, s.eta, BC[s.bc],
+                            BC[s.bc_y] if s.bc_y else -1, None if tab is None else tab.ctypes.data_as(D), shape,
+                            state.ctypes.data_as(D), nsteps, dts.ctypes.data_as(D))
+    assert rc != -1, "a tile's staging wait expired"
+    return state, dts[:nsteps], rc - 1 if rc > 0 else -1
+
+
+@pytest.mark.parametrize("shape", [0, 1])
+@pytest.mark.parametrize("dims,nsteps,bc,bc_y,with_table", [
+    ((20, 18), 3, "periodic", None, False),
+    ((37, 29), 2, "periodic", None, True),
+    ((26, 40), 2, "symmetric", None, True),
+    ((23, 19), 2, "periodic", "symmetric", False),
+    ((21, 25), 2, "flare", "wall", True),
+    ((18, 17), 2, "zero_gradient", "periodic", False),
+])
+def test_host_stage_step_equals_oracle(host_stage, oracle, shape, dims, nsteps, bc, bc_y, with_table):
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(*dims, seed=17, bc=bc, bc_y=bc_y, with_table=with_table)
+    want, want_dts, want_crash = oracle.run(s, s.state, nsteps)
+    got, got_dts, got_crash = run_host(host_stage, s, nsteps, shape)
+    assert got_crash == want_crash
+    assert np.array_equal(got_dts, want_dts)
+    assert np.array_equal(got, want, equal_nan=True)
