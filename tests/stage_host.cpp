@@ -89,4 +89,82 @@ int host_stage_run(int nx, int ny, double dx, double dy, double gamma, double cf
     return rc;
 }
 
+// A batch of `nruns` runs (per run: nx, ny, dx, dy, eta, bc_x, bc_y; the
+// states concatenated in `states`, updated in place) stepped nsteps times
+// as rmhd2d_batch_run steps them, with `ctas` persistent CTAs per stage
+// launch; dts[r * nsteps + n] is run r's dt of step n.  gamma, cfl and eps
+// are shared.  Returns 0, or -1 when a tile's staging wait expired.
+int host_batch_run(int nruns, const int *nx, const int *ny, const double *dx, const double *dy, const double *eta,
+                   const int *bc_x, const int *bc_y, double gamma, double cfl, double eps, int shape, int ctas,
+                   double *states, int nsteps, double *dts)
+{
+    std::vector<Grid> grids(nruns);
+    std::vector<std::vector<double>> A(nruns), B(nruns), row2(nruns);
+    std::vector<Control> ctl(nruns);
+    std::vector<BatchRun> runs(nruns);
+    std::vector<CUtensorMap> maps((size_t)nruns * MAPS_PER_RUN);
+    std::vector<TileRef> tiles[2];
+    long long max_ghost = 0;
+    size_t off = 0;
+    for (int r = 0; r < nruns; ++r) {
+        Grid &g = grids[r];
+        g = Grid{};
+        g.nx = nx[r];
+        g.ny = ny[r];
+        g.pitch = (g.ny + 31) / 32 * 32;
+        g.plane = (long long)g.nx * g.pitch;
+        g.dx = dx[r];
+        g.dy = dy[r];
+        g.gamma = gamma;
+        g.cfl = cfl;
+        g.eps = eps;
+        g.eta = eta[r];
+        g.bc_x = bc_x[r];
+        g.bc_y = bc_y[r] < 0 ? bc_x[r] : bc_y[r];
+        const size_t P = (size_t)g.plane;
+        A[r].assign(P * NFIELD, 0.0);
+        B[r].assign(P * NFIELD, 0.0);
+        row2[r].assign((size_t)g.nx, 0.0);
+        launch_aos_to_planes(g, states + off, A[r].data(), nullptr);
+        if (g.bc_x == BC_SYMMETRIC) launch_snapshot_row2(g, A[r].data(), row2[r].data(), nullptr);
+        launch_boundary(g, A[r].data(), row2[r].data(), nullptr, 0, nullptr);
+        launch_rate(g, A[r].data(), &ctl[r], 0, 1, nullptr);
+        off += (size_t)g.nx * g.ny * NFIELD;
+        runs[r] = BatchRun{g, A[r].data(), B[r].data(), nullptr, row2[r].data(), &ctl[r]};
+        const unsigned long long st0 = (unsigned long long)g.pitch * 8, st1 = (unsigned long long)P * 8;
+        const unsigned uj = (unsigned)shape_uj(shape);
+        for (int st = 1; st <= 2; ++st)
+            maps[(size_t)r * MAPS_PER_RUN + st - 1] = host_map(st == 1 ? A[r].data() : B[r].data(), 3, g.ny, g.nx,
+                                                               NFIELD, st0, st1, uj, (unsigned)stage_ui(st, shape), NFIELD);
+        const long long ng = 6LL * g.ny + 6LL * (g.nx - 6);
+        max_ghost = ng > max_ghost ? ng : max_ghost;
+        for (int st = 1; st <= 2; ++st) {
+            const int ti = stage_ti(st, shape), tj = shape_tj(shape);
+            const int nti = (g.nx - 2 * HALO + ti - 1) / ti, ntj = (g.ny - 2 * HALO + tj - 1) / tj;
+            for (int a = 0; a < nti; ++a)
+                for (int c = 0; c < ntj; ++c) tiles[st - 1].push_back(TileRef{r, a, c, 0});
+        }
+    }
+    int parity = 0;
+    for (int n = 0; n < nsteps; ++n) {
+        exact::launch_stage_batch(1, shape, runs.data(), maps.data(), tiles[0].data(), (int)tiles[0].size(), ctas,
+                                  parity, nullptr);
+        launch_boundary_batch(runs.data(), nruns, max_ghost, 0, 0, nullptr);
+        exact::launch_stage_batch(2, shape, runs.data(), maps.data(), tiles[1].data(), (int)tiles[1].size(), ctas,
+                                  parity, nullptr);
+        launch_boundary_batch(runs.data(), nruns, max_ghost, 1, parity ^ 1, nullptr);
+        for (int r = 0; r < nruns; ++r) {
+            if (ctl[r].error) return -1;
+            dts[(size_t)r * nsteps + n] = ctl[r].dt;
+        }
+        parity ^= 1;
+    }
+    off = 0;
+    for (int r = 0; r < nruns; ++r) {
+        launch_planes_to_aos(grids[r], A[r].data(), states + off, nullptr);
+        off += (size_t)grids[r].nx * grids[r].ny * NFIELD;
+    }
+    return 0;
+}
+
 }  // extern "C"

@@ -71,3 +71,37 @@ def test_host_stage_step_equals_oracle(host_stage, oracle, shape, dims, nsteps, 
     assert got_crash == want_crash
     assert np.array_equal(got_dts, want_dts)
     assert np.array_equal(got, want, equal_nan=True)
+
+
+@pytest.mark.parametrize("shape,ctas", [(0, 1), (0, 3), (1, 2)])
+def test_host_batch_equals_single_oracle_runs(host_stage, oracle, shape, ctas):
+    """The persistent batch kernel over runs of uneven size and walls: a few
+    CTAs walk the tile table (flipping the mbarrier's phase tile by tile),
+    and every run equals its own oracle run bit for bit."""
+    from resistivemhd_gpu_b200 import setups
+
+    setups_ = [setups.random_smooth_state(21, 14, seed=31, bc="periodic"),
+               setups.random_smooth_state(9, 27, seed=32, bc="symmetric"),
+               setups.random_smooth_state(16, 16, seed=33, bc="periodic", bc_y="symmetric")]
+    nsteps = 2
+    I = lambda v: (ctypes.c_int * len(v))(*v)          # noqa: E731
+    F = lambda v: (ctypes.c_double * len(v))(*v)       # noqa: E731
+    states = np.concatenate([s.state.ravel() for s in setups_])
+    dts = np.zeros(len(setups_) * nsteps)
+    lib = host_stage
+    lib.host_batch_run.restype = ctypes.c_int
+    D = ctypes.POINTER(ctypes.c_double)
+    rc = lib.host_batch_run(len(setups_), I([s.nx for s in setups_]), I([s.ny for s in setups_]),
+                            F([s.dx for s in setups_]), F([s.dy for s in setups_]), F([s.eta for s in setups_]),
+                            I([BC[s.bc] for s in setups_]), I([BC[s.bc_y] if s.bc_y else -1 for s in setups_]),
+                            ctypes.c_double(setups_[0].gamma), ctypes.c_double(setups_[0].cfl),
+                            ctypes.c_double(setups_[0].eps), shape, ctas, states.ctypes.data_as(D), nsteps,
+                            dts.ctypes.data_as(D))
+    assert rc == 0
+    off = 0
+    for r, s in enumerate(setups_):
+        n = s.state.size
+        want, want_dts, _ = oracle.run(s, s.state, nsteps)
+        assert np.array_equal(states[off:off + n].reshape(s.state.shape), want, equal_nan=True), r
+        assert np.array_equal(dts[r * nsteps:(r + 1) * nsteps], want_dts), r
+        off += n
