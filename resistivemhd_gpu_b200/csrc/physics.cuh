@@ -49,37 +49,55 @@ template <typename T> __device__ __forceinline__ T minmod(T x, T y, T eps)
 }
 
 // Single-precision reciprocal and square roots of the FP32-bulk variant
-// (hardware approximations, ~1 ulp of float).
+// (hardware approximations, ~1 ulp of float).  A host build of the kernels
+// (CPU tests, RMHD_HOST_EMULATION) takes the correctly rounded values.
 __device__ __forceinline__ float rcp_nr(float a)
 {
+#if defined(RMHD_HOST_EMULATION)
+    return 1.0f / a;
+#else
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
     return r;
+#endif
 }
 __device__ __forceinline__ float rsqrt_t(float a)
 {
+#if defined(RMHD_HOST_EMULATION)
+    return 1.0f / sqrtf(a);
+#else
     float r;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
     return r;
+#endif
 }
 __device__ __forceinline__ float sqrt_t(float a)
 {
+#if defined(RMHD_HOST_EMULATION)
+    return sqrtf(a);
+#else
     float r;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
     return r;
+#endif
 }
 __device__ __forceinline__ double rsqrt_t(double a) { return rsqrt(a); }
 __device__ __forceinline__ double sqrt_t(double a) { return sqrt(a); }
 
 // Reciprocal by Newton-Raphson iteration on 1/a (x' = x + x (1 - a x), two
 // steps, each squaring the relative error) from the hardware seed
-// rcp.approx.ftz.f64; used by the fast variant only.  Accurate to about one
-// ulp for normal finite a; a = 0 or +-inf give NaN (the fast variant's
-// denominators carry the reference's +EPS and are never 0 in a finite state).
+// rcp.approx.ftz.f64 (a host build: the correctly rounded 1/a); used by the
+// fast variant only.  Accurate to about one ulp for normal finite a; a = 0
+// or +-inf give NaN (the fast variant's denominators carry the reference's
+// +EPS and are never 0 in a finite state).
 __device__ __forceinline__ double rcp_nr(double a)
 {
     double r;
+#if defined(RMHD_HOST_EMULATION)
+    r = 1.0 / a;
+#else
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(a));
+#endif
     double e = fma(-a, r, 1.0);
     r = fma(r, e, r);
     e = fma(-a, r, 1.0);

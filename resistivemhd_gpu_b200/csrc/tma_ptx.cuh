@@ -4,7 +4,7 @@
 // function each.
 //
 // A host build of the stage kernel (CPU tests) defines
-// RMHD_HOST_TMA_EMULATION and supplies its own definitions of these
+// RMHD_HOST_EMULATION and supplies its own definitions of these
 // functions; this header then only declares them.
 #pragma once
 
@@ -15,7 +15,7 @@
 
 namespace rmhd2d {
 
-#if defined(RMHD_HOST_TMA_EMULATION)
+#if defined(RMHD_HOST_EMULATION)
 
 void mbar_init_tile(uint64_t *bar);
 bool mbar_try_wait(uint64_t *bar, uint32_t phase);

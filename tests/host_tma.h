@@ -1,5 +1,5 @@
 // host_tma.h -- TEST INFRASTRUCTURE.  The tensor map of the host build of the
-// stage kernel (RMHD_HOST_TMA_EMULATION): what cuTensorMapEncodeTiled would
+// stage kernel (RMHD_HOST_EMULATION): what cuTensorMapEncodeTiled would
 // encode for the library's maps (csrc/api.cu: encode_state_map,
 // encode_eta_map), held in the bytes of a CUtensorMap.
 #pragma once

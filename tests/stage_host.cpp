@@ -1,6 +1,7 @@
 // stage_host.cpp -- TEST INFRASTRUCTURE.  The stage-1-EMF RK2 step of the C
-// ABI run on the CPU over the fused stage kernel's own source (the exact
-// variant, stage_exact.cu) and the ghost-fill / CFL kernels
+// ABI run on the CPU over the fused stage kernel's own source (the variant
+// STAGE_VARIANT names: stage_exact.cu, stage_fast.cu or stage_bulk32.cu)
+// and the ghost-fill / CFL kernels
 // (aux_kernels.cu), compiled for the host through cuda_host_shim.h with the
 // tile staging of host_tma.cpp.  The set-up mirrors rmhd2d_create +
 // rmhd2d_set_state(apply_boundary = 1), the tensor maps those of
@@ -13,6 +14,11 @@
 #include "physics.cuh"
 #include "rmhd2d_internal.h"
 #include "stage.cuh"
+
+// The kernel variant this driver steps (exact, fast or bulk32).
+#ifndef STAGE_VARIANT
+#define STAGE_VARIANT exact
+#endif
 
 using namespace rmhd2d;
 
@@ -70,12 +76,12 @@ int host_stage_run(int nx, int ny, double dx, double dy, double gamma, double cf
         a.src = A.data();
         a.un = A.data();
         a.dst = B.data();
-        exact::launch_stage(1, shape, &mapA, &mapE1, a, nullptr);
+        STAGE_VARIANT::launch_stage(1, shape, &mapA, &mapE1, a, nullptr);
         launch_boundary(g, B.data(), row2.data(), nullptr, 0, nullptr);
         a.src = B.data();
         a.un = A.data();
         a.dst = A.data();
-        exact::launch_stage(2, shape, &mapB, &mapE2, a, nullptr);
+        STAGE_VARIANT::launch_stage(2, shape, &mapB, &mapE2, a, nullptr);
         launch_boundary(g, A.data(), row2.data(), &ctl, parity ^ 1, nullptr);
         dts[n] = ctl.dt;
         parity ^= 1;
@@ -147,10 +153,10 @@ int host_batch_run(int nruns, const int *nx, const int *ny, const double *dx, co
     }
     int parity = 0;
     for (int n = 0; n < nsteps; ++n) {
-        exact::launch_stage_batch(1, shape, runs.data(), maps.data(), tiles[0].data(), (int)tiles[0].size(), ctas,
+        STAGE_VARIANT::launch_stage_batch(1, shape, runs.data(), maps.data(), tiles[0].data(), (int)tiles[0].size(), ctas,
                                   parity, nullptr);
         launch_boundary_batch(runs.data(), nruns, max_ghost, 0, 0, nullptr);
-        exact::launch_stage_batch(2, shape, runs.data(), maps.data(), tiles[1].data(), (int)tiles[1].size(), ctas,
+        STAGE_VARIANT::launch_stage_batch(2, shape, runs.data(), maps.data(), tiles[1].data(), (int)tiles[1].size(), ctas,
                                   parity, nullptr);
         launch_boundary_batch(runs.data(), nruns, max_ghost, 1, parity ^ 1, nullptr);
         for (int r = 0; r < nruns; ++r) {

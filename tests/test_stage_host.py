@@ -1,6 +1,6 @@
 """The fused stage kernel on the CPU: the exact variant (stage_exact.cu) and
 the ghost-fill / CFL kernels compiled for the host (tests/host_build.py,
-RMHD_HOST_TMA_EMULATION with tests/host_tma.cpp for the tile staging; the
+RMHD_HOST_EMULATION with tests/host_tma.cpp for the tile staging; the
 kernels run one host thread per CUDA thread) and driven as enqueue_step
 drives them (tests/stage_host.cpp).  Built without contraction, as nvcc
 builds the exact variant (-fmad=false), states and dts must equal the
@@ -17,18 +17,28 @@ from host_build import compile_unit, link, shim_dir
 
 HERE = Path(__file__).resolve().parent
 BC = {"periodic": 0, "symmetric": 1, "zero_gradient": 2, "wall": 3, "flare": 4}
-EMU = "-DRMHD_HOST_TMA_EMULATION"
+EMU = "-DRMHD_HOST_EMULATION"
 
 
-def build_stage(d: Path, extra: tuple[str, ...] = ()):
-    """stage_exact.cu, aux_kernels.cu, the staging emulation and the step
-    driver as a host library; `extra` adds compiler flags to every unit."""
+# the host flags that model each variant's device build: -fmad=false for the
+# exact one, contraction into fused multiply-adds for the others
+VARIANTS = {"exact": ("stage_exact.cu", ["-ffp-contract=off"]),
+            "fast": ("stage_fast.cu", ["-ffp-contract=fast", "-mfma"]),
+            "bulk32": ("stage_bulk32.cu", ["-ffp-contract=fast", "-mfma"])}
+
+
+def build_stage(d: Path, extra: tuple[str, ...] = (), variant: str = "exact"):
+    """A stage kernel variant, aux_kernels.cu, the staging emulation and the
+    step driver as a host library; `extra` adds compiler flags to every
+    unit."""
     shim_dir(d)
-    objs = [compile_unit(d, "stage_exact.cu", ["-ffp-contract=off", EMU, *extra],
+    unit, flags = VARIANTS[variant]
+    objs = [compile_unit(d, unit, [*flags, EMU, *extra],
                          threaded=("stage_kernel", "stage_batch_kernel"), headers=("stage_impl.cuh",)),
             compile_unit(d, "aux_kernels.cu", ["-ffp-contract=off", *extra],
                          threaded=("kernel", "rate_kernel", "boundary_batch_kernel"))]
-    lib = link(d, objs, [HERE / "host_tma.cpp", HERE / "stage_host.cpp"], "libstagehost.so", (EMU, *extra))
+    lib = link(d, objs, [HERE / "host_tma.cpp", HERE / "stage_host.cpp"], "libstagehost.so",
+               (EMU, f"-DSTAGE_VARIANT={variant}", *extra))
     D = ctypes.POINTER(ctypes.c_double)
     lib.host_stage_run.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 6 + [
         ctypes.c_int, ctypes.c_int, D, ctypes.c_int, D, ctypes.c_int, D]
@@ -105,3 +115,38 @@ def test_host_batch_equals_single_oracle_runs(host_stage, oracle, shape, ctas):
         assert np.array_equal(states[off:off + n].reshape(s.state.shape), want, equal_nan=True), r
         assert np.array_equal(dts[r * nsteps:(r + 1) * nsteps], want_dts), r
         off += n
+
+
+@pytest.fixture(scope="module", params=["fast", "bulk32"])
+def host_stage_contracted(request, tmp_path_factory):
+    if " fma " not in open("/proc/cpuinfo").read().replace("\n", " "):
+        pytest.skip("the host has no fused multiply-add to model the device build with")
+    return request.param, build_stage(tmp_path_factory.mktemp("stagehost_" + request.param), variant=request.param)
+
+
+# relative L1 per field against the exact oracle after the steps (the GPU
+# tests' bounds: fp64_fast differs by rounding only, fp32_bulk by its FP32 core)
+HOST_REL_L1 = {"fast": 1e-12, "bulk32": 1e-5}
+
+
+@pytest.mark.parametrize("shape", [0, 1])
+@pytest.mark.parametrize("dims,bc,bc_y,with_table", [
+    ((37, 29), "periodic", None, True),
+    ((26, 40), "symmetric", None, True),
+    ((21, 25), "flare", "wall", False),
+])
+def test_host_contracted_variants_within_bounds(host_stage_contracted, oracle, shape, dims, bc, bc_y, with_table):
+    """The fast and FP32-bulk variants built as nvcc builds them (contracted;
+    the hardware reciprocal and square-root seeds replaced by correctly
+    rounded values) stay within their bounds of the exact oracle."""
+    from resistivemhd_gpu_b200 import setups
+
+    variant, lib = host_stage_contracted
+    s = setups.random_smooth_state(*dims, seed=19, bc=bc, bc_y=bc_y, with_table=with_table)
+    want, want_dts, _ = oracle.run(s, s.state, 3)
+    got, got_dts, crashed = run_host(lib, s, 3, shape)
+    assert crashed == -1 and np.isfinite(got).all()
+    assert np.allclose(got_dts, want_dts, rtol=HOST_REL_L1[variant], atol=0)
+    for f in range(8):
+        rel = np.abs(got[..., f] - want[..., f]).sum() / max(np.abs(want[..., f]).sum(), 1e-300)
+        assert rel <= HOST_REL_L1[variant], (variant, f, rel)
