@@ -72,33 +72,36 @@ template <class F> void host_launch(dim3 grid, dim3 block, F &&kernel_call)
 // the device.
 struct ShimBarrier {
     std::mutex m;
-    std::condition_variable cv;
     unsigned expected = 0, arrived = 0;
-    unsigned long generation = 0;
+    std::atomic<unsigned long> generation{0};
     void reset(unsigned n)
     {
+        std::lock_guard<std::mutex> lk(m);
         expected = n;
         arrived = 0;
     }
-    void release()
+    void release()   // with m held
     {
         arrived = 0;
-        ++generation;
-        cv.notify_all();
+        generation.fetch_add(1);
     }
+    // State changes under the mutex; the waiters spin on the generation.
     void arrive_and_wait()
     {
-        std::unique_lock<std::mutex> lk(m);
-        const unsigned long gen = generation;
-        if (++arrived == expected) {
-            release();
-            return;
+        unsigned long gen;
+        {
+            std::lock_guard<std::mutex> lk(m);
+            gen = generation.load();
+            if (++arrived == expected) {
+                release();
+                return;
+            }
         }
-        cv.wait(lk, [&] { return generation != gen; });
+        while (generation.load() == gen) std::this_thread::yield();
     }
     void drop()
     {
-        std::unique_lock<std::mutex> lk(m);
+        std::lock_guard<std::mutex> lk(m);
         --expected;
         if (expected > 0 && arrived == expected) release();
     }
@@ -187,35 +190,57 @@ template <class T> inline T __ldcg(const T *p)
     return *p;
 }
 
+inline ShimBarrier g_launch_barrier;   // between the blocks of one threaded launch
+
+inline void shim_begin_block(size_t smem_bytes, unsigned n)
+{
+    void *smem = nullptr;
+    if (smem_bytes && posix_memalign(&smem, 1024, smem_bytes) != 0) std::abort();
+    if (smem) std::memset(smem, 0xFF, smem_bytes);
+    g_dynamic_smem = static_cast<unsigned char *>(smem);
+    g_block_or.store(0);
+    g_block_barrier.reset(n);
+    for (unsigned w = 0; w < (n + 31) / 32; ++w) g_warp_barrier[w].reset(n - 32 * w < 32 ? n - 32 * w : 32);
+}
+
+inline void shim_end_block()
+{
+    std::free(g_dynamic_smem);
+    g_dynamic_smem = nullptr;
+}
+
+// One host thread per CUDA thread of a block; the same threads run the
+// launch's blocks one after another, meeting between blocks while one of
+// them sets up the next block's shared memory and barriers.
 template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_call, size_t smem_bytes = 0)
 {
     gridDim = grid;
     blockDim = block;
     const unsigned n = block.x * block.y * block.z;
-    for (unsigned bz = 0; bz < grid.z; ++bz)
-        for (unsigned by = 0; by < grid.y; ++by)
-            for (unsigned bx = 0; bx < grid.x; ++bx) {
-                void *smem = nullptr;
-                if (smem_bytes && posix_memalign(&smem, 1024, smem_bytes) != 0) std::abort();
-                if (smem) std::memset(smem, 0xFF, smem_bytes);
-                g_dynamic_smem = static_cast<unsigned char *>(smem);
-                g_block_or.store(0);
-                g_block_barrier.reset(n);
-                for (unsigned w = 0; w < (n + 31) / 32; ++w) g_warp_barrier[w].reset(n - 32 * w < 32 ? n - 32 * w : 32);
-                std::vector<std::thread> threads;
-                threads.reserve(n);
-                for (unsigned t = 0; t < n; ++t)
-                    threads.emplace_back([&, t, bx, by, bz] {
-                        blockIdx = dim3(bx, by, bz);
-                        threadIdx = dim3(t % block.x, (t / block.x) % block.y, t / (block.x * block.y));
-                        kernel_call();
-                        g_warp_barrier[t >> 5].drop();
-                        g_block_barrier.drop();
-                    });
-                for (auto &th : threads) th.join();
-                std::free(smem);
-                g_dynamic_smem = nullptr;
+    const unsigned long long nblocks = (unsigned long long)grid.x * grid.y * grid.z;
+    if (nblocks == 0 || n == 0) return;
+    g_launch_barrier.reset(n);
+    shim_begin_block(smem_bytes, n);
+    std::vector<std::thread> threads;
+    threads.reserve(n);
+    for (unsigned t = 0; t < n; ++t)
+        threads.emplace_back([&, t] {
+            for (unsigned long long b = 0; b < nblocks; ++b) {
+                blockIdx = dim3((unsigned)(b % grid.x), (unsigned)((b / grid.x) % grid.y),
+                                (unsigned)(b / ((unsigned long long)grid.x * grid.y)));
+                threadIdx = dim3(t % block.x, (t / block.x) % block.y, t / (block.x * block.y));
+                kernel_call();
+                g_warp_barrier[t >> 5].drop();
+                g_block_barrier.drop();
+                g_launch_barrier.arrive_and_wait();
+                if (t == 0) {
+                    shim_end_block();
+                    if (b + 1 < nblocks) shim_begin_block(smem_bytes, n);
+                }
+                g_launch_barrier.arrive_and_wait();
             }
+        });
+    for (auto &th : threads) th.join();
 }
 
 // The runtime calls the kernels' host launchers make.

@@ -150,3 +150,20 @@ def test_host_contracted_variants_within_bounds(host_stage_contracted, oracle, s
     for f in range(8):
         rel = np.abs(got[..., f] - want[..., f]).sum() / max(np.abs(want[..., f]).sum(), 1e-300)
         assert rel <= HOST_REL_L1[variant], (variant, f, rel)
+
+
+@pytest.mark.parametrize("shape", [0, 1])
+def test_host_stage_matches_reference_golden_outputs(host_stage, shape):
+    """The exact variant's host build against the committed outputs of the
+    reference library itself (tests/golden, from the reference built for the
+    host): states, dts and the total time, bit for bit."""
+    from conftest import GOLDEN_CASES, load_golden
+
+    assert GOLDEN_CASES
+    for name in GOLDEN_CASES:
+        s, init, final, dts, total_time = load_golden(name)
+        s.state = init
+        got, got_dts, crashed = run_host(host_stage, s, len(dts), shape)
+        assert crashed == -1, name
+        assert np.array_equal(got_dts, dts), name
+        assert np.array_equal(got, final), name
