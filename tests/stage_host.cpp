@@ -24,12 +24,14 @@ using namespace rmhd2d;
 
 extern "C" {
 
-// nsteps steps from the reference-layout state (updated in place; the
-// boundary is applied first), each step's dt in dts, with the stage kernels'
-// tile shape `shape`.  Returns 0, or 1 + the step whose output raised the
-// crash flag.
+// nsteps steps from the reference-layout state (updated in place; with
+// apply_boundary the boundary is applied first, as set_state does), each
+// step's dt in dts, with the stage kernels' tile shape `shape`.  With
+// fixed_dts the steps take those dts (rmhd2d_run_fixed_dt) instead of the
+// CFL dt.  Returns 0, or 1 + the step whose output raised the crash flag.
 int host_stage_run(int nx, int ny, double dx, double dy, double gamma, double cfl, double eps, double eta, int bc_x,
-                   int bc_y, const double *eta_table, int shape, double *state, int nsteps, double *dts)
+                   int bc_y, const double *eta_table, int shape, double *state, int nsteps, double *dts,
+                   int apply_boundary, const double *fixed_dts)
 {
     Grid g{};
     g.nx = nx;
@@ -61,12 +63,16 @@ int host_stage_run(int nx, int ny, double dx, double dy, double gamma, double cf
 
     Control ctl{};
     launch_aos_to_planes(g, state, A.data(), nullptr);
-    if (g.bc_x == BC_SYMMETRIC) launch_snapshot_row2(g, A.data(), row2.data(), nullptr);
-    launch_boundary(g, A.data(), row2.data(), nullptr, 0, nullptr);
+    if (apply_boundary) {
+        if (g.bc_x == BC_SYMMETRIC) launch_snapshot_row2(g, A.data(), row2.data(), nullptr);
+        launch_boundary(g, A.data(), row2.data(), nullptr, 0, nullptr);
+    }
     int parity = 0;
     launch_rate(g, A.data(), &ctl, parity, 1, nullptr);
     int rc = 0;
     for (int n = 0; n < nsteps; ++n) {
+        ctl.use_fixed_dt = fixed_dts ? 1 : 0;
+        if (fixed_dts) ctl.dt_fixed = fixed_dts[n];
         StageArgs a{};
         a.g = g;
         a.eta = ep;

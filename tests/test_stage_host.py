@@ -41,7 +41,7 @@ def build_stage(d: Path, extra: tuple[str, ...] = (), variant: str = "exact"):
                (EMU, f"-DSTAGE_VARIANT={variant}", *extra))
     D = ctypes.POINTER(ctypes.c_double)
     lib.host_stage_run.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 6 + [
-        ctypes.c_int, ctypes.c_int, D, ctypes.c_int, D, ctypes.c_int, D]
+        ctypes.c_int, ctypes.c_int, D, ctypes.c_int, D, ctypes.c_int, D, ctypes.c_int, D]
     lib.host_stage_run.restype = ctypes.c_int
     return lib
 
@@ -51,14 +51,16 @@ def host_stage(tmp_path_factory):
     return build_stage(tmp_path_factory.mktemp("stagehost"))
 
 
-def run_host(lib, s, nsteps, shape):
+def run_host(lib, s, nsteps, shape, apply_boundary=True, fixed_dts=None):
     D = ctypes.POINTER(ctypes.c_double)
     tab = None if s.eta_table is None else np.ascontiguousarray(s.eta_table, dtype=np.float64)
     state = np.ascontiguousarray(s.state, dtype=np.float64).copy()
     dts = np.zeros(max(nsteps, 1))
+    fixed = None if fixed_dts is None else np.ascontiguousarray(fixed_dts, dtype=np.float64)
     rc = lib.host_stage_run(s.nx, s.ny, s.dx, s.dy, s.gamma, s.cfl, s.eps, s.eta, BC[s.bc],
                             BC[s.bc_y] if s.bc_y else -1, None if tab is None else tab.ctypes.data_as(D), shape,
-                            state.ctypes.data_as(D), nsteps, dts.ctypes.data_as(D))
+                            state.ctypes.data_as(D), nsteps, dts.ctypes.data_as(D), int(apply_boundary),
+                            None if fixed is None else fixed.ctypes.data_as(D))
     assert rc != -1, "a tile's staging wait expired"
     return state, dts[:nsteps], rc - 1 if rc > 0 else -1
 
@@ -167,3 +169,29 @@ def test_host_stage_matches_reference_golden_outputs(host_stage, shape):
         assert crashed == -1, name
         assert np.array_equal(got_dts, dts), name
         assert np.array_equal(got, final), name
+
+
+def test_host_exact_reproduces_the_reference_nan_at_the_degenerate_face(host_stage):
+    """The plasmoid sheet's degenerate HLLD face (tests/test_degenerate_face.py):
+    one fixed-dt step of the window, no boundary first; the exact variant's
+    host build turns the same three cells non-finite as the reference's
+    arithmetic, and equals the oracle bit for bit at the centre."""
+    import test_degenerate_face as F
+
+    s, dt, bad = F._window()
+    want, _ = F._oracle_step()
+    got, _, _ = run_host(host_stage, s, 1, 0, apply_boundary=False, fixed_dts=[dt])
+    assert np.array_equal(got[F.CENTRE], want[F.CENTRE], equal_nan=True)
+    assert sorted(map(tuple, np.argwhere(~np.isfinite(got[..., 7])).tolist())) == sorted(bad)
+
+
+def test_host_contracted_variants_survive_the_degenerate_face(host_stage_contracted):
+    import test_degenerate_face as F
+
+    variant, lib = host_stage_contracted
+    s, dt, _ = F._window()
+    got, _, crashed = run_host(lib, s, 1, 0, apply_boundary=False, fixed_dts=[dt])
+    c = got[F.CENTRE]
+    assert crashed == -1 and np.isfinite(c).all(), variant
+    rel = np.abs(c[..., 7] - s.state[F.CENTRE][..., 7]) / np.abs(s.state[F.CENTRE][..., 7])
+    assert rel.max() < 1e-2, (variant, rel.max())
