@@ -17,7 +17,9 @@
 #pragma once
 
 #include <atomic>
+#include <chrono>
 #include <cmath>
+#include <functional>
 #include <condition_variable>
 #include <cstdint>
 #include <cstdlib>
@@ -51,7 +53,37 @@ typedef struct CUtensorMap_st {
     alignas(64) unsigned long long opaque[16];
 } CUtensorMap;
 
+// What the host build's tensor maps hold (written by cuTensorMapEncodeTiled
+// below or by the tests' drivers, read by tests/host_tma.cpp).
+struct HostMap {
+    const double *base;
+    unsigned long long dims[3];      // innermost first: j (ny), i (nx), field (8)
+    unsigned long long strides[2];   // bytes between consecutive i, between fields
+    unsigned box[3];                 // box extent per dimension
+    int rank;                        // 2 or 3
+};
+static_assert(sizeof(HostMap) <= sizeof(CUtensorMap), "a host map fits a tensor map's bytes");
+
+// Stream capture (cudaStreamBeginCapture .. EndCapture): launches and async
+// copies are recorded instead of run, and a graph launch runs the record.
+inline bool g_capturing = false;
+inline std::vector<std::function<void()>> *g_capture_ops = nullptr;
+inline bool shim_record(std::function<void()> op)
+{
+    if (!g_capturing) return false;
+    g_capture_ops->push_back(std::move(op));
+    return true;
+}
+
+template <class F> void host_launch_now(dim3 grid, dim3 block, F &kernel_call);
 template <class F> void host_launch(dim3 grid, dim3 block, F &&kernel_call)
+{
+    std::decay_t<F> call = kernel_call;
+    if (shim_record([=]() mutable { host_launch_now(grid, block, call); })) return;
+    host_launch_now(grid, block, call);
+}
+
+template <class F> void host_launch_now(dim3 grid, dim3 block, F &kernel_call)
 {
     gridDim = grid;
     blockDim = block;
@@ -212,7 +244,15 @@ inline void shim_end_block()
 // One host thread per CUDA thread of a block; the same threads run the
 // launch's blocks one after another, meeting between blocks while one of
 // them sets up the next block's shared memory and barriers.
+template <class F> void host_launch_threaded_now(dim3 grid, dim3 block, F &kernel_call, size_t smem_bytes);
 template <class F> void host_launch_threaded(dim3 grid, dim3 block, F &&kernel_call, size_t smem_bytes = 0)
+{
+    std::decay_t<F> call = kernel_call;
+    if (shim_record([=]() mutable { host_launch_threaded_now(grid, block, call, smem_bytes); })) return;
+    host_launch_threaded_now(grid, block, call, smem_bytes);
+}
+
+template <class F> void host_launch_threaded_now(dim3 grid, dim3 block, F &kernel_call, size_t smem_bytes)
 {
     gridDim = grid;
     blockDim = block;
@@ -250,12 +290,12 @@ enum cudaMemcpyKind { cudaMemcpyHostToHost, cudaMemcpyHostToDevice, cudaMemcpyDe
 inline cudaError_t cudaGetLastError() { return cudaSuccess; }
 inline cudaError_t cudaMemsetAsync(void *p, int v, size_t n, cudaStream_t = nullptr)
 {
-    std::memset(p, v, n);
+    if (!shim_record([=] { std::memset(p, v, n); })) std::memset(p, v, n);
     return cudaSuccess;
 }
 inline cudaError_t cudaMemcpyAsync(void *d, const void *s, size_t n, cudaMemcpyKind, cudaStream_t = nullptr)
 {
-    std::memcpy(d, s, n);
+    if (!shim_record([=] { std::memcpy(d, s, n); })) std::memcpy(d, s, n);
     return cudaSuccess;
 }
 inline cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
@@ -308,3 +348,5 @@ inline double __longlong_as_double(long long x)
     std::memcpy(&r, &x, sizeof r);
     return r;
 }
+
+#include "cuda_host_runtime.h"

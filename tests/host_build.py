@@ -35,8 +35,9 @@ def _split_top_level(s: str) -> list[str]:
 
 def rewrite_launches(src: str, threaded: tuple[str, ...] = ()) -> str:
     """`kernel<T><<<grid, block, smem, stream>>>(args)` -> host_launch(grid,
-    block, [&]() { kernel<T>(args); }); host_launch_threaded for the kernels
-    named in `threaded`."""
+    block, [=]() { kernel<T>(args); }); host_launch_threaded for the kernels
+    named in `threaded`.  The arguments are captured by value, as a launch
+    copies them, so a recorded launch (stream capture) replays with them."""
     out, pos = [], 0
     while True:
         k = src.find("<<<", pos)
@@ -71,9 +72,9 @@ def rewrite_launches(src: str, threaded: tuple[str, ...] = ()) -> str:
         out.append(src[pos:j])
         if name in threaded:
             smem = cfg[2] if len(cfg) > 2 else "0"
-            out.append(f"host_launch_threaded({cfg[0]}, {cfg[1]}, [&]() {{ {kernel}({src[e + 4:m]}); }}, {smem})")
+            out.append(f"host_launch_threaded({cfg[0]}, {cfg[1]}, [=]() {{ {kernel}({src[e + 4:m]}); }}, {smem})")
         else:
-            out.append(f"host_launch({cfg[0]}, {cfg[1]}, [&]() {{ {kernel}({src[e + 4:m]}); }})")
+            out.append(f"host_launch({cfg[0]}, {cfg[1]}, [=]() {{ {kernel}({src[e + 4:m]}); }})")
         pos = m + 1
     out.append(src[pos:])
     return "".join(out)
@@ -110,6 +111,7 @@ def shim_dir(d: Path) -> Path:
     """A directory whose cuda_runtime.h and cuda.h are the host shim."""
     (d / "cuda_runtime.h").write_text(f'#include "{HERE / "cuda_host_shim.h"}"\n')
     (d / "cuda.h").write_text(f'#include "{HERE / "cuda_host_shim.h"}"\n')
+    (d / "cudaTypedefs.h").write_text(f'#include "{HERE / "cuda_host_shim.h"}"\n')
     return d
 
 

@@ -89,8 +89,8 @@ def test_launch_rewrite_keeps_template_kernels_and_nested_arguments():
     src = ("  k1<<<dim3(f(n, 2), 2), T, 0, st>>>(a);\n"
            "  ytrans_kernel<BC_PERIODIC><<<g(x), 128, 0, st>>>(g, h(u, v));\n")
     out = rewrite_launches(src)
-    assert out == ("  host_launch(dim3(f(n, 2), 2), T, [&]() { k1(a); });\n"
-                   "  host_launch(g(x), 128, [&]() { ytrans_kernel<BC_PERIODIC>(g, h(u, v)); });\n")
+    assert out == ("  host_launch(dim3(f(n, 2), 2), T, [=]() { k1(a); });\n"
+                   "  host_launch(g(x), 128, [=]() { ytrans_kernel<BC_PERIODIC>(g, h(u, v)); });\n")
 
 
 @pytest.mark.parametrize("build", ["plain", "contracted"])
