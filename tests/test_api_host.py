@@ -128,3 +128,11 @@ def test_host_abi_gpu_parity_and_io_tests(on_host, oracle, tmp_path):
         for ct in ("stage1", "contact"):
             W.test_walls_match_oracle_bit_for_bit(None, oracle, bcx, bcy, ct)
     C.test_contact_refuses_batch_adjoint_and_profile(None)
+
+
+def test_host_abi_smoke(on_host, capsys):
+    """__graft_entry__.smoke(), run against the host build."""
+    import __graft_entry__ as entry
+
+    entry.smoke()
+    assert "smoke ok" in capsys.readouterr().out
