@@ -47,11 +47,27 @@ def tangent():
 
 
 @pytest.fixture(scope="session")
-def gpu():
-    """Skips nothing: a GPU test run without a usable B200 is a failure."""
+def gpu(request, tmp_path_factory):
+    """Skips nothing: a GPU test run without a usable B200 is a failure.
+
+    With RMHD_TESTS_ON_HOST_BUILD=1 the GPU tests run instead against the
+    host build of the whole C ABI (tests/host_build.py: build_host_abi),
+    bound to the Python mirror for the session: a check of the sources on a
+    machine without a GPU, not a measurement of the CUDA library.  Tests
+    that link librmhd2d.so into their own programs, or that need torch's
+    device memory, still need the GPU."""
     import ctypes
+    import os
 
     from resistivemhd_gpu_b200 import _lib
+
+    if os.environ.get("RMHD_TESTS_ON_HOST_BUILD") == "1":
+        from host_build import build_host_abi
+
+        mp = pytest.MonkeyPatch()
+        mp.setattr(_lib, "_lib", build_host_abi(tmp_path_factory.mktemp("abihost")))
+        request.addfinalizer(mp.undo)
+        return _lib._lib
 
     lib = _lib.load()
     cudart_ok = True

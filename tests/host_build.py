@@ -121,3 +121,44 @@ def link(d: Path, objs: list[str], sources: list[Path], name: str, flags: tuple[
                     "-I", str(CSRC), "-I", str(ORACLE), *objs, *[str(s) for s in sources], "-o", str(so), "-lpthread"],
                    check=True, capture_output=True)
     return ctypes.CDLL(str(so))
+
+
+EMU = "-DRMHD_HOST_EMULATION"
+THREADED = ("stage_kernel", "stage_batch_kernel", "kernel", "rate_kernel", "boundary_batch_kernel",
+            "dt_noalloc_kernel", "contact_flux_tiled_kernel")
+OFF = ["-ffp-contract=off"]
+CONTRACTED = ["-ffp-contract=fast", "-mfma"]
+# each unit with the contraction nvcc gives it (resistivemhd_gpu_b200/build.py)
+ABI_UNITS = {"api.cu": OFF, "stage_exact.cu": OFF, "stage_fast.cu": CONTRACTED, "stage_bulk32.cu": CONTRACTED,
+             "aux_kernels.cu": OFF, "noalloc_dt.cu": OFF, "adjoint_prep.cu": OFF, "contact.cu": OFF,
+             "adjoint.cu": CONTRACTED + ["-DRMHD_ADJ_HOST_RN"]}
+
+
+def has_fma() -> bool:
+    return " fma " in open("/proc/cpuinfo").read().replace("\n", " ")
+
+
+def build_host_abi(d: Path) -> ctypes.CDLL:
+    """Every unit of csrc/, api.cu included, built for the host into one
+    library with the C ABI's signatures set (tests/cuda_host_runtime.h
+    answers api.cu's runtime calls)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from resistivemhd_gpu_b200 import _lib
+
+    shim_dir(d)
+    # stage_impl.cuh is rewritten into d by each stage unit: write it once first
+    compile_unit(d, "stage_exact.cu", [*OFF, EMU, "-fsyntax-only"], threaded=THREADED, headers=("stage_impl.cuh",))
+
+    def unit(item):
+        u, f = item
+        return compile_unit(d, u, [*f, EMU], threaded=THREADED)
+
+    with ThreadPoolExecutor(max_workers=8) as pool:
+        objs = list(pool.map(unit, ABI_UNITS.items()))
+    lib = link(d, objs, [HERE / "host_tma.cpp"], "librmhd2d_host.so", (EMU,))
+    for name, res, args in _lib.SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib

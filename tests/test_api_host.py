@@ -7,53 +7,17 @@ on it: the drop-in's parity through the graph-replayed run and step paths,
 the checkpoint-interval and whole-trajectory invariances of the adjoint, its
 refusals, batches and autotuning, snapshots, walls and the CT-Contact
 step.  The product never loads this library."""
-from pathlib import Path
-
 import numpy as np
 import pytest
 
-from host_build import compile_unit, link, shim_dir
-
-HERE = Path(__file__).resolve().parent
-EMU = "-DRMHD_HOST_EMULATION"
-THREADED = ("stage_kernel", "stage_batch_kernel", "kernel", "rate_kernel", "boundary_batch_kernel",
-            "dt_noalloc_kernel", "contact_flux_tiled_kernel")
-OFF = ["-ffp-contract=off"]
-CONTRACTED = ["-ffp-contract=fast", "-mfma"]
-# each unit with the contraction nvcc gives it (resistivemhd_gpu_b200/build.py)
-UNITS = {"api.cu": OFF, "stage_exact.cu": OFF, "stage_fast.cu": CONTRACTED, "stage_bulk32.cu": CONTRACTED,
-         "aux_kernels.cu": OFF, "noalloc_dt.cu": OFF, "adjoint_prep.cu": OFF, "contact.cu": OFF,
-         "adjoint.cu": CONTRACTED + ["-DRMHD_ADJ_HOST_RN"]}
-
-
-def _has_fma() -> bool:
-    return " fma " in open("/proc/cpuinfo").read().replace("\n", " ")
+from host_build import build_host_abi, has_fma
 
 
 @pytest.fixture(scope="module")
 def host_abi(tmp_path_factory):
-    if not _has_fma():
+    if not has_fma():
         pytest.skip("the host has no fused multiply-add to model the device build with")
-    from concurrent.futures import ThreadPoolExecutor
-
-    from resistivemhd_gpu_b200 import _lib
-
-    d = shim_dir(tmp_path_factory.mktemp("abihost"))
-    # stage_impl.cuh is rewritten into d by each stage unit: write it once first
-    compile_unit(d, "stage_exact.cu", [*OFF, EMU, "-fsyntax-only"], threaded=THREADED, headers=("stage_impl.cuh",))
-
-    def unit(item):
-        u, f = item
-        return compile_unit(d, u, [*f, EMU], threaded=THREADED)
-
-    with ThreadPoolExecutor(max_workers=8) as pool:
-        objs = list(pool.map(unit, UNITS.items()))
-    lib = link(d, objs, [HERE / "host_tma.cpp"], "librmhd2d_host.so", (EMU,))
-    for name, res, args in _lib.SIGNATURES:
-        fn = getattr(lib, name)
-        fn.restype = res
-        fn.argtypes = args
-    return lib
+    return build_host_abi(tmp_path_factory.mktemp("abihost"))
 
 
 @pytest.fixture
