@@ -59,10 +59,16 @@ void mbar_init_tile(uint64_t *bar)
     new (bar + 1) std::atomic<long long>(0);
 }
 
+// One try polls for up to 2 ms, so the kernel's bound of 50,000 tries (about
+// a second on the device) becomes about 100 s here: loaded test machines
+// and sanitizer builds stay well inside it.
 bool mbar_try_wait(uint64_t *bar, uint32_t phase)
 {
-    if ((phases(bar).load() & 1ull) != phase) return true;
-    std::this_thread::sleep_for(std::chrono::microseconds(20));
+    const auto until = std::chrono::steady_clock::now() + std::chrono::milliseconds(2);
+    do {
+        if ((phases(bar).load() & 1ull) != phase) return true;
+        std::this_thread::yield();
+    } while (std::chrono::steady_clock::now() < until);
     return false;
 }
 
