@@ -138,10 +138,11 @@ def has_fma() -> bool:
     return " fma " in open("/proc/cpuinfo").read().replace("\n", " ")
 
 
-def build_host_abi(d: Path) -> ctypes.CDLL:
+def build_host_abi(d: Path, extra: tuple[str, ...] = ()) -> ctypes.CDLL:
     """Every unit of csrc/, api.cu included, built for the host into one
     library with the C ABI's signatures set (tests/cuda_host_runtime.h
-    answers api.cu's runtime calls)."""
+    answers api.cu's runtime calls); `extra` adds compiler flags to every
+    unit."""
     from concurrent.futures import ThreadPoolExecutor
 
     from resistivemhd_gpu_b200 import _lib
@@ -152,11 +153,11 @@ def build_host_abi(d: Path) -> ctypes.CDLL:
 
     def unit(item):
         u, f = item
-        return compile_unit(d, u, [*f, EMU], threaded=THREADED)
+        return compile_unit(d, u, [*f, EMU, *extra], threaded=THREADED)
 
     with ThreadPoolExecutor(max_workers=8) as pool:
         objs = list(pool.map(unit, ABI_UNITS.items()))
-    lib = link(d, objs, [HERE / "host_tma.cpp"], "librmhd2d_host.so", (EMU,))
+    lib = link(d, objs, [HERE / "host_tma.cpp"], "librmhd2d_host.so", (EMU, *extra))
     for name, res, args in _lib.SIGNATURES:
         fn = getattr(lib, name)
         fn.restype = res
