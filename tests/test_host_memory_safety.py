@@ -1,7 +1,7 @@
-"""Memory safety of kernel index arithmetic, checked on the CPU: the host
-builds of the adjoint, CT-Contact, ghost-fill/CFL and allocation-free dt
-kernels run under the address and undefined-behaviour sanitizers (tests/host_sanitized_run.py) in a child
-process that preloads the sanitizer runtime."""
+"""Memory safety on the CPU: the host build of the whole C ABI, every
+kernel and api.cu included, runs under the address and undefined-behaviour
+sanitizers (tests/host_sanitized_run.py) in a child process that preloads
+the sanitizer runtime."""
 import os
 import subprocess
 import sys
