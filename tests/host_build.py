@@ -80,7 +80,7 @@ def rewrite_launches(src: str, threaded: tuple[str, ...] = ()) -> str:
     return "".join(out)
 
 
-SANITIZE = ["-fsanitize=address,undefined", "-fno-omit-frame-pointer", "-fno-sanitize-recover=all"]
+SANITIZE = ["-O1", "-fsanitize=address,undefined", "-fno-omit-frame-pointer", "-fno-sanitize-recover=all"]
 
 
 def _rewrite(name: str, threaded: tuple[str, ...]) -> str:

@@ -6,8 +6,8 @@ through the Python mirror: every wall pairing of the stage-1-EMF step (in
 all three precisions on the diagonal pairings) and half of them with the
 CT-Contact step, on small ragged grids down to the smallest legal 6 x 6
 interior, the adjoint with checkpoints and with the
-whole trajectory kept on every periodic/symmetric pairing, and a batch with
-autotuning.  Any read or write outside an allocation, and any undefined
+whole trajectory kept on every periodic/symmetric pairing, a batch, and the
+batch and solver autotuners.  Any read or write outside an allocation, and any undefined
 behaviour, aborts the child: the kernels' index arithmetic and the ABI's
 buffer handling are checked against their buffers on the CPU.  Each exact
 run is also compared with the oracle.  Prints "ok" at the end."""
@@ -72,6 +72,8 @@ def main() -> None:
     with Batch([setups.random_smooth_state(9, 14, seed=8), setups.random_smooth_state(15, 7, seed=9)]) as b:
         b.run(3)
         b.autotune(2)
+    with Solver.from_setup(setups.random_smooth_state(10, 9, seed=10)) as sol:
+        sol.autotune(2)
     print("ok", flush=True)
 
 

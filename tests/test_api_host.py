@@ -67,9 +67,8 @@ def test_host_abi_gpu_batch_tests(on_host):
     import test_gpu_batch as B
 
     B.test_batch_odd_steps_and_graph_replay(None)
-    B.test_batch_autotune_restores_state(None)
     B.test_member_cannot_step_alone(None)
-    B.test_solver_autotune(None)
+    # (the batch and solver autotuners run in tests/host_sanitized_run.py)
 
 
 def test_host_abi_gpu_parity_and_io_tests(on_host, oracle, tmp_path):
