@@ -5,8 +5,7 @@ one library, which this module hands to the Python mirror in place of
 librmhd2d.so for its own tests only.  The GPU tests' own functions then run
 on it: the drop-in's parity through the graph-replayed run and step paths,
 the checkpoint-interval and whole-trajectory invariances of the adjoint, its
-refusals, batches and autotuning, snapshots, walls and the CT-Contact
-step.  The product never loads this library."""
+refusals, batches, snapshots, walls and the CT-Contact step.  The product never loads this library."""
 import numpy as np
 import pytest
 
