@@ -2,11 +2,15 @@
 """Benchmark of the B200 resistive-MHD RK2 step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64_fast|fp64_exact] [--workload harris|orszag_tang]
+                    [--precision fp64_exact|fp64_fast|fp32_bulk] [--workload harris|orszag_tang]
 
 Workload (default): the Harris current sheet, 2048 x 1024 interior cells,
 symmetric walls, uniform eta 1e-3 plus a Gaussian eta bump (cell-centred
-table), FP64 -- the configuration the headline metric is quoted on.  A
+table), FP64 -- the configuration the headline metric is quoted on.  The
+headline precision is fp64_exact, the drop-in: bit-identical to the
+reference's IEEE binary64 arithmetic.  fp64_fast (FMA contraction, shared
+reciprocals) and fp32_bulk are reported beside it with their relative L1
+against fp64_exact at the same dts.  A
 "step" is one full RK2 step (two fused stage kernels, two boundary fills,
 the CFL reduction for the next dt).  The state (2 x 135 MB) is larger than
 the 126 MB L2, so no L2 flush is needed between steps.
@@ -39,6 +43,10 @@ Extra blocks of the same JSON line (each can be switched off):
              steps) in one persistent batch in FP32-bulk, against the FP64
              path looped one run at a time; with N > 1 the runs are sharded
              over the ranks (no collective on the data path).
+  ref_gpu    the reference's own library built for sm_100a on the same GPU,
+             timed with CUDA events inside its driver, and the relative L1
+             of its final state against fp64_exact after the same steps.
+  summary    the figures above in a few keys, last in the line.
 
 --study harris|plasmoid replaces the benchmark with the long error study of
 FP32-bulk against FP64 at the same dts, beside an FP64 run that differs from
@@ -196,6 +204,15 @@ def cpu_model() -> str:
     return "unknown"
 
 
+def workload_config(setup, label: str, precision: str, world: int) -> dict:
+    """The config object of the JSON line, the same for both arms."""
+    return {"workload": label, "cells": setup.interior_cells, "nx": setup.nx, "ny": setup.ny, "bc": setup.bc,
+            "eta": "uniform 1e-3 + gaussian bump (cell-centred table)" if setup.eta_table is not None
+            else f"uniform {setup.eta}",
+            "precision": precision, "parallelism": f"replicas x{world}" if world > 1 else "single",
+            "l2": "inputs larger than L2 (2 x state = %.0f MB)" % (2 * setup.state.nbytes / 1e6)}
+
+
 def reference_arm(args, rank: int) -> None:
     if rank != 0:
         return
@@ -208,7 +225,7 @@ def reference_arm(args, rank: int) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": label, "cells": setup.interior_cells, "bc": setup.bc, "eta": "uniform + gaussian bump table"},
+        "config": workload_config(setup, label, args.precision, 1),
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
                          "sample": f"{label}: {args.warmup} warm-up + {args.steps} timed steps of the reference "
                                    f"library built for the host (Thrust OMP backend) on {threads} threads, "
@@ -314,11 +331,7 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if args.precision == "fp32_bulk" else "f64", "data": "synthetic",
-            "config": {"workload": label, "cells": cells, "nx": setup.nx, "ny": setup.ny, "bc": setup.bc,
-                       "eta": "uniform 1e-3 + gaussian bump (cell-centred table)" if setup.eta_table is not None
-                       else f"uniform {setup.eta}",
-                       "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (2 x state = %.0f MB)" % (2 * setup.state.nbytes / 1e6)},
+            "config": workload_config(setup, label, args.precision, world),
             "roofline": roofline,
             "clocks": clocks,
             "gpu_launches": gpu_launches,
@@ -341,13 +354,10 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
     sol.close()
 
     if rank == 0 and world == 1 and args.baselines:
-        # reference's own CUDA build on the same GPU (bounded sample)
+        # reference's own CUDA build on the same GPU (bounded sample), timed
+        # with CUDA events around its step loop inside the reference driver
         try:
-            info = run_reference_binary("gpu", setup, 2, min(args.steps, 10), None)
-            rv = cells * info["steps"] / info["seconds"]
-            line["ref_gpu"] = {"value": rv, "unit": METRIC, "speedup": value / rv,
-                               "sample": f"{label}: 2 warm-up + {info['steps']} steps of the reference library "
-                                         "built for sm_100a (oneStepRK2 + checkCalculationIsCrashed), wall clock"}
+            line["ref_gpu"] = ref_gpu_block(setup, label, value, local_rank)
         except Exception as e:  # reported, never fatal
             line["ref_gpu"] = {"unavailable": str(e)[:200]}
         # reference's own CPU build on the host cores (bounded sample)
@@ -372,7 +382,84 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
         if line is not None:
             line["ensemble"] = ens
     if line is not None:
+        line["summary"] = summary_of(line)
         print(json.dumps(line), flush=True)
+
+
+def summary_of(line: dict) -> dict:
+    """The figures of the extra blocks in a few keys, placed last in the
+    line so that they sit in the end of the output that a log tail keeps."""
+    out = {"headline_precision": line["config"]["precision"], "value": line["value"],
+           "ms_per_step": line["ms_per_step"], "roofline_frac": line["roofline"]["frac"]}
+    pr = line.get("precision")
+    if pr:
+        for prec in ("fp64_exact", "fp64_fast", "fp32_bulk"):
+            out[f"{prec}_value"] = pr[prec]["value"]
+            out[f"{prec}_ms_per_step"] = pr[prec]["ms_per_step"]
+            if "rel_l1" in pr[prec]:
+                out[f"{prec}_max_rel_l1_vs_exact"] = max(pr[prec]["rel_l1"][k] for k in ("rho", "p", "B"))
+        out["error_steps"] = pr.get("error_steps")
+        out["fp32_bulk_over_fp64_fast"] = pr["bulk_speedup_vs_fp64_fast"]
+        out["fp32_bulk_over_fp64_exact"] = pr["bulk_speedup_vs_fp64_exact"]
+    rg = line.get("ref_gpu")
+    if rg and "value" in rg:
+        out["ref_gpu_value"] = rg["value"]
+        out["speedup_vs_ref_gpu"] = rg["speedup"]
+        out["ref_gpu_vs_ref_host_max_rel_l1"] = rg.get("vs_fp64_exact_max_rel_l1")
+    cb = line.get("cpu_baseline")
+    if cb and "value" in cb:
+        out["cpu_baseline_value"] = cb["value"]
+    ad = line.get("adjoint")
+    if ad:
+        for prec in ("fp32_bulk", "fp64_exact", "fp32_bulk_whole_trajectory", "fp64_exact_whole_trajectory"):
+            if prec in ad and "adjoint_over_forward" in ad[prec]:
+                out[f"adjoint_over_forward_{prec}"] = ad[prec]["adjoint_over_forward"]
+        for key in ("fd", "fd_noisy_start", "fd_smooth_control"):
+            if key in ad and "frac_le_1e-6" in ad[key]:
+                out[f"adjoint_{key}_frac_le_1e-6"] = ad[key]["frac_le_1e-6"]
+    en = line.get("ensemble")
+    if en and "speedup_vs_loop_fp64" in en:
+        out["ensemble_value"] = en["batch_fp32_bulk"]["value"]
+        out["ensemble_speedup_vs_loop_fp64"] = en["speedup_vs_loop_fp64"]
+    ct = line.get("ct_contact")
+    if ct:
+        out["ct_contact_over_stage1_time"] = ct["contact_over_stage1_time"]
+    return out
+
+
+def ref_gpu_block(setup, label, value, local_rank, warmup=2, steps=20):
+    """The reference's own library built for sm_100a (nvcc -O3, contraction
+    on, as its example makefiles build it) on the same GPU: throughput from
+    CUDA events around its oneStepRK2 + checkCalculationIsCrashed loop, and
+    how far its final state lies from this library's FP64-exact step (the
+    reference's IEEE arithmetic without contraction) after the same steps."""
+    import numpy as np
+
+    from resistivemhd_gpu_b200 import Solver
+
+    ref_state, ref_dts, info = _reference_run("gpu", setup, warmup, steps)
+    secs = info["event_seconds"] if info.get("event_seconds", -1) > 0 else info["seconds"]
+    rv = setup.interior_cells * info["steps"] / secs
+    with Solver.from_setup(setup, precision="fp64_exact", device=local_rank) as sol:
+        for _ in range(len(ref_dts)):
+            sol.step()
+        ours = sol.get_state()
+    d_ref = _diagnostics(ref_state, setup.dx, setup.dy, setup.gamma)
+    d_our = _diagnostics(ours, setup.dx, setup.dy, setup.gamma)
+    err = {k: _rel_l1(d_ref[k], d_our[k]) for k in d_ref}
+    return {"value": rv, "unit": METRIC, "speedup": value / rv, "ms_per_step": 1e3 * secs / info["steps"],
+            "timing": "CUDA events on the legacy default stream around the timed steps",
+            "wall_ms_per_step": 1e3 * info["seconds"] / info["steps"],
+            "vs_fp64_exact_rel_l1": err, "vs_fp64_exact_max_rel_l1": max(err[k] for k in ("rho", "p", "B")),
+            "vs_fp64_exact_steps": len(ref_dts),
+            "sample": f"{label}: {warmup} warm-up + {info['steps']} steps of the reference library built for "
+                      "sm_100a (nvcc -O3, FMA contraction on; oneStepRK2 + checkCalculationIsCrashed)"}
+
+
+def _reference_run(kind, setup, warmup, steps, threads=None):
+    from oracle.oracle import run_reference
+
+    return run_reference(setup, setup.state, steps, n_warmup=warmup, kind=kind, threads=threads, timeout=3600)
 
 
 def _diagnostics(state, dx, dy, gamma):
@@ -397,10 +484,12 @@ def precision_block(args, setup, label, local_rank):
     """FP32-bulk against FP64 on the headline workload."""
     from resistivemhd_gpu_b200 import Solver
 
-    out = {"workload": label, "steps": args.steps, "error_reference": "fp64_exact at the same dts"}
+    nerr = max(args.steps, 100)
+    out = {"workload": label, "steps": args.steps, "error_steps": nerr,
+           "error_reference": f"fp64_exact at the same dts after {nerr} steps"}
     with Solver.from_setup(setup, precision="fp64_exact", device=local_rank) as ref:
         dts = []
-        for _ in range(args.steps):
+        for _ in range(nerr):
             ref.step()
             dts.append(ref.dt)
         ref_diag = _diagnostics(ref.get_state(), setup.dx, setup.dy, setup.gamma)
@@ -778,7 +867,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64_fast", "fp64_exact", "fp32_bulk"], default="fp64_fast")
+    ap.add_argument("--precision", choices=["fp64_fast", "fp64_exact", "fp32_bulk"], default="fp64_exact")
     ap.add_argument("--workload", choices=["harris", "orszag_tang"], default="harris")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-baselines", dest="baselines", action="store_false")

@@ -295,12 +295,14 @@ int rmhd2d_adjoint_release(rmhd2d_solver *s);
 
    Scratch is a fixed device array inside the library: grids with more than
    RMHD2D_NOALLOC_MAX_CELLS cells (nx*ny) are rejected with
-   RMHD2D_ERR_INVALID.  The first call on each device looks up that array's
-   address (cudaGetSymbolAddress), which loads the library's module onto
-   the device; make that first call before any stream capture, e.g. once
-   at initialisation.  All calls on one device share the array: calls that
-   overlap in time (from several host threads) race and may return a wrong
-   dt. */
+   RMHD2D_ERR_INVALID.  Every call looks up that array's address on the
+   device (cudaGetSymbolAddress, which allocates nothing); the first call on
+   a device also loads the library's module there, so make it once at
+   initialisation, before any stream capture.  The function may not be
+   called while cfg->stream is being captured (it synchronises that
+   stream): it then returns RMHD2D_ERR_STATE and enqueues nothing.  All
+   calls on one device share the array: calls that overlap in time (from
+   several host threads) race and may return a wrong dt. */
 #define RMHD2D_NOALLOC_MAX_CELLS 16777216
 int rmhd2d_calculate_dt_noalloc(const rmhd2d_config *cfg, const double *device_state, double *dt);
 

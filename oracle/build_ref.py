@@ -15,6 +15,13 @@ together with the project-written driver ``oracle/ref_driver.cu``:
   compiler on stdin; nothing of the reference is written to disk.  No
   arithmetic is edited.
 
+* ``oracle/_ref/mc_host`` -- the CT-Contact and wall parts of the multi-GPU
+  library (ResistiveMHD_multiGPU_cuda/ResistiveMHD2D_GPU: const.cu, ct.cu,
+  boundary.cu, mpi.cu, sign.cu), unmodified, with the project-written driver
+  ``oracle/mc_driver.cu``, built the same way for the host on one rank: its
+  ``#include <mpi.h>`` (mpi.hpp) finds the single-rank stand-in
+  ``oracle/mpi_stub/mpi.h`` first on the include path.
+
 Outputs go only to ``oracle/_ref/`` (git-ignored; it travels to the GPU box).
 When the reference tree is absent (the GPU box) nothing is built.
 """
@@ -101,6 +108,52 @@ def _cpu_objects(name: str, libdir: Path, objdir: Path, pool) -> list:
     return jobs
 
 
+MC_LIB = "ResistiveMHD_multiGPU_cuda/ResistiveMHD2D_GPU"
+MC_SOURCES = ("const.cu", "ct.cu", "boundary.cu", "mpi.cu", "sign.cu")
+
+
+def mc_binary() -> Path:
+    return OUT / "mc_host"
+
+
+def build_mc(verbose=True) -> bool:
+    """Build oracle/_ref/mc_host; returns False when the reference is absent."""
+    libdir = REF_ROOT / MC_LIB
+    if not libdir.is_dir():
+        return False
+    OUT.mkdir(parents=True, exist_ok=True)
+    target = mc_binary()
+    deps = [libdir / f for f in MC_SOURCES] + list(libdir.glob("*.hpp")) + [
+        HERE / f for f in ("mc_driver.cu", "ref_host_shim.h", "build_ref.py")] + [HERE / "mpi_stub" / "mpi.h"]
+    if target.exists() and target.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
+        return True
+    objdir = OUT / "obj_mc"
+    objdir.mkdir(parents=True, exist_ok=True)
+    common = ["g++", "-O3", "-fopenmp", "-std=c++17", "-DTHRUST_DEVICE_SYSTEM=THRUST_DEVICE_SYSTEM_OMP",
+              "-DREF_HOST_BUILD", "-include", str(HERE / "ref_host_shim.h"), "-I", str(HERE / "mpi_stub"),
+              "-I", str(libdir), "-I", CUDA_INC, "-w"]
+    shim_defs = ("thread_local ref_uint3 blockIdx; thread_local ref_uint3 threadIdx; "
+                 "thread_local dim3 blockDim; thread_local dim3 gridDim;\n")
+    objs = []
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        jobs = []
+        for name in MC_SOURCES:
+            obj = objdir / (Path(name).stem + ".o")
+            text = rewrite_launches((libdir / name).read_text())
+            jobs.append((obj, pool.submit(_run, common + ["-x", "c++", "-c", "-", "-o", str(obj)], text)))
+        obj = objdir / "mc_driver.o"
+        text = rewrite_launches((HERE / "mc_driver.cu").read_text()) + "\n" + shim_defs
+        jobs.append((obj, pool.submit(_run, common + ["-x", "c++", "-c", "-", "-o", str(obj)], text)))
+        for obj, fut in jobs:
+            fut.result()
+            objs.append(str(obj))
+    _run(["g++", "-O3", "-fopenmp", *objs, "-o", str(target)])
+    shutil.rmtree(objdir, ignore_errors=True)
+    if verbose:
+        print(f"[build_ref] built {target.relative_to(HERE.parent)}", file=sys.stderr)
+    return True
+
+
 def build(which=("gpu", "cpu"), verbose=True) -> bool:
     """Build the reference binaries; returns False when the reference is absent."""
     if not REF_ROOT.is_dir():
@@ -139,5 +192,7 @@ def build(which=("gpu", "cpu"), verbose=True) -> bool:
 
 
 if __name__ == "__main__":
-    kinds = tuple(sys.argv[1:]) or ("gpu", "cpu")
-    build(kinds)
+    kinds = tuple(sys.argv[1:]) or ("gpu", "cpu", "mc")
+    build(tuple(k for k in kinds if k != "mc"))
+    if "mc" in kinds:
+        build_mc()

@@ -5,6 +5,9 @@
 * ``run_reference`` -- runs the reference's own step built by
   ``oracle/build_ref.py`` (``oracle/_ref/ref_{cpu,gpu}_{periodic,symmetric}``)
   on a state and returns the final state, the per-step dt and the timing.
+* ``run_mc_boundary`` / ``run_mc_ct`` -- run the multi-GPU library's own wall
+  functions and CT-Contact closing CT (``oracle/_ref/mc_host``) on given
+  inputs.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline and
 reference legs may import this module.
@@ -135,6 +138,9 @@ class OracleLib:
         self.lib.orc_run.restype = ctypes.c_int
         self.lib.orc_run_keep_stages.argtypes = [P, D, ctypes.c_int, D, D, D]
         self.lib.orc_run_keep_stages.restype = ctypes.c_int
+        self.lib.orc_contact_ct_work_doubles.argtypes = [ctypes.c_int, ctypes.c_int]
+        self.lib.orc_contact_ct_work_doubles.restype = ctypes.c_size_t
+        self.lib.orc_contact_ct.argtypes = [P, D, D, D, D, D, D, D, ctypes.c_double, D, D]
 
     @staticmethod
     def _params(setup, eta_keep):
@@ -153,6 +159,20 @@ class OracleLib:
         p = self._params(setup, keep)
         out = np.ascontiguousarray(state, dtype=np.float64).copy()
         self.lib.orc_boundary(ctypes.byref(p), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
+    def contact_ct(self, setup, u_old, f_old, g_old, u_now, f_now, g_now, bx_old, by_old, dt: float) -> np.ndarray:
+        """The closing CT of the CT-Contact step on given inputs
+        (orc_contact_ct): returns u_now with its face B replaced."""
+        keep = []
+        p = self._params(setup, keep)
+        D = ctypes.POINTER(ctypes.c_double)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u_old, f_old, g_old, f_now, g_now, bx_old,
+                                                                    by_old)]
+        out = np.ascontiguousarray(u_now, dtype=np.float64).copy()
+        work = np.empty(self.lib.orc_contact_ct_work_doubles(setup.nx, setup.ny), dtype=np.float64)
+        self.lib.orc_contact_ct(ctypes.byref(p), *[a.ctypes.data_as(D) for a in arrs], float(dt),
+                                out.ctypes.data_as(D), work.ctypes.data_as(D))
         return out
 
     def calc_dt(self, setup, state: np.ndarray) -> float:
@@ -202,6 +222,59 @@ class OracleLib:
 
 def reference_binary(kind: str, bc: str) -> Path:
     return REF_DIR / f"ref_{kind}_{bc}"
+
+
+MC_BINARY = REF_DIR / "mc_host"
+# wall pairs of the multi-GPU library's step variants, as (x wall, y wall) of
+# this project's configuration; the library's symmetricBoundaryY2nd is the
+# zero-gradient copy
+MC_PAIRS = {"periodic_periodic": ("periodic", "periodic"), "periodic_wall": ("periodic", "wall"),
+            "periodic_zerogradient": ("periodic", "zero_gradient"), "flare_wall": ("flare", "wall")}
+
+
+def _mc_env(setup, dt: float = 0.0) -> dict:
+    env = dict(os.environ)
+    env.update({"REF_NX": str(setup.nx), "REF_NY": str(setup.ny), "REF_DX": repr(setup.dx),
+                "REF_DY": repr(setup.dy), "REF_GAMMA": repr(setup.gamma), "REF_EPS": repr(setup.eps),
+                "REF_ETA": repr(setup.eta), "MC_DT": repr(float(dt)), "OMP_NUM_THREADS": "1"})
+    return env
+
+
+def run_mc_boundary(setup, state: np.ndarray, pair: str) -> np.ndarray:
+    """The multi-GPU library's own ghost fill for a wall pair (sendrecv_U on
+    one rank, then its x and y wall functions), built by build_ref.build_mc."""
+    if not MC_BINARY.exists():
+        raise FileNotFoundError(f"{MC_BINARY} not built (oracle/build_ref.py mc)")
+    with tempfile.TemporaryDirectory(dir=os.environ.get("RMHD_TMPDIR")) as td:
+        td = Path(td)
+        np.ascontiguousarray(state, dtype=np.float64).tofile(td / "in.bin")
+        r = subprocess.run([str(MC_BINARY), "boundary", pair, str(td / "in.bin"), str(td / "out.bin")],
+                           env=_mc_env(setup), capture_output=True, text=True, timeout=600)
+        if r.returncode != 0:
+            raise RuntimeError(f"mc_host boundary failed ({r.returncode}): {r.stderr[-2000:]}")
+        return np.fromfile(td / "out.bin", dtype=np.float64).reshape(state.shape)
+
+
+def run_mc_ct(setup, u_old, f_old, g_old, u_now, f_now, g_now, bx_old, by_old, dt: float) -> np.ndarray:
+    """The multi-GPU library's own CT-Contact closing CT (CT::setOldFlux2D,
+    CT::setNowFlux2D, CT::divBClean) on given inputs; returns u_now with the
+    face B it writes."""
+    if not MC_BINARY.exists():
+        raise FileNotFoundError(f"{MC_BINARY} not built (oracle/build_ref.py mc)")
+    with tempfile.TemporaryDirectory(dir=os.environ.get("RMHD_TMPDIR")) as td:
+        td = Path(td)
+        for name, a in (("u_old", u_old), ("f_old", f_old), ("g_old", g_old), ("u_now", u_now), ("f_now", f_now),
+                        ("g_now", g_now), ("bx_old", bx_old), ("by_old", by_old)):
+            np.ascontiguousarray(a, dtype=np.float64).tofile(td / name)
+        env = _mc_env(setup, dt)
+        if setup.eta_table is not None:
+            np.ascontiguousarray(setup.eta_table, dtype=np.float64).tofile(td / "eta.bin")
+            env["REF_ETA_TABLE"] = str(td / "eta.bin")
+        r = subprocess.run([str(MC_BINARY), "ct", str(td), str(td / "out.bin")], env=env, capture_output=True,
+                           text=True, timeout=600)
+        if r.returncode != 0:
+            raise RuntimeError(f"mc_host ct failed ({r.returncode}): {r.stderr[-2000:]}")
+        return np.fromfile(td / "out.bin", dtype=np.float64).reshape(np.shape(u_now))
 
 
 def run_reference(setup, state: np.ndarray, n_timed: int, n_warmup: int = 0, kind: str = "cpu",

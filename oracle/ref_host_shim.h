@@ -11,11 +11,13 @@
 //     nor __syncthreads, and no thread reads what another thread of the same
 //     kernel writes),
 //   * cudaMemcpyToSymbol as memcpy and cudaDeviceSynchronize as a no-op,
+//   * cudaMalloc / cudaMemcpy on host memory,
 //   * the CUDA host overloads min(double,double) / max(double,double).
 #ifndef REF_HOST_SHIM_H
 #define REF_HOST_SHIM_H
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <math.h>
 
@@ -67,6 +69,20 @@ static void host_launch(int g, int b, F body)
 
 #define cudaMemcpyToSymbol(sym, src, n) std::memcpy(&(sym), (src), (n))
 static inline int cudaDeviceSynchronize() { return 0; }
+
+// device memory is host memory (the multi-GPU library's Boundary copies its
+// MPIInfo to the device, ResistiveMHD2D_GPU/boundary.cu:4-11)
+enum ref_memcpy_kind { cudaMemcpyHostToHost, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice };
+template <class T> static inline int cudaMalloc(T **p, size_t n)
+{
+    *p = static_cast<T *>(std::malloc(n));
+    return *p ? 0 : 2;
+}
+static inline int cudaMemcpy(void *dst, const void *src, size_t n, ref_memcpy_kind)
+{
+    std::memcpy(dst, src, n);
+    return 0;
+}
 
 static inline double min(double a, double b) { return fmin(a, b); }
 static inline double max(double a, double b) { return fmax(a, b); }

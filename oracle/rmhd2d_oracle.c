@@ -815,6 +815,27 @@ static double contact_corner(int index, int ny, const double *NF5, const double 
     return avg + 0.125 * (eS - eN + eW - eE);
 }
 
+/* Corner EMFs of the CT-Contact step (ct.cu:124-200 getEZVector_kernel):
+   the mean of the two stages' contact EMFs at every corner (i+1/2, j+1/2)
+   with i < nx-1, j < ny-1; NaN elsewhere.  o and n point to the six
+   per-cell input planes of each stage (NF5, NG4, CF5, CG4, NF0, NG0 in a row
+   of nx*ny doubles each). */
+static void contact_ez(const orc_params *p, const double *o, const double *n, double *Ez)
+{
+    const int nx = p->nx, ny = p->ny, N = nx * ny;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const int index = j + i * ny;
+            if (i < nx - 1 && j < ny - 1) {
+                double eOld = contact_corner(index, ny, o, o + N, o + 2 * N, o + 3 * N, o + 4 * N, o + 5 * N);
+                double eNow = contact_corner(index, ny, n, n + N, n + 2 * N, n + 3 * N, n + 4 * N, n + 5 * N);
+                Ez[index] = 0.5 * (eOld + eNow);
+            } else {
+                Ez[index] = NAN;
+            }
+        }
+}
+
 /* The step with the CT-Contact EMF of the multi-GPU library
    (ResistiveMHD2D_GPU/resistiveMHD2D.cu:147-221 oneStepRK2 ordering,
    ct.cu:26-257): both stages update B by flux differences like every other
@@ -881,21 +902,35 @@ double orc_step_contact(const orc_params *p, double *U, double *work)
     }
     orc_boundary(p, U);
     contact_set_flux(p, F, G, U, nNF5, nNG4, nCF5, nCG4, nNF0, nNG0);
-
-    for (int i = 0; i < nx; ++i)
-        for (int j = 0; j < ny; ++j) {
-            const int index = j + i * ny;
-            if (i < nx - 1 && j < ny - 1) {
-                double eOld = contact_corner(index, ny, oNF5, oNG4, oCF5, oCG4, oNF0, oNG0);
-                double eNow = contact_corner(index, ny, nNF5, nNG4, nCF5, nCG4, nNF0, nNG0);
-                Ez[index] = 0.5 * (eOld + eNow);
-            } else {
-                Ez[index] = NAN;
-            }
-        }
+    contact_ez(p, oNF5, nNF5, Ez);
     ct_update(p, bXOld, bYOld, Ez, dt, U);
     orc_boundary(p, U);
     return dt;
+}
+
+size_t orc_contact_ct_work_doubles(int nx, int ny) { return (size_t)13 * nx * ny; }
+
+/* The closing constrained transport of the CT-Contact step on given inputs:
+   the contact inputs of the first stage from (Fold, Gold, Uold), those of
+   the second from (Fnow, Gnow, U), the corner EMF 0.5 (eOld + eNow), and the
+   CT of U's face B from bXOld, bYOld with dt, in place in U (which holds the
+   second stage's state on entry).  This is the composition
+   CT::setOldFlux2D, CT::setNowFlux2D, CT::divBClean of the multi-GPU library
+   (ResistiveMHD2D_GPU/ct.cu:26-257, called at resistiveMHD2D.cu:177,212-214)
+   that orc_step_contact ends with; exposed so that it can be checked against
+   that library's own code. */
+void orc_contact_ct(const orc_params *p, const double *Uold, const double *Fold, const double *Gold,
+                    const double *Fnow, const double *Gnow, const double *bXOld, const double *bYOld, double dt,
+                    double *U, double *work)
+{
+    const int N = p->nx * p->ny;
+    double *Ez = work;
+    double *oNF5 = Ez + N, *oNG4 = oNF5 + N, *oCF5 = oNG4 + N, *oCG4 = oCF5 + N, *oNF0 = oCG4 + N, *oNG0 = oNF0 + N;
+    double *nNF5 = oNG0 + N, *nNG4 = nNF5 + N, *nCF5 = nNG4 + N, *nCG4 = nCF5 + N, *nNF0 = nCG4 + N, *nNG0 = nNF0 + N;
+    contact_set_flux(p, Fold, Gold, Uold, oNF5, oNG4, oCF5, oCG4, oNF0, oNG0);
+    contact_set_flux(p, Fnow, Gnow, U, nNF5, nNG4, nCF5, nCG4, nNF0, nNG0);
+    contact_ez(p, oNF5, nNF5, Ez);
+    ct_update(p, bXOld, bYOld, Ez, dt, U);
 }
 
 /* Runs nsteps steps; dts (may be NULL) receives each step's dt.  Returns 0,

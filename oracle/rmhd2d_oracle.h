@@ -34,6 +34,10 @@ void orc_boundary(const orc_params *p, double *U);
 size_t orc_work_doubles(int nx, int ny);
 double orc_step(const orc_params *p, double *U, double *work);
 double orc_step_contact(const orc_params *p, double *U, double *work);
+size_t orc_contact_ct_work_doubles(int nx, int ny);
+void orc_contact_ct(const orc_params *p, const double *Uold, const double *Fold, const double *Gold,
+                    const double *Fnow, const double *Gnow, const double *bXOld, const double *bYOld, double dt,
+                    double *U, double *work);
 int orc_run(const orc_params *p, double *U, int nsteps, double *dts);
 int orc_run_keep_stages(const orc_params *p, double *U, int nsteps, double *dts, double *Un, double *Ustar);
 

@@ -1275,9 +1275,17 @@ int rmhd2d_calculate_dt_noalloc(const rmhd2d_config *cfg, const double *device_s
     CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, cfg->device));
     CK(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, cfg->device));
     if (major != 10 || minor != 0) return fail(s, RMHD2D_ERR_NO_DEVICE, "librmhd2d is built for sm_100a (B200) only");
-    unsigned long long *scratch = nullptr;
-    CK(noalloc_scratch(cfg->device, &scratch));
     const cudaStream_t st = static_cast<cudaStream_t>(cfg->stream);
+    // The call ends with a synchronisation of its stream, which a capture
+    // would turn into an error that invalidates the caller's whole graph:
+    // refuse before enqueuing anything.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(s, RMHD2D_ERR_STATE, "rmhd2d_calculate_dt_noalloc: cfg->stream is being captured; the call "
+                                         "synchronises its stream and cannot be captured");
+    unsigned long long *scratch = nullptr;
+    CK(noalloc_scratch(&scratch));
     double out = 0.0;
     CK(enqueue_dt_noalloc(device_state, ncell, cfg->gamma_mhd, cfg->dx, cfg->dy, cfg->eps, cfg->eta, cfg->cfl,
                           scratch, &out, st));

@@ -21,8 +21,6 @@
 // race.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "../../include/rmhd2d.h"
 #include "noalloc_dt.h"
 #include "physics.cuh"
@@ -41,8 +39,6 @@ constexpr int W_RESULT = NA_MAX_BLOCKS + 2;
 constexpr int NA_WORDS = NA_MAX_BLOCKS + 32;   // 256-byte multiple
 static_assert(RMHD2D_NOALLOC_MAX_CELLS % NA_CELLS_PER_BLOCK == 0, "limit must be whole blocks");
 static_assert((NA_WORDS * 8) % 256 == 0, "scratch is a 256-byte multiple");
-
-constexpr int NA_MAX_DEVICES = 64;
 
 }  // namespace
 
@@ -111,22 +107,18 @@ __global__ void __launch_bounds__(NA_THREADS) dt_noalloc_kernel(const double *__
     }
 }
 
-std::mutex g_scratch_mu;
-unsigned long long *g_scratch_ptr[NA_MAX_DEVICES] = {};
-
 }  // namespace
 
-cudaError_t noalloc_scratch(int device, unsigned long long **ptr)
+cudaError_t noalloc_scratch(unsigned long long **ptr)
 {
-    if (device < 0 || device >= NA_MAX_DEVICES) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_ptr[device]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_dt_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[device] = static_cast<unsigned long long *>(p);
-    }
-    *ptr = g_scratch_ptr[device];
+    // Looked up on every call, not cached: the address belongs to the
+    // module loaded into the current context, and a context reset
+    // (cudaDeviceReset) loads the module again at another address.  The
+    // lookup allocates nothing.
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_dt_scratch);
+    if (e != cudaSuccess) return e;
+    *ptr = static_cast<unsigned long long *>(p);
     return cudaSuccess;
 }
 

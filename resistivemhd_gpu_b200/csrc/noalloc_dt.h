@@ -5,10 +5,10 @@
 
 namespace rmhd2d {
 
-// Device address of the file-scope scratch array on `device`, looked up with
-// cudaGetSymbolAddress the first time (that device must be current) and
-// cached per device afterwards.
-cudaError_t noalloc_scratch(int device, unsigned long long **ptr);
+// Device address of the file-scope scratch array on the current device,
+// looked up with cudaGetSymbolAddress on every call (no cache that a context
+// reset could leave dangling).
+cudaError_t noalloc_scratch(unsigned long long **ptr);
 
 // Enqueues on `st`: the clear of the completion counter, the reduction over
 // ncell cells of the array-of-structures state `aos`, and the copy of the dt

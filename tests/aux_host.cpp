@@ -71,7 +71,7 @@ int host_dt_noalloc(int nx, int ny, double dx, double dy, double gamma, double c
                     const double *state, double *dt)
 {
     unsigned long long *scratch = nullptr;
-    if (noalloc_scratch(0, &scratch) != cudaSuccess) return 1;
+    if (noalloc_scratch(&scratch) != cudaSuccess) return 1;
     double out = 0.0;
     if (enqueue_dt_noalloc(state, (long long)nx * ny, gamma, dx, dy, eps, eta, cfl, scratch, &out, nullptr) !=
         cudaSuccess)
