@@ -105,6 +105,108 @@ __device__ __forceinline__ double rcp_nr(double a)
     return r;
 }
 
+// ---- correctly rounded division through a shared reciprocal ----
+//
+// An IEEE division costs about as much FP64 issue as 14 fused multiply-adds
+// on sm_100.  The exact variant divides by the same denominator several
+// times per interface, so it divides through the correctly rounded
+// reciprocal y = RN(1/b) instead, with Markstein's correction (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990; Theorem 4.10 of Muller et al.,
+// Handbook of Floating-Point Arithmetic): with q = RN(a y) within one ulp of
+// a/b, the remainder r = a - b q is exact in one fma and RN(q + r y) =
+// RN(a/b), as long as nothing overflows or underflows.
+//
+// y comes from the hardware seed by two Newton steps (each squares the
+// relative error, leaving y within an ulp of 1/b) and Markstein's last
+// step y + y (1 - b y), which rounds correctly except for significands of b
+// that are all ones.  The guard of MdDiv records every operand outside the
+// range where all of this holds -- a divisor outside [2^-400, 2^400) or with
+// an all-ones significand, a quotient outside [2^-500, 2^500) unless the
+// dividend is zero -- and the caller then repeats the computation with IEEE
+// division.  A zero dividend returns q itself, which carries the sign
+// IEEE division gives (q + r y would turn -0 into +0).
+//
+// tests/test_division.py checks both against IEEE division on random and
+// special operands (on the CPU for this algorithm, on the GPU for the
+// hardware seed).
+__device__ __forceinline__ double rcp_rn_md(double b)
+{
+    double y;
+#if defined(RMHD_HOST_EMULATION)
+    // a seed with the precision of the hardware's (its low 28 significand
+    // bits cleared), so that a host build exercises the refinement
+    {
+        unsigned long long u;
+        const double r = 1.0 / b;
+        memcpy(&u, &r, sizeof(u));
+        u &= ~((1ull << 28) - 1);
+        memcpy(&y, &u, sizeof(y));
+    }
+#else
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+#endif
+    double e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-b, y, 1.0);
+    return fma(y, e, y);
+}
+
+__host__ __device__ __forceinline__ unsigned int hi_word(double x)
+{
+#ifdef __CUDA_ARCH__
+    return (unsigned int)__double2hiint(x);
+#else
+    unsigned long long u;
+    memcpy(&u, &x, sizeof(u));
+    return (unsigned int)(u >> 32);
+#endif
+}
+__host__ __device__ __forceinline__ unsigned int lo_word(double x)
+{
+#ifdef __CUDA_ARCH__
+    return (unsigned int)__double2loint(x);
+#else
+    unsigned long long u;
+    memcpy(&u, &x, sizeof(u));
+    return (unsigned int)u;
+#endif
+}
+
+// Division policy of the exact arithmetic: shared reciprocals with the
+// guard above.  recip(b) returns y; div(a, b, y) returns RN(a/b) whenever ok
+// stays true.
+struct MdDiv {
+    bool ok = true;
+    __device__ __forceinline__ double recip(double b)
+    {
+        const unsigned int h = hi_word(b);
+        // |b| in [2^-400, 2^400): biased exponent in [623, 1423)
+        ok &= ((h & 0x7FFFFFFFu) - 0x26F00000u) < 0x32000000u;
+        ok &= ((h & 0x000FFFFFu) != 0x000FFFFFu) | (lo_word(b) != 0xFFFFFFFFu);
+        return rcp_rn_md(b);
+    }
+    __device__ __forceinline__ double div(double a, double b, double y)
+    {
+        const double q = a * y;
+        const double r = fma(-q, b, a);
+        const double q1 = fma(r, y, q);
+        const bool z = a == 0.0;
+        // |q| in [2^-500, 2^500): biased exponent in [523, 1523)
+        ok &= z | (((hi_word(q) & 0x7FFFFFFFu) - 0x20B00000u) < 0x3E800000u);
+        return z ? q : q1;
+    }
+};
+
+// Division policy with plain IEEE division (the fallback of MdDiv).
+struct IeeeDiv {
+    static constexpr bool ok = true;
+    __device__ __forceinline__ double recip(double b) { return b; }
+    __device__ __forceinline__ double div(double a, double b, double) { return a / b; }
+};
+
 // Interface state fed to HLLD: BasicParameter (basic_parameter_struct.hpp:5-27).
 template <typename T> struct PrimT {
     T rho, u, v, w, bX, bY, bZ, p;
@@ -144,7 +246,10 @@ __device__ __forceinline__ void add_weighted_flux(double rho, double u, double v
 
 // HLLD flux through one interface: hlld.cu:256-432
 // (calculateHLLDParameterFunctor), hlld.cu:469-549 (setFluxFunctor) and
-// hlld.cu:35-107 (CalculateFluxFunctor).
+// hlld.cu:35-107 (CalculateFluxFunctor), with the divisions of the policy
+// Div (MdDiv: shared correctly rounded reciprocals; IeeeDiv: plain division);
+// both give the reference's quotients bit for bit while Div::ok holds.
+// ygm1 is Div's reciprocal handle of gm - 1.
 //
 // ALL_CANDIDATES = true gives the bits of the reference's sum of all six
 // candidate fluxes with 0/1 indicator weights for every input, including
@@ -153,31 +258,33 @@ __device__ __forceinline__ void add_weighted_flux(double rho, double u, double v
 // same bits.  ALL_CANDIDATES = false forms only the candidates whose
 // indicator is 1 and adds them in the reference's order, which gives the same
 // bits whenever all six candidates are finite.
-template <bool ALL_CANDIDATES>
-__device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double gm, double EPS,
+template <bool ALL_CANDIDATES, class Div>
+__device__ __forceinline__ void hlld_body(const Prim &L, const Prim &R, double gm, double EPS, double ygm1, Div &dv,
                                           double f[8])
 {
     const double rhoL = L.rho, uL = L.u, vL = L.v, wL = L.w, bXL = L.bX, bYL = L.bY, bZL = L.bZ, pL = L.p;
     const double rhoR = R.rho, uR = R.u, vR = R.v, wR = R.w, bXR = R.bX, bYR = R.bY, bZR = R.bZ, pR = R.p;
+    const double gm1 = gm - 1.0;
 
-    const double eL = pL / (gm - 1.0)
+    const double eL = dv.div(pL, gm1, ygm1)
                     + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL)
                     + 0.5 * (bXL * bXL + bYL * bYL + bZL * bZL);
     const double pTL = pL + 0.5 * (bXL * bXL + bYL * bYL + bZL * bZL);
-    const double eR = pR / (gm - 1.0)
+    const double eR = dv.div(pR, gm1, ygm1)
                     + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR)
                     + 0.5 * (bXR * bXR + bYR * bYR + bZR * bZR);
     const double pTR = pR + 0.5 * (bXR * bXR + bYR * bYR + bZR * bZR);
 
-    const double csL = sqrt(gm * pL / rhoL);
-    const double caL = sqrt((bXL * bXL + bYL * bYL + bZL * bZL) / rhoL);
-    const double vaL = sqrt(bXL * bXL / rhoL);
+    const double yrL = dv.recip(rhoL), yrR = dv.recip(rhoR);
+    const double csL = sqrt(dv.div(gm * pL, rhoL, yrL));
+    const double caL = sqrt(dv.div(bXL * bXL + bYL * bYL + bZL * bZL, rhoL, yrL));
+    const double vaL = sqrt(dv.div(bXL * bXL, rhoL, yrL));
     const double cfL = sqrt(0.5 * (csL * csL + caL * caL
                      + sqrt((csL * csL + caL * caL) * (csL * csL + caL * caL)
                      - 4.0 * csL * csL * vaL * vaL)));
-    const double csR = sqrt(gm * pR / rhoR);
-    const double caR = sqrt((bXR * bXR + bYR * bYR + bZR * bZR) / rhoR);
-    const double vaR = sqrt(bXR * bXR / rhoR);
+    const double csR = sqrt(dv.div(gm * pR, rhoR, yrR));
+    const double caR = sqrt(dv.div(bXR * bXR + bYR * bYR + bZR * bZR, rhoR, yrR));
+    const double vaR = sqrt(dv.div(bXR * bXR, rhoR, yrR));
     const double cfR = sqrt(0.5 * (csR * csR + caR * caR
                      + sqrt((csR * csR + caR * caR) * (csR * csR + caR * caR)
                      - 4.0 * csR * csR * vaR * vaR)));
@@ -187,37 +294,41 @@ __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double g
     SL = tmin(SL, 0.0);
     SR = tmax(SR, 0.0);
 
-    const double SM = ((SR - uR) * rhoR * uR - (SL - uL) * rhoL * uL - pTR + pTL)
-                    / ((SR - uR) * rhoR - (SL - uL) * rhoL + EPS);
-    const double pT1 = ((SR - uR) * rhoR * pTL - (SL - uL) * rhoL * pTR
-                     + rhoL * rhoR * (SR - uR) * (SL - uL) * (uR - uL))
-                     / ((SR - uR) * rhoR - (SL - uL) * rhoL + EPS);
+    const double den = (SR - uR) * rhoR - (SL - uL) * rhoL + EPS;
+    const double yden = dv.recip(den);
+    const double SM = dv.div((SR - uR) * rhoR * uR - (SL - uL) * rhoL * uL - pTR + pTL, den, yden);
+    const double pT1 = dv.div((SR - uR) * rhoR * pTL - (SL - uL) * rhoL * pTR
+                              + rhoL * rhoR * (SR - uR) * (SL - uL) * (uR - uL), den, yden);
 
-    const double rho1L = rhoL * (SL - uL) / (SL - SM + EPS);
+    const double dLM = SL - SM + EPS, dRM = SR - SM + EPS;
+    const double yLM = dv.recip(dLM), yRM = dv.recip(dRM);
+    const double DL = rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS;
+    const double DR = rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS;
+    const double yDL = dv.recip(DL), yDR = dv.recip(DR);
+    const double NL = rhoL * (SL - uL) * (SL - uL) - bXL * bXL;
+    const double NR = rhoR * (SR - uR) * (SR - uR) - bXR * bXR;
+
+    const double rho1L = dv.div(rhoL * (SL - uL), dLM, yLM);
     const double u1L = SM;
-    const double v1L = vL - bXL * bYL * (SM - uL) / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
-    const double w1L = wL - bXL * bZL * (SM - uL) / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
+    const double v1L = vL - dv.div(bXL * bYL * (SM - uL), DL, yDL);
+    const double w1L = wL - dv.div(bXL * bZL * (SM - uL), DL, yDL);
     const double bX1L = bXL;
-    const double bY1L = bYL * (rhoL * (SL - uL) * (SL - uL) - bXL * bXL)
-                      / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
-    const double bZ1L = bZL * (rhoL * (SL - uL) * (SL - uL) - bXL * bXL)
-                      / (rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS);
-    const double e1L = ((SL - uL) * eL - pTL * uL + pT1 * SM
-                     + bXL * ((uL * bXL + vL * bYL + wL * bZL) - (u1L * bX1L + v1L * bY1L + w1L * bZ1L)))
-                     / (SL - SM + EPS);
+    const double bY1L = dv.div(bYL * NL, DL, yDL);
+    const double bZ1L = dv.div(bZL * NL, DL, yDL);
+    const double e1L = dv.div((SL - uL) * eL - pTL * uL + pT1 * SM
+                              + bXL * ((uL * bXL + vL * bYL + wL * bZL) - (u1L * bX1L + v1L * bY1L + w1L * bZ1L)),
+                              dLM, yLM);
 
-    const double rho1R = rhoR * (SR - uR) / (SR - SM + EPS);
+    const double rho1R = dv.div(rhoR * (SR - uR), dRM, yRM);
     const double u1R = SM;
-    const double v1R = vR - bXR * bYR * (SM - uR) / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
-    const double w1R = wR - bXR * bZR * (SM - uR) / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
+    const double v1R = vR - dv.div(bXR * bYR * (SM - uR), DR, yDR);
+    const double w1R = wR - dv.div(bXR * bZR * (SM - uR), DR, yDR);
     const double bX1R = bXR;
-    const double bY1R = bYR * (rhoR * (SR - uR) * (SR - uR) - bXR * bXR)
-                      / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
-    const double bZ1R = bZR * (rhoR * (SR - uR) * (SR - uR) - bXR * bXR)
-                      / (rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS);
-    const double e1R = ((SR - uR) * eR - pTR * uR + pT1 * SM
-                     + bXR * ((uR * bXR + vR * bYR + wR * bZR) - (u1R * bX1R + v1R * bY1R + w1R * bZ1R)))
-                     / (SR - SM + EPS);
+    const double bY1R = dv.div(bYR * NR, DR, yDR);
+    const double bZ1R = dv.div(bZR * NR, DR, yDR);
+    const double e1R = dv.div((SR - uR) * eR - pTR * uR + pT1 * SM
+                              + bXR * ((uR * bXR + vR * bYR + wR * bZR) - (u1R * bX1R + v1R * bY1R + w1R * bZ1R)),
+                              dRM, yRM);
 
     const double S1L = SM - sqrt(bX1L * bX1L / rho1L);
     const double S1R = SM + sqrt(bX1R * bX1R / rho1R);
@@ -225,10 +336,12 @@ __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double g
     const double sqL = sqrt(rho1L), sqR = sqrt(rho1R), sqLR = sqrt(rho1L * rho1R);
     const double sbX = sgn(bX1L);
     const double u2 = SM;
-    const double v2 = (sqL * v1L + sqR * v1R + (bY1R - bY1L) * sbX) / (sqL + sqR + EPS);
-    const double w2 = (sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sbX) / (sqL + sqR + EPS);
-    const double bY2 = (sqL * bY1R + sqR * bY1L + sqLR * (v1R - v1L) * sbX) / (sqL + sqR + EPS);
-    const double bZ2 = (sqL * bZ1R + sqR * bZ1L + sqLR * (w1R - w1L) * sbX) / (sqL + sqR + EPS);
+    const double dsq = sqL + sqR + EPS;
+    const double ysq = dv.recip(dsq);
+    const double v2 = dv.div(sqL * v1L + sqR * v1R + (bY1R - bY1L) * sbX, dsq, ysq);
+    const double w2 = dv.div(sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sbX, dsq, ysq);
+    const double bY2 = dv.div(sqL * bY1R + sqR * bY1L + sqLR * (v1R - v1L) * sbX, dsq, ysq);
+    const double bZ2 = dv.div(sqL * bZ1R + sqR * bZ1L + sqLR * (w1R - w1L) * sbX, dsq, ysq);
     const double e2L = e1L - sqL * ((u1L * bX1L + v1L * bY1L + w1L * bZ1L) - (u2 * bXL + v2 * bY2 + w2 * bZ2))
                      * sgn(bXL);
     const double e2R = e1R + sqR * ((u1R * bX1R + v1R * bY1R + w1R * bZ1R) - (u2 * bXR + v2 * bY2 + w2 * bZ2))
@@ -289,6 +402,31 @@ __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double g
         if (bMR) add_one_flux(rho1R, u1R, v1R, w1R, bXR, bY1R, bZ1R, e1R, pT1, f);
         if (bIR) add_one_flux(rho1R, u2, v2, w2, bXR, bY2, bZ2, e2R, pT1, f);
     }
+}
+
+// The exact HLLD flux: shared correctly rounded reciprocals, repeated with
+// IEEE division where the guard of MdDiv fails (non-finite, huge or tiny
+// operands).  ygm1 = rcp_rn_md(gm - 1), gm1_ok = MdDiv's guard on it.
+template <bool ALL_CANDIDATES>
+__device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double gm, double EPS, double ygm1,
+                                          bool gm1_ok, double f[8])
+{
+    MdDiv md;
+    md.ok = gm1_ok;
+    hlld_body<ALL_CANDIDATES>(L, R, gm, EPS, ygm1, md, f);
+    if (!md.ok) {
+        IeeeDiv id;
+        hlld_body<ALL_CANDIDATES>(L, R, gm, EPS, gm - 1.0, id, f);
+    }
+}
+
+// The same, forming the reciprocal of gm - 1 itself.
+template <bool ALL_CANDIDATES>
+__device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double gm, double EPS, double f[8])
+{
+    MdDiv g1;
+    const double ygm1 = g1.recip(gm - 1.0);
+    hlld_flux<ALL_CANDIDATES>(L, R, gm, EPS, ygm1, g1.ok, f);
 }
 
 // HLLD flux of the fast variant: the same wave-speed estimates, star and
@@ -588,6 +726,39 @@ __device__ __forceinline__ double cfl_rate(double rho, double mx, double my, dou
     const double sx = fabs(u) + sqrt(cs * cs + ca * ca);
     const double sy = fabs(v) + sqrt(cs * cs + ca * ca);
     return sx / dx + sy / dy;
+}
+
+// cfl_rate with the divisions of a policy (MdDiv / IeeeDiv); ydx, ydy are
+// the policy's reciprocal handles of dx and dy.
+template <class Div>
+__device__ __forceinline__ double cfl_rate_body(double rho, double mx, double my, double mz, double bX, double bY,
+                                                double bZ, double e, double gm, double dx, double dy, double ydx,
+                                                double ydy, Div &dv)
+{
+    const double yr = dv.recip(rho);
+    const double u = dv.div(mx, rho, yr), v = dv.div(my, rho, yr), w = dv.div(mz, rho, yr);
+    const double p = (gm - 1.0)
+                   * (e - 0.5 * rho * (u * u + v * v + w * w)
+                   - 0.5 * (bX * bX + bY * bY + bZ * bZ));
+    const double cs = sqrt(dv.div(gm * p, rho, yr));
+    const double ca = sqrt(dv.div(bX * bX + bY * bY + bZ * bZ, rho, yr));
+    const double sx = fabs(u) + sqrt(cs * cs + ca * ca);
+    const double sy = fabs(v) + sqrt(cs * cs + ca * ca);
+    return dv.div(sx, dx, ydx) + dv.div(sy, dy, ydy);
+}
+
+// cfl_rate through shared reciprocals, repeated with IEEE division where the
+// guard fails; ydx = rcp_rn_md(dx), ydy = rcp_rn_md(dy), d_ok their guard.
+__device__ __forceinline__ double cfl_rate_md(double rho, double mx, double my, double mz, double bX, double bY,
+                                              double bZ, double e, double gm, double dx, double dy, double ydx,
+                                              double ydy, bool d_ok)
+{
+    MdDiv md;
+    md.ok = d_ok;
+    const double r = cfl_rate_body(rho, mx, my, mz, bX, bY, bZ, e, gm, dx, dy, ydx, ydy, md);
+    if (md.ok) return r;
+    IeeeDiv id;
+    return cfl_rate_body(rho, mx, my, mz, bX, bY, bZ, e, gm, dx, dy, dx, dy, id);
 }
 
 // Order-preserving encoding of a non-negative rate for atomicMax.  A NaN

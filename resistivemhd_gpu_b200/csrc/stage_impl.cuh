@@ -206,6 +206,13 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
     const Real gmR = (Real)gm, EPSR = (Real)EPS, inv_gm1 = (Real)(1.0 / (gm - 1.0));
 #else
     const Real EPSR = EPS;
+    // reciprocals of the constant divisors, for the shared-reciprocal
+    // division of the exact arithmetic (MdDiv), and whether they qualify
+    MdDiv cdiv;
+    const double ygm1 = cdiv.recip(gm - 1.0);
+    const bool gm1_ok = cdiv.ok;
+    const double y2dx = cdiv.recip(2.0 * g.dx), y2dy = cdiv.recip(2.0 * g.dy);
+    const bool d2_ok = cdiv.ok;
 #endif
 
     // ---- primitives on (TI+4) x (TJ+4) cells ----
@@ -222,9 +229,16 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
         const double v = u0[MY * UF] * irho;
         const double w = u0[MZ * UF] * irho;
 #else
-        const double u = u0[MX * UF] / rho;
-        const double v = u0[MY * UF] / rho;
-        const double w = u0[MZ * UF] / rho;
+        MdDiv md;
+        const double yr = md.recip(rho);
+        double u = md.div(u0[MX * UF], rho, yr);
+        double v = md.div(u0[MY * UF], rho, yr);
+        double w = md.div(u0[MZ * UF], rho, yr);
+        if (!md.ok) {
+            u = u0[MX * UF] / rho;
+            v = u0[MY * UF] / rho;
+            w = u0[MZ * UF] / rho;
+        }
 #endif
         const double bXc = 0.5 * (u0[BXF * UF] + u0[BXF * UF - UJ]);
         const double bYc = 0.5 * (u0[BYF * UF] + u0[BYF * UF - 1]);
@@ -265,10 +279,19 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
             const Real jZ = (Real)(p0[B_YC * PF + PJ_] - p0[B_YC * PF - PJ_]) * i2dx
                           - (Real)(p0[B_XC * PF + 1] - p0[B_XC * PF - 1]) * i2dy;
 #else
-            const double jY = -(z0[UJ] - z0[-UJ]) / two_dx;
-            const double jX = (z0[1] - z0[-1]) / two_dy;
-            const double jZ = (p0[B_YC * PF + PJ_] - p0[B_YC * PF - PJ_]) / two_dx
-                            - (p0[B_XC * PF + 1] - p0[B_XC * PF - 1]) / two_dy;
+            const double nY = -(z0[UJ] - z0[-UJ]), nX = z0[1] - z0[-1];
+            const double nZx = p0[B_YC * PF + PJ_] - p0[B_YC * PF - PJ_];
+            const double nZy = p0[B_XC * PF + 1] - p0[B_XC * PF - 1];
+            MdDiv md;
+            md.ok = d2_ok;
+            double jY = md.div(nY, two_dx, y2dx);
+            double jX = md.div(nX, two_dy, y2dy);
+            double jZ = md.div(nZx, two_dx, y2dx) - md.div(nZy, two_dy, y2dy);
+            if (!md.ok) {
+                jY = nY / two_dx;
+                jX = nX / two_dy;
+                jZ = nZx / two_dx - nZy / two_dy;
+            }
 #endif
             const Real eta = (Real)(has_eta ? Et[(ri + 2) * UJ + (rj + 2)] : g.eta);
             Real *r0 = Rs + c;
@@ -389,7 +412,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
 #if RMHD_FAST_MATH
             hlld_flux_fast(L, R, gmR, inv_gm1, EPSR, f);
 #else
-            hlld_flux<RMHD_ALL_CANDIDATES>(L, R, gm, EPS, f);
+            hlld_flux<RMHD_ALL_CANDIDATES>(L, R, gm, EPS, ygm1, gm1_ok, f);
 #endif
             fmv[0] = f[1]; fmv[1] = f[2]; fmv[2] = f[3];
             fov[0] = f[0]; fov[1] = f[6]; fov[2] = f[7]; fov[3] = f[5];
@@ -521,8 +544,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
             const double r = cfl_rate_fast(nv[RHO], nv[MX], nv[MY], nv[MZ], nv[BXF], nv[BYF], nv[BZF], nv[EN],
                                            gm, 1.0 / g.dx, 1.0 / g.dy);
 #else
-            const double r = cfl_rate(nv[RHO], nv[MX], nv[MY], nv[MZ], nv[BXF], nv[BYF], nv[BZF], nv[EN],
-                                      gm, g.dx, g.dy);
+            MdDiv dd;
+            const double ydx = dd.recip(g.dx), ydy = dd.recip(g.dy);
+            const double r = cfl_rate_md(nv[RHO], nv[MX], nv[MY], nv[MZ], nv[BXF], nv[BYF], nv[BZF], nv[EN],
+                                         gm, g.dx, g.dy, ydx, ydy, dd.ok);
 #endif
             bits = rate_bits(r);
             nan_e = nv[EN] != nv[EN];

@@ -22,7 +22,8 @@ def build_contact(d: Path, extra: tuple[str, ...] = ()):
     """contact.cu, the oracle and the step driver as a host library; `extra`
     adds compiler flags to every unit (e.g. sanitizers)."""
     shim_dir(d)
-    objs = [compile_unit(d, "contact.cu", ["-ffp-contract=off", *extra], threaded=("contact_flux_tiled_kernel",))]
+    objs = [compile_unit(d, "contact.cu", ["-ffp-contract=off", "-DRMHD_HOST_EMULATION", *extra],
+                          threaded=("contact_flux_tiled_kernel",))]
     orc = d / "oracle.o"
     subprocess.run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", *extra, "-fPIC", "-c",
                     str(ORACLE / "rmhd2d_oracle.c"), "-o", str(orc)], check=True, capture_output=True)
