@@ -414,9 +414,15 @@ def summary_of(line: dict) -> dict:
         for prec in ("fp32_bulk", "fp64_exact", "fp32_bulk_whole_trajectory", "fp64_exact_whole_trajectory"):
             if prec in ad and "adjoint_over_forward" in ad[prec]:
                 out[f"adjoint_over_forward_{prec}"] = ad[prec]["adjoint_over_forward"]
-        for key in ("fd", "fd_noisy_start", "fd_smooth_control"):
+        for key in ("fd", "fd_smooth_control"):
             if key in ad and "frac_le_1e-6" in ad[key]:
                 out[f"adjoint_{key}_frac_le_1e-6"] = ad[key]["frac_le_1e-6"]
+        for hk, hv in ad.get("fd_noisy_start", {}).items():
+            if isinstance(hv, dict) and "frac_le_1e-6" in hv:
+                out[f"adjoint_fd_noisy_{hk}_frac_le_1e-6"] = hv["frac_le_1e-6"]
+                out[f"adjoint_fd_noisy_{hk}_taylor_slope"] = hv["taylor_remainder_slope_median"]
+        for hk, hv in ad.get("bulk_forward_gradient_vs_horizon", {}).items():
+            out[f"adjoint_bulk_gradient_rel_l2_{hk}"] = hv["state"]
     en = line.get("ensemble")
     if en and "speedup_vs_loop_fp64" in en:
         out["ensemble_value"] = en["batch_fp32_bulk"]["value"]
@@ -666,28 +672,29 @@ def adjoint_block(args, local_rank, n=512, nsteps=2000, ndirs=32, h=1e-6):
             out[prec] = {"forward_ms": ms_fwd, "recorded_forward_ms": 1e3 * t_rec, "backward_ms": 1e3 * t_bwd,
                          "backward_over_forward": 1e3 * t_bwd / ms_fwd,
                          "adjoint_over_forward": 1e3 * (t_rec + t_bwd) / ms_fwd, "misfit": J}
-    # the same FP64 run with the whole trajectory kept in HBM (every step's
-    # U^n and U*, 2 x 2000 states): the backward recomputes nothing
-    try:
-        with Solver.from_setup(s, precision="fp64_exact", device=local_rank) as sol:
-            sol.adjoint_forward(nsteps, -1)                        # allocates the trajectory
-            sol.set_state(s.state, apply_boundary=True)
-            t0 = time.perf_counter()
-            sol.adjoint_forward(nsteps, -1)
-            t_rec = time.perf_counter() - t0
-            J, seed = misfit_and_seed(sol.get_state())
-            t0 = time.perf_counter()
-            gs, ge = sol.adjoint_backward(seed)
-            t_bwd = time.perf_counter() - t0
-            ms_fwd = out["fp64_exact"]["forward_ms"]
-            out["fp64_exact_whole_trajectory"] = {
-                "recorded_forward_ms": 1e3 * t_rec, "backward_ms": 1e3 * t_bwd,
-                "adjoint_over_forward": 1e3 * (t_rec + t_bwd) / ms_fwd,
-                "trajectory_states": 2 * nsteps,
-                "gradient_equals_checkpointed": bool(np.array_equal(gs, grads["fp64_exact"][0])
-                                                     and np.array_equal(ge, grads["fp64_exact"][1]))}
-    except Exception as e:  # reported, never fatal
-        out["fp64_exact_whole_trajectory"] = {"unavailable": str(e)[:200]}
+    # the same runs with the whole trajectory kept in HBM (every step's U^n
+    # and U*, 2 x 2000 states): the backward recomputes nothing
+    for prec in ("fp32_bulk", "fp64_exact"):
+        try:
+            with Solver.from_setup(s, precision=prec, device=local_rank) as sol:
+                sol.adjoint_forward(nsteps, -1)                        # allocates the trajectory
+                sol.set_state(s.state, apply_boundary=True)
+                t0 = time.perf_counter()
+                sol.adjoint_forward(nsteps, -1)
+                t_rec = time.perf_counter() - t0
+                J, seed = misfit_and_seed(sol.get_state())
+                t0 = time.perf_counter()
+                gs, ge = sol.adjoint_backward(seed)
+                t_bwd = time.perf_counter() - t0
+                ms_fwd = out[prec]["forward_ms"]
+                out[f"{prec}_whole_trajectory"] = {
+                    "recorded_forward_ms": 1e3 * t_rec, "backward_ms": 1e3 * t_bwd,
+                    "adjoint_over_forward": 1e3 * (t_rec + t_bwd) / ms_fwd,
+                    "trajectory_states": 2 * nsteps,
+                    "gradient_equals_checkpointed": bool(np.array_equal(gs, grads[prec][0])
+                                                         and np.array_equal(ge, grads[prec][1]))}
+        except Exception as e:  # reported, never fatal
+            out[f"{prec}_whole_trajectory"] = {"unavailable": str(e)[:200]}
     gx, gex = grads["fp64_exact"][0], grads["fp64_exact"][1]
     gb, geb = grads["fp32_bulk"][0], grads["fp32_bulk"][1]
     out["bulk_forward_gradient_rel_l2"] = {
@@ -714,6 +721,8 @@ def adjoint_block(args, local_rank, n=512, nsteps=2000, ndirs=32, h=1e-6):
             errs.append(abs(fd - ad) / max(abs(ad), 1e-300))
     errs = np.array(errs)
     out["fd_smooth_control"] = _fd_control(local_rank, h)
+    out["fd_noisy_start"] = _fd_noisy_start(local_rank, s, target, fields)
+    out["bulk_forward_gradient_vs_horizon"] = _bulk_gradient_vs_horizon(local_rank, s, target, fields)
     out["fd"] = {"h": h, "directions": ndirs, "forward": "fp64_exact",
                  "direction": "delta (rho vx, rho vy) of the initial state + delta eta, seeded normal",
                  "rel_err_median": float(np.median(errs)), "rel_err_max": float(errs.max()),
@@ -723,6 +732,132 @@ def adjoint_block(args, local_rank, n=512, nsteps=2000, ndirs=32, h=1e-6):
                          "perturbation out of the linear range; central differences then measure neither. "
                          "Against the oracle's dual-number tangent the adjoint agrees to 1e-10 "
                          "(tests/test_gpu_adjoint.py); fd_smooth_control is the same check where FD is valid"}
+    return out
+
+
+def _noisy(s, seed=6, amp=1e-3):
+    """The adjoint workload's start with seeded relative noise on rho and on
+    the thermal energy, so that no field is exactly uniform and minmod's
+    slopes are nonzero (the step map is then differentiable there)."""
+    import dataclasses
+
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    st = s.state.copy()
+    core = st[3:-3, 3:-3]
+    kin = 0.5 * (core[..., 1] ** 2 + core[..., 2] ** 2 + core[..., 3] ** 2) / core[..., 0]
+    eth = core[..., 7] - kin - 0.5 * (core[..., 4] ** 2 + core[..., 5] ** 2 + core[..., 6] ** 2)
+    f = 1.0 + amp * rng.uniform(-1.0, 1.0, core.shape[:2])
+    g = 1.0 + amp * rng.uniform(-1.0, 1.0, core.shape[:2])
+    core[..., 0] *= f
+    core[..., 1:4] *= f[..., None]          # same velocity
+    core[..., 7] = kin * f + eth * g        # same magnetic energy, thermal energy scaled by g
+    return dataclasses.replace(s, state=st, name=s.name + "_noisy")
+
+
+def _fd_noisy_start(local_rank, s0, target, fields, horizons=(20, 200), ndirs=32,
+                    hs=(1e-4, 1e-5, 1e-6, 1e-7, 1e-8)):
+    """Central differences and the Taylor remainder of the misfit against
+    the FP64 adjoint on the adjoint workload's grid and eta field (512^2
+    periodic Orszag-Tang, eta = 1e-3 exp(g/2)), from a start with rho and p
+    noise, over horizons where an h-perturbation stays in the linear range.
+    Per direction: the relative error of the central difference at each h
+    and the best over h; the remainder |J(x + h d) - J(x) - h <grad, d>| at
+    the h values, whose log-log slope is 2 where the map is smooth.
+
+    Two kinds of direction: "field" perturbs (rho vx, rho vy) and eta in
+    every cell; "local" perturbs them on a 3 x 3 patch.  The step map is
+    piecewise smooth -- minmod switches between its arguments where two
+    neighbouring differences are equal in size -- and a field direction
+    crosses such kinks in many cells within any h, so its central
+    differences converge only like a power of h below 1 (the field rows show
+    it); a local direction reaches few cells and is where FD measures the
+    gradient."""
+    import numpy as np
+
+    from resistivemhd_gpu_b200 import Solver
+
+    s = _noisy(s0)
+    out = {"workload": f"{s0.name} with 1e-3 rho and thermal-energy noise", "directions": ndirs, "h": list(hs),
+           "forward": "fp64_exact", "direction": "delta (rho vx, rho vy) of the initial state + delta eta"}
+    for nsteps in horizons:
+        with Solver.from_setup(s, precision="fp64_exact", device=local_rank) as sol:
+            sol.adjoint_forward(nsteps)
+            final = sol.get_state()
+            seed = np.zeros_like(final)
+            seed[3:-3, 3:-3, fields] = final[3:-3, 3:-3, fields] - target[3:-3, 3:-3, fields]
+            gs, ge = sol.adjoint_backward(seed)
+            dts = sol.adjoint_dts()
+
+            def final_of(state, eta):
+                sol.set_eta_table(eta)
+                sol.set_state(state, apply_boundary=True)
+                sol.run_fixed_dt(dts)
+                return sol.get_state()
+
+            base = final_of(s.state, s.eta_table)
+            for kind in ("local", "field"):
+                rng = np.random.default_rng(11 + nsteps)
+                best, per_h, slopes = [], {h: [] for h in hs}, []
+                for _ in range(ndirs):
+                    d = np.zeros_like(s.state)
+                    de = np.zeros_like(s.eta_table)
+                    if kind == "field":
+                        d[3:-3, 3:-3, 1:3] = (rng.standard_normal(d[3:-3, 3:-3, 1:3].shape)
+                                              * s.state[3:-3, 3:-3, 0:1])
+                        de[...] = rng.standard_normal(s.eta_table.shape) * s.eta_table
+                    else:
+                        i0, j0 = rng.integers(3, s.nx - 6), rng.integers(3, s.ny - 6)
+                        d[i0:i0 + 3, j0:j0 + 3, 1:3] = rng.standard_normal((3, 3, 2)) * s.state[i0:i0 + 3, j0:j0 + 3, 0:1]
+                        de[i0:i0 + 3, j0:j0 + 3] = rng.standard_normal((3, 3)) * s.eta_table[i0:i0 + 3, j0:j0 + 3]
+                    ad = float((gs * d).sum() + (ge * de).sum())
+                    errs, rem = [], []
+                    for h in hs:
+                        fp = final_of(s.state + h * d, s.eta_table + h * de)
+                        fm = final_of(s.state - h * d, s.eta_table - h * de)
+                        fd = _misfit_difference(fp, fm, target, fields) / (2 * h)
+                        e = abs(fd - ad) / max(abs(ad), 1e-300)
+                        errs.append(e)
+                        per_h[h].append(e)
+                        rem.append(abs(_misfit_difference(fp, base, target, fields) - h * ad))
+                    best.append(min(errs))
+                    # slope of the remainder over the three largest h (above the rounding floor)
+                    lr = np.log10(np.maximum(rem[:3], 1e-300))
+                    slopes.append(float(np.polyfit(np.log10(hs[:3]), lr, 1)[0]))
+                best = np.array(best)
+                out[f"{kind}_steps_{nsteps}"] = {
+                    "frac_le_1e-6": float((best <= 1e-6).mean()), "rel_err_median": float(np.median(best)),
+                    "rel_err_max": float(best.max()),
+                    "rel_err_median_per_h": {f"{h:g}": float(np.median(per_h[h])) for h in hs},
+                    "taylor_remainder_slope_median": float(np.median(slopes)),
+                    "taylor_remainder_slope_min": float(np.min(slopes))}
+    return out
+
+
+def _bulk_gradient_vs_horizon(local_rank, s, target, fields, horizons=(20, 200, 2000)):
+    """Relative L2 distance of the gradients with the FP32-bulk forward from
+    those with the FP64-exact forward (both reversed in FP64), by horizon: the
+    FP32 trajectory departs from the FP64 one by its rounding, amplified by
+    the flow, and the adjoint is linearised about it."""
+    import numpy as np
+
+    from resistivemhd_gpu_b200 import Solver
+
+    out = {}
+    for nsteps in horizons:
+        g = {}
+        for prec in ("fp32_bulk", "fp64_exact"):
+            with Solver.from_setup(s, precision=prec, device=local_rank) as sol:
+                sol.adjoint_forward(nsteps)
+                final = sol.get_state()
+                seed = np.zeros_like(final)
+                seed[3:-3, 3:-3, fields] = final[3:-3, 3:-3, fields] - target[3:-3, 3:-3, fields]
+                g[prec] = sol.adjoint_backward(seed)
+        gx, gex = g["fp64_exact"]
+        gb, geb = g["fp32_bulk"]
+        out[f"steps_{nsteps}"] = {"state": float(np.linalg.norm(gb - gx) / np.linalg.norm(gx)),
+                                  "eta": float(np.linalg.norm(geb - gex) / np.linalg.norm(gex))}
     return out
 
 

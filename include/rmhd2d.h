@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RMHD2D_ABI_VERSION 2
+#define RMHD2D_ABI_VERSION 3
 #define RMHD2D_GHOST 3
 
 typedef enum {
@@ -305,6 +305,76 @@ int rmhd2d_adjoint_release(rmhd2d_solver *s);
    several host threads) race and may return a wrong dt. */
 #define RMHD2D_NOALLOC_MAX_CELLS 16777216
 int rmhd2d_calculate_dt_noalloc(const rmhd2d_config *cfg, const double *device_state, double *dt);
+
+/* ---- single domain decomposed into x slabs ----------------------------------
+   Replaces the multi-GPU library's decomposition
+   (ResistiveMHD_multiGPU_cuda/ResistiveMHD2D_GPU/mpi.cu:104-276: sendrecv_U
+   of 3 ghost layers through host-staged MPI_Sendrecv; resistiveMHD2D.cu:550,574:
+   MPI_Allreduce of dt and of the crash flag) for the single-GPU library's
+   step.  A slab is a solver whose array holds a contiguous range of the
+   domain's interior columns i plus 3 columns on each side: the x wall's ghost
+   columns where the side is the domain's edge, else a halo of the
+   neighbouring slab's first (last) 3 columns.  Periodic x over several
+   slabs makes both sides of every slab halos (the first slab's low halo is
+   the last slab's high edge).  The library runs the stages and fills wall
+   ghosts; the host (the Python SlabDomain, resistivemhd_gpu_b200/slab.py, over
+   torch.distributed) moves halo columns between slabs and combines three
+   control words across slabs with a max.  The slabs' steps are then
+   bit-identical to one solver on the whole domain.
+
+   One step of every slab, in this order:
+     rmhd2d_slab_stage(s, 1);  exchange(state 1); rmhd2d_slab_fill(s, 1); exchange(state 1);
+     rmhd2d_slab_stage(s, 2);  exchange(state 0); rmhd2d_slab_fill(s, 2); exchange(state 0);
+     rmhd2d_slab_get_words(s, w);  max-combine w over slabs;  rmhd2d_slab_set_words(s, w);
+   where exchange(k) packs the own edge columns of state k on each halo side
+   (rmhd2d_slab_pack) and unpacks the neighbour's into the halo
+   (rmhd2d_slab_unpack).  The first exchange of a pair brings the halo's
+   interior rows, which the ghost fill of a mirror y wall reads; the second
+   brings the ghost rows the neighbour filled.  After rmhd2d_set_state(s, x,
+   0) of each slab's part of the initial state: exchange(0);
+   rmhd2d_slab_fill(s, 0); exchange(0); rmhd2d_slab_refresh_rate(s); then the
+   word combination as above.  Work is enqueued on the solver's stream.
+   A slab with halo columns refuses rmhd2d_step_rk2, run, run_fixed_dt,
+   profile_step, autotune, calculate_dt, apply_boundary, set_state with
+   apply_boundary, and the adjoint: their whole-array work needs the
+   exchange. */
+#define RMHD2D_SLAB_LO 1      /* the low x side borders another slab (its 3 ghost columns are a halo) */
+#define RMHD2D_SLAB_HI 2      /* the high x side borders another slab */
+#define RMHD2D_SLAB_ORIGIN 4  /* this slab holds the domain's first interior column (the first slab) */
+
+/* cfg describes the slab's own array: nx = its interior columns + 6, the
+   domain's ny, dx, dy and physics; cfg->bc is the x wall on the sides that
+   are not halos.  sides: RMHD2D_SLAB_* flags; a slab whose low side is a wall
+   must be the first (RMHD2D_SLAB_ORIGIN).  Stage-1-EMF CT only. */
+int rmhd2d_create_slab(const rmhd2d_config *cfg, int sides, rmhd2d_solver **out);
+/* Doubles of one packed halo: 8 fields x 3 columns x the array's row pitch. */
+int rmhd2d_slab_halo_doubles(const rmhd2d_solver *s, long long *n);
+/* state: 0 = the current state, 1 = the stage-1 state; side: 0 = low x,
+   1 = high x.  pack copies the 3 own columns next to that side into
+   dev_buf; unpack copies dev_buf (a neighbour's pack) into that side's halo
+   columns (refused on a wall side).  dev_buf: device memory of
+   rmhd2d_slab_halo_doubles doubles. */
+int rmhd2d_slab_pack(rmhd2d_solver *s, int state, int side, double *dev_buf);
+int rmhd2d_slab_unpack(rmhd2d_solver *s, int state, int side, const double *dev_buf);
+/* Stage 1 (current -> stage-1 state) or stage 2 (-> current) on the own
+   columns, with the dt of the combined words. */
+int rmhd2d_slab_stage(rmhd2d_solver *s, int stage);
+/* Ghost fill of the wall sides and of the y walls of the own columns:
+   which = 0 the current state after set_state / load, 1 the stage-1 state,
+   2 the current state after stage 2, with the CFL and NaN reductions of the
+   own cells and wall ghosts into the next step's words; 2 ends the step. */
+int rmhd2d_slab_fill(rmhd2d_solver *s, int which);
+/* The CFL and NaN reductions of the current state (after set_state and its
+   fill), into the words of the next step. */
+int rmhd2d_slab_refresh_rate(rmhd2d_solver *s);
+/* The next step's words w[0..2] = (bits of the maximum CFL rate, cell 0's dt
+   candidate is NaN, crash flag), to or from 3 int64 of device memory; the
+   host combines them with a max over all slabs in between.  Called after the
+   exchange that ends a step (or the initial fill): on the first slab of a
+   periodic-x decomposition it also completes the domain's ghost column 0,
+   which that slab holds in its low halo. */
+int rmhd2d_slab_get_words(rmhd2d_solver *s, long long *dev_words);
+int rmhd2d_slab_set_words(rmhd2d_solver *s, const long long *dev_words);
 
 /* Text of the last error of this solver (or of the last failed create when
    s is NULL); never NULL. */

@@ -79,6 +79,15 @@ SIGNATURES = [
     ("rmhd2d_adjoint_release", ctypes.c_int, [_S]),
     ("rmhd2d_calculate_dt_noalloc", ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_void_p,
                                                     ctypes.POINTER(ctypes.c_double)]),
+    ("rmhd2d_create_slab", ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("rmhd2d_slab_halo_doubles", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_longlong)]),
+    ("rmhd2d_slab_pack", ctypes.c_int, [_S, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    ("rmhd2d_slab_unpack", ctypes.c_int, [_S, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    ("rmhd2d_slab_stage", ctypes.c_int, [_S, ctypes.c_int]),
+    ("rmhd2d_slab_fill", ctypes.c_int, [_S, ctypes.c_int]),
+    ("rmhd2d_slab_refresh_rate", ctypes.c_int, [_S]),
+    ("rmhd2d_slab_get_words", ctypes.c_int, [_S, ctypes.c_void_p]),
+    ("rmhd2d_slab_set_words", ctypes.c_int, [_S, ctypes.c_void_p]),
     ("rmhd2d_last_error", ctypes.c_char_p, [_S]),
     ("rmhd2d_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("rmhd2d_abi_version", ctypes.c_int, []),

@@ -42,6 +42,14 @@ UNITS = {
 }
 
 
+# A test build of the library (tests/test_gpu_wait_expiry.py): the stage
+# units compiled with RMHD_TEST_WAIT_EXPIRY issue no tile load, so every
+# CTA's bounded wait for its tile expires; the other units are the product's.
+WAIT_TEST_DIR = ROOT / "tests" / "_build"
+WAIT_TEST_LIB = WAIT_TEST_DIR / "librmhd2d_waittest.so"
+STAGE_UNITS = ("stage_exact.cu", "stage_fast.cu", "stage_bulk32.cu")
+
+
 def _deps() -> list[Path]:
     return sorted(CSRC.glob("*")) + [ROOT / "include" / "rmhd2d.h", Path(__file__)]
 
@@ -83,6 +91,38 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     return LIB
 
 
+def build_wait_test(verbose: bool = False) -> Path:
+    """tests/_build/librmhd2d_waittest.so (after build())."""
+    deps = _deps() + [LIB]
+    if not _stale(WAIT_TEST_LIB, deps):
+        return WAIT_TEST_LIB
+    WAIT_TEST_DIR.mkdir(parents=True, exist_ok=True)
+    objs = []
+    cmds = []
+    for unit, extra in UNITS.items():
+        if unit in STAGE_UNITS:
+            obj = WAIT_TEST_DIR / (Path(unit).stem + "_waittest.o")
+            cmds.append(["nvcc", *ARCH, *COMMON, *extra, "-DRMHD_TEST_WAIT_EXPIRY", "-c", str(CSRC / unit), "-o",
+                         str(obj)])
+        else:
+            obj = OBJ / (Path(unit).stem + ".o")
+        objs.append(str(obj))
+
+    def run(cmd):
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+
+    with cf.ThreadPoolExecutor(max_workers=len(cmds)) as pool:
+        list(pool.map(run, cmds))
+    run(["nvcc", *ARCH, "-shared", "-cudart", "static", "-o", str(WAIT_TEST_LIB), *objs])
+    for o in objs:
+        if o.endswith("_waittest.o"):
+            Path(o).unlink()
+    return WAIT_TEST_LIB
+
+
 if __name__ == "__main__":
     build(verbose=True, ptxas_info="-v" in sys.argv)
+    build_wait_test()
     print(LIB)

@@ -59,6 +59,7 @@ struct rmhd2d_solver {
     cudaGraphExec_t graph1[2] = {nullptr, nullptr};   // one step per parity (rmhd2d_step_rk2)
     AdjointWork *adj = nullptr;          // recorded trajectory and workspace of the discrete adjoint
     double *contact = nullptr;           // CT-Contact workspace: C, F1, G1, F2, G2 (8 planes each), R1, R2, E
+    int slab = 0;                        // RMHD2D_SLAB_* flags of a slab of a decomposed domain (rmhd2d_create_slab)
     std::string err;
 };
 
@@ -182,6 +183,19 @@ int do_boundary(rmhd2d_solver *s)
     launch_boundary(s->g, s->A, s->row2, nullptr, 0, s->stream);
     CK(cudaGetLastError());
     return RMHD2D_OK;
+}
+
+// rmhd2d_solver::slab: set (with the RMHD2D_SLAB_* flags) by rmhd2d_create_slab.
+constexpr int SLAB_CREATED = 1 << 8;
+
+// Entry points that step, fill or reduce over the whole array refuse a slab
+// with halo columns: its neighbours' exchange and the cross-slab reduction
+// are steps the host takes between the rmhd2d_slab_* calls.
+int refuse_halo_slab(rmhd2d_solver *s, const char *what)
+{
+    return fail(s, RMHD2D_ERR_STATE,
+                std::string(what) + " on a slab with halo columns: step it with rmhd2d_slab_stage / "
+                                    "rmhd2d_slab_fill and the host's exchange");
 }
 
 using StageLauncher = void (*)(int, int, const CUtensorMap *, const CUtensorMap *, const StageArgs &, cudaStream_t);
@@ -527,6 +541,7 @@ static int destroy_solver(rmhd2d_solver *s)
 int rmhd2d_set_state(rmhd2d_solver *s, const double *host, int apply_boundary)
 {
     if (!s || !host) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (apply_boundary && s->g.x_halo) return refuse_halo_slab(s, "set_state with apply_boundary");
     CK(cudaSetDevice(s->device));
     const size_t n = (size_t)s->g.nx * s->g.ny * NFIELD;
     // B doubles as the AoS staging buffer (it holds no live data between steps).
@@ -537,6 +552,7 @@ int rmhd2d_set_state(rmhd2d_solver *s, const double *host, int apply_boundary)
 int rmhd2d_set_state_device(rmhd2d_solver *s, const double *dev, int apply_boundary)
 {
     if (!s || !dev) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (apply_boundary && s->g.x_halo) return refuse_halo_slab(s, "set_state_device with apply_boundary");
     CK(cudaSetDevice(s->device));
     const size_t n = (size_t)s->g.nx * s->g.ny * NFIELD;
     CK(cudaMemcpyAsync(s->B, dev, n * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
@@ -588,6 +604,7 @@ int rmhd2d_set_eta_table(rmhd2d_solver *s, const double *host_eta)
 int rmhd2d_apply_boundary(rmhd2d_solver *s)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->g.x_halo) return refuse_halo_slab(s, "apply_boundary");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
     int rc = do_boundary(s);
@@ -598,6 +615,7 @@ int rmhd2d_apply_boundary(rmhd2d_solver *s)
 int rmhd2d_calculate_dt(rmhd2d_solver *s, double *dt)
 {
     if (!s || !dt) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (s->g.x_halo) return refuse_halo_slab(s, "calculate_dt");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
     int rc = sync_and_check(s);
@@ -610,6 +628,7 @@ int rmhd2d_calculate_dt(rmhd2d_solver *s, double *dt)
 int rmhd2d_step_rk2(rmhd2d_solver *s)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->g.x_halo) return refuse_halo_slab(s, "step_rk2");
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
@@ -647,6 +666,7 @@ int rmhd2d_step_rk2(rmhd2d_solver *s)
 int rmhd2d_run(rmhd2d_solver *s, int nsteps)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->g.x_halo) return refuse_halo_slab(s, "run");
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (nsteps < 0) return fail(s, RMHD2D_ERR_INVALID, "nsteps < 0");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
@@ -695,6 +715,7 @@ int rmhd2d_run_timed(rmhd2d_solver *s, int nsteps, float *ms)
 int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
 {
     if (!s || !ms4) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (s->g.x_halo) return refuse_halo_slab(s, "profile_step");
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (s->contact) return fail(s, RMHD2D_ERR_STATE, "profile_step times the four launches of the stage-1-EMF step");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
@@ -870,6 +891,7 @@ static int snapshot_restore(rmhd2d_solver *s, Snapshot &sn)
 int rmhd2d_autotune(rmhd2d_solver *s, int trial_steps, int *best_shape)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->g.x_halo) return refuse_halo_slab(s, "autotune");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: tune the batch");
     if (trial_steps < 2) trial_steps = 2;
@@ -1294,11 +1316,162 @@ int rmhd2d_calculate_dt_noalloc(const rmhd2d_config *cfg, const double *device_s
     return RMHD2D_OK;
 }
 
+// ---- slabs of a single domain decomposed along x -----------------------------
+//
+// One slab per rank (or per solver): its own interior columns plus 3 halo
+// columns on each side that borders another slab.  The host exchanges halo
+// columns between neighbours and combines the CFL / NaN reductions across
+// slabs; the library fills the ghost cells of walls and runs the stages.
+
+int rmhd2d_create_slab(const rmhd2d_config *cfg, int sides, rmhd2d_solver **out)
+{
+    rmhd2d_solver *s = nullptr;
+    if (!cfg || !out) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (sides & ~(RMHD2D_SLAB_LO | RMHD2D_SLAB_HI | RMHD2D_SLAB_ORIGIN))
+        return fail(s, RMHD2D_ERR_INVALID, "unknown slab flags");
+    if (!(sides & RMHD2D_SLAB_LO) && !(sides & RMHD2D_SLAB_ORIGIN))
+        return fail(s, RMHD2D_ERR_INVALID, "a slab whose low x side is a wall is the first slab: set RMHD2D_SLAB_ORIGIN");
+    if (cfg->ct_scheme != RMHD2D_CT_STAGE1)
+        return fail(s, RMHD2D_ERR_INVALID, "slabs run the stage-1-EMF CT only");
+    const int rc = rmhd2d_create(cfg, out);
+    if (rc) return rc;
+    (*out)->g.x_halo = sides & (RMHD2D_SLAB_LO | RMHD2D_SLAB_HI);
+    (*out)->slab = sides | SLAB_CREATED;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_slab_halo_doubles(const rmhd2d_solver *s, long long *n)
+{
+    if (!s || !n) return fail(const_cast<rmhd2d_solver *>(s), RMHD2D_ERR_INVALID, "null argument");
+    *n = (long long)NFIELD * 3 * s->g.pitch;
+    return RMHD2D_OK;
+}
+
+static int slab_state(rmhd2d_solver *s, int state, double **p)
+{
+    if (state != 0 && state != 1) return fail(s, RMHD2D_ERR_INVALID, "state must be 0 (current) or 1 (stage 1)");
+    *p = state == 0 ? s->A : s->B;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_slab_pack(rmhd2d_solver *s, int state, int side, double *dev_buf)
+{
+    if (!s || !dev_buf) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!(s->slab & SLAB_CREATED)) return fail(s, RMHD2D_ERR_STATE, "not a slab (rmhd2d_create_slab)");
+    if (side != 0 && side != 1) return fail(s, RMHD2D_ERR_INVALID, "side must be 0 (low x) or 1 (high x)");
+    double *st = nullptr;
+    int rc = slab_state(s, state, &st);
+    if (rc) return rc;
+    CK(cudaSetDevice(s->device));
+    launch_slab_halo(s->g, st, dev_buf, side == 0 ? HALO : s->g.nx - 2 * HALO, 1, s->stream);
+    CK(cudaGetLastError());
+    return RMHD2D_OK;
+}
+
+int rmhd2d_slab_unpack(rmhd2d_solver *s, int state, int side, const double *dev_buf)
+{
+    if (!s || !dev_buf) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!(s->slab & SLAB_CREATED)) return fail(s, RMHD2D_ERR_STATE, "not a slab (rmhd2d_create_slab)");
+    if (side != 0 && side != 1) return fail(s, RMHD2D_ERR_INVALID, "side must be 0 (low x) or 1 (high x)");
+    if (!(s->g.x_halo & (1 << side))) return fail(s, RMHD2D_ERR_STATE, "that side is a wall, not a halo");
+    double *st = nullptr;
+    int rc = slab_state(s, state, &st);
+    if (rc) return rc;
+    CK(cudaSetDevice(s->device));
+    launch_slab_halo(s->g, st, const_cast<double *>(dev_buf), side == 0 ? 0 : s->g.nx - HALO, 0, s->stream);
+    CK(cudaGetLastError());
+    return RMHD2D_OK;
+}
+
+int rmhd2d_slab_stage(rmhd2d_solver *s, int stage)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (!(s->slab & SLAB_CREATED)) return fail(s, RMHD2D_ERR_STATE, "not a slab (rmhd2d_create_slab)");
+    if (stage != 1 && stage != 2) return fail(s, RMHD2D_ERR_INVALID, "stage must be 1 or 2");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    StageArgs a{};
+    a.g = s->g;
+    a.eta = s->eta;
+    a.row2 = s->g.bc_x == BC_SYMMETRIC ? s->row2 : nullptr;
+    a.ctl = s->ctl;
+    a.parity = s->parity;
+    auto launch = stage_launcher(s->cfg.precision);
+    if (stage == 1) {
+        a.src = s->A;
+        a.un = s->A;
+        a.dst = s->B;
+        launch(1, s->shape, &s->mapA[s->shape], &s->mapE1[s->shape], a, s->stream);
+    } else {
+        a.src = s->B;
+        a.un = s->A;
+        a.dst = s->A;
+        launch(2, s->shape, &s->mapB[s->shape], &s->mapE2[s->shape], a, s->stream);
+    }
+    CK(cudaGetLastError());
+    return RMHD2D_OK;
+}
+
+int rmhd2d_slab_fill(rmhd2d_solver *s, int which)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (!(s->slab & SLAB_CREATED)) return fail(s, RMHD2D_ERR_STATE, "not a slab (rmhd2d_create_slab)");
+    if (which < 0 || which > 2) return fail(s, RMHD2D_ERR_INVALID, "which must be 0, 1 or 2");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    if (which == 0) {
+        if (s->g.bc_x == BC_SYMMETRIC) launch_snapshot_row2(s->g, s->A, s->row2, s->stream);
+        launch_boundary(s->g, s->A, s->row2, nullptr, 0, s->stream);
+    } else if (which == 1) {
+        launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
+    } else {
+        launch_boundary(s->g, s->A, s->row2, s->ctl, s->parity ^ 1, s->stream);
+        s->parity ^= 1;
+        s->steps += 1;
+    }
+    CK(cudaGetLastError());
+    return RMHD2D_OK;
+}
+
+int rmhd2d_slab_refresh_rate(rmhd2d_solver *s)
+{
+    if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (!(s->slab & SLAB_CREATED)) return fail(s, RMHD2D_ERR_STATE, "not a slab (rmhd2d_create_slab)");
+    if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
+    CK(cudaSetDevice(s->device));
+    return refresh_rate(s);
+}
+
+int rmhd2d_slab_get_words(rmhd2d_solver *s, long long *dev_words)
+{
+    if (!s || !dev_words) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!(s->slab & SLAB_CREATED)) return fail(s, RMHD2D_ERR_STATE, "not a slab (rmhd2d_create_slab)");
+    CK(cudaSetDevice(s->device));
+    // the domain's ghost column 0 of a periodic-x decomposition sits in the
+    // first slab's low halo, which its neighbour has just filled
+    if ((s->slab & RMHD2D_SLAB_ORIGIN) && (s->g.x_halo & 1))
+        launch_slab_origin_column(s->g, s->A, s->ctl, s->parity, s->stream);
+    launch_slab_words(s->ctl, s->parity, dev_words, 1, s->stream);
+    CK(cudaGetLastError());
+    return RMHD2D_OK;
+}
+
+int rmhd2d_slab_set_words(rmhd2d_solver *s, const long long *dev_words)
+{
+    if (!s || !dev_words) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (!(s->slab & SLAB_CREATED)) return fail(s, RMHD2D_ERR_STATE, "not a slab (rmhd2d_create_slab)");
+    CK(cudaSetDevice(s->device));
+    launch_slab_words(s->ctl, s->parity, const_cast<long long *>(dev_words), 0, s->stream);
+    CK(cudaGetLastError());
+    return RMHD2D_OK;
+}
+
 // ---- discrete adjoint -------------------------------------------------------
 
 extern "C" int rmhd2d_run_fixed_dt(rmhd2d_solver *s, int nsteps, const double *host_dts)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->g.x_halo) return refuse_halo_slab(s, "run_fixed_dt");
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (nsteps < 0 || (nsteps > 0 && !host_dts)) return fail(s, RMHD2D_ERR_INVALID, "bad nsteps or dts");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
@@ -1326,6 +1499,7 @@ extern "C" int rmhd2d_run_fixed_dt(rmhd2d_solver *s, int nsteps, const double *h
 extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoint_interval)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
+    if (s->g.x_halo) return refuse_halo_slab(s, "adjoint_forward");
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: step the batch");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     if (nsteps < 1) return fail(s, RMHD2D_ERR_INVALID, "nsteps must be >= 1");
@@ -1441,6 +1615,7 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
                                        double *host_grad_eta)
 {
     if (!s || !host_seed || !host_grad_state) return fail(s, RMHD2D_ERR_INVALID, "null argument");
+    if (s->g.x_halo) return refuse_halo_slab(s, "adjoint_backward");
     if (!s->adj || !s->adj->recorded)
         return fail(s, RMHD2D_ERR_STATE, "no recorded forward run (rmhd2d_adjoint_forward)");
     CK(cudaSetDevice(s->device));

@@ -21,6 +21,20 @@ __device__ __forceinline__ int mirror(int c, int n)
     return c;
 }
 
+// A column that holds cells of the domain's interior: the interior columns
+// of the array and, in a slab of a decomposed domain, its halo columns
+// (copies of the neighbouring slab's own columns).
+__device__ __forceinline__ bool x_inner(const Grid &g, int i)
+{
+    return (i >= 3 || (g.x_halo & 1)) && (i < g.nx - 3 || (g.x_halo & 2));
+}
+
+// A halo column of a slab (filled by the exchange, never by the ghost fill).
+__device__ __forceinline__ bool halo_col(const Grid &g, int i)
+{
+    return (i < 3 && (g.x_halo & 1)) || (i >= g.nx - 3 && (g.x_halo & 2));
+}
+
 // Periodic wrap (boundary.cu:9-57, period n-6).
 __device__ __forceinline__ int wrap(int c, int n)
 {
@@ -99,7 +113,7 @@ __device__ __forceinline__ void load_cell(const Grid &g, const double *s, int i,
 template <int BX>
 __device__ void after_x_cell(const Grid &g, const double *s, const double *row2, int i, int j, double *v)
 {
-    if (i >= 3 && i < g.nx - 3) {
+    if (x_inner(g, i)) {
         load_cell(g, s, i, j, v);
         return;
     }
@@ -131,7 +145,7 @@ __device__ __forceinline__ double after_x_field(const Grid &g, const double *s, 
                                                 int j)
 {
     const int kx = BX >= 0 ? BX : g.bc_x;
-    if (i >= 3 && i < g.nx - 3) return s[f * g.plane + at(g, i, j)];
+    if (x_inner(g, i)) return s[f * g.plane + at(g, i, j)];
     if (kx == BC_PERIODIC) return s[f * g.plane + at(g, wrap(i, g.nx), j)];
     if (kx == BC_SYMMETRIC)
         return f == BXF ? bX_xghost(g, s + BXF * g.plane, s + BYF * g.plane, row2, i, j)
@@ -198,6 +212,7 @@ __device__ __forceinline__ void fill_ghost(const Grid &g, double *s, const doubl
 {
     int i, j;
     ghost_cell(g, t, i, j);
+    if (halo_col(g, i)) return;   // a slab's halo comes from its neighbour
     const long long P = g.plane;
     const long long k = at(g, i, j);
     double v[8];
@@ -300,6 +315,7 @@ __global__ void rate_kernel(Grid g, const double *s, Control *ctl, int slot, int
     int nan_e = 0;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t / g.ny), j = (int)(t - (long long)i * g.ny);
+        if (halo_col(g, i)) continue;   // a slab's halo cells are reduced by their owner
         const long long k = at(g, i, j);
         const long long P = g.plane;
         const double e = s[EN * P + k];
@@ -355,6 +371,57 @@ __global__ void table_to_plane_kernel(Grid g, const double *tab, double *plane)
     }
 }
 
+// Slab halo exchange: the 3 columns starting at col0 (all rows, all fields)
+// to (to_buf) or from a packed buffer laid out [field][3 columns][pitch].
+__global__ void slab_halo_kernel(Grid g, double *s, double *buf, int col0, int to_buf)
+{
+    const long long per_field = 3LL * g.pitch;
+    const long long n = NFIELD * per_field;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long f = t / per_field;
+        double *p = s + f * g.plane + (long long)col0 * g.pitch + (t - f * per_field);
+        if (to_buf) buf[t] = *p;
+        else *p = buf[t];
+    }
+}
+
+// The first slab of a periodic-x decomposition holds the domain's ghost
+// column 0 in its low halo, copied from the last slab's column nx-6.  A
+// mirror y wall fills column 0's ghost bY without the div-B integration, for
+// want of a column to its left (TS boundary.cu:159-188 at i = 0), where the
+// copied column integrated: restore those 6 values.  The copies' CFL rates
+// were reduced by their owner, these 6 cells' are reduced here, with cell
+// (0, 0)'s NaN test for first_nan.  One thread per ghost row.
+__global__ void slab_origin_column_kernel(Grid g, double *s, Control *ctl, int slot)
+{
+    const int t = threadIdx.x;
+    if (t >= 6) return;
+    const int j = t < 3 ? t : g.ny - 6 + t;
+    const long long P = g.plane;
+    const long long k = at(g, 0, j);
+    if (g.bc_y == BC_SYMMETRIC) s[BYF * P + k] = s[BYF * P + at(g, 0, j < 3 ? 3 : g.ny - 4)];
+    const double r = cfl_rate(s[RHO * P + k], s[MX * P + k], s[MY * P + k], s[MZ * P + k], s[BXF * P + k],
+                              s[BYF * P + k], s[BZF * P + k], s[EN * P + k], g.gamma, g.dx, g.dy);
+    const unsigned long long b = rate_bits(r);
+    if (b) atomicMax(&ctl->amax[slot], b);
+    if (j == 0 && r != r) ctl->first_nan[slot] = 1;
+}
+
+// The reductions a decomposed domain combines across slabs: w = [amax bits
+// of slot, first_nan of slot, crashed], to (to_buf) or from the buffer.
+__global__ void slab_words_kernel(Control *ctl, int slot, long long *w, int to_buf)
+{
+    if (to_buf) {
+        w[0] = (long long)ctl->amax[slot];
+        w[1] = ctl->first_nan[slot];
+        w[2] = ctl->crashed;
+    } else {
+        ctl->amax[slot] = (unsigned long long)w[0];
+        ctl->first_nan[slot] = (int)w[1];
+        ctl->crashed = (int)w[2];
+    }
+}
+
 int grid_for(long long n, int threads)
 {
     long long b = (n + threads - 1) / threads;
@@ -403,6 +470,21 @@ void launch_snapshot_row2(const Grid &g, const double *s, double *row2, cudaStre
 void launch_rate(const Grid &g, const double *s, Control *ctl, int slot, int set_crash, cudaStream_t st)
 {
     rate_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, st>>>(g, s, ctl, slot, set_crash);
+}
+
+void launch_slab_halo(const Grid &g, double *s, double *buf, int col0, int to_buf, cudaStream_t st)
+{
+    slab_halo_kernel<<<grid_for(8LL * 3 * g.pitch, 256), 256, 0, st>>>(g, s, buf, col0, to_buf);
+}
+
+void launch_slab_origin_column(const Grid &g, double *s, Control *ctl, int slot, cudaStream_t st)
+{
+    slab_origin_column_kernel<<<1, 32, 0, st>>>(g, s, ctl, slot);
+}
+
+void launch_slab_words(Control *ctl, int slot, long long *w, int to_buf, cudaStream_t st)
+{
+    slab_words_kernel<<<1, 1, 0, st>>>(ctl, slot, w, to_buf);
 }
 
 void launch_aos_to_planes(const Grid &g, const double *aos, double *s, cudaStream_t st)

@@ -127,9 +127,9 @@ __device__ __forceinline__ double rcp_nr(double a)
 // division.  A zero dividend returns q itself, which carries the sign
 // IEEE division gives (q + r y would turn -0 into +0).
 //
-// tests/test_division.py checks both against IEEE division on random and
-// special operands (on the CPU for this algorithm, on the GPU for the
-// hardware seed).
+// tests/test_division.py checks the quotients against IEEE division on
+// random and special operands (on the CPU for the algorithm, on the GPU for
+// the hardware seed).
 __device__ __forceinline__ double rcp_rn_md(double b)
 {
     double y;

@@ -24,6 +24,11 @@ struct Grid {
     double dx, dy;
     double gamma, cfl, eps, eta;
     int bc_x, bc_y;      // Bc of the x walls (i) and the y walls (j)
+    // Slab of a decomposed domain: bit 0 (bit 1) set when the 3 columns
+    // i < 3 (i >= nx-3) are the halo of the neighbouring slab, filled by the
+    // host's exchange and read as interior columns; the x wall applies only
+    // on the other sides.  0 for a whole domain.
+    int x_halo;
 };
 
 // Device-side control block (one per solver), zero-initialised at create.

@@ -109,11 +109,22 @@ __device__ __forceinline__ void muscl_dev(double qm, double q0, double qp, doubl
     qR = qp - (double)(0.5f * mR);
 }
 
+// Tries of the bounded wait for the staged tile.  A separate test build of
+// the library (RMHD_TEST_WAIT_EXPIRY, tests/test_gpu_wait_expiry.py) issues
+// no tile load and gives up after a few tries, so that the expiry path --
+// error flag, RMHD2D_ERR_KERNEL, a usable context afterwards -- is exercised
+// without a fault.
+#if defined(RMHD_TEST_WAIT_EXPIRY)
+constexpr int STAGE_WAIT_TRIES = 4;
+#else
+constexpr int STAGE_WAIT_TRIES = 50000;
+#endif
+
 // Waits for phase `phase` of the mbarrier with a bounded number of tries
 // (each try suspends for at most 20 us); false when the bound expired.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase)
 {
-    for (int tries = 0; tries < 50000; ++tries)
+    for (int tries = 0; tries < STAGE_WAIT_TRIES; ++tries)
         if (mbar_try_wait(bar, phase)) return true;
     return false;
 }
@@ -155,10 +166,12 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
         // order this CTA's earlier shared-memory accesses before the async copy
         fence_proxy_async();
         mbar_expect_tx(bar, T::U_BYTES + (has_eta ? T::E_BYTES : 0u));
+#if !defined(RMHD_TEST_WAIT_EXPIRY)
         // x coordinate (j) = j0 - 3 = tj * TJ: a multiple of TJ (even), so
         // 16-byte aligned in the global tensor as TMA requires.
         tma_load_3d(Ut, tmap, bar, j0 - HALO, i0 - HALO, 0);
         if (has_eta) tma_load_2d(Et, emap, bar, j0 - HALO, i0 - HALO);
+#endif
     }
 
     // own cell of this thread in the update phase

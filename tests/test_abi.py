@@ -33,7 +33,7 @@ def test_abi_version_and_status_strings():
     from resistivemhd_gpu_b200 import _lib
 
     lib = _lib.load()
-    assert lib.rmhd2d_abi_version() == 2
+    assert lib.rmhd2d_abi_version() == 3
     for code, text in _lib.STATUS.items():
         assert lib.rmhd2d_status_string(code).decode() == text
 

@@ -15,7 +15,6 @@ pytestmark = pytest.mark.gpu
 
 ADJ_REL = 1e-10
 FD_REL = 1e-6
-HARRIS_REL = 1e-5
 
 
 def _dirs(setup, seed):
@@ -223,10 +222,9 @@ def test_adjoint_on_the_harris_sheet(gpu, tangent):
 
     Here the fast and Alfven waves meet and the HLLD star states' N and D
     are differences of nearly equal terms.  With those recomputed through
-    contracted multiply-adds the reverse was 1e-6 off on the GPU, which
-    HARRIS_REL allows; it now forms them exactly rounded, as the forward
-    does, and the CPU build of the same kernels holds ADJ_REL on this case
-    with the rest of its arithmetic contracted (tests/test_adjoint_host.py)."""
+    contracted multiply-adds the reverse was 1e-6 off; formed exactly
+    rounded, as the forward forms them, it holds ADJ_REL here as everywhere
+    (on the CPU build of the same kernels too, tests/test_adjoint_host.py)."""
     from resistivemhd_gpu_b200 import Solver, setups
 
     s = setups.harris_sheet(64, 32)
@@ -239,5 +237,5 @@ def test_adjoint_on_the_harris_sheet(gpu, tangent):
     for k in range(2):
         d, deta = _dirs(s, 200 + k)
         _, dU = tangent.tangent(s, s.state, d, dts, deta=deta)
-        assert float((gs * d).sum() + (ge * deta).sum()) == pytest.approx(float((w * dU).sum()), rel=HARRIS_REL,
+        assert float((gs * d).sum() + (ge * deta).sum()) == pytest.approx(float((w * dU).sum()), rel=ADJ_REL,
                                                                             abs=1e-14)
