@@ -201,13 +201,24 @@ int rmhd2d_load(rmhd2d_solver *s, const char *path);
    save/load round trip and by host tools. */
 int rmhd2d_write_snapshot(const char *path, const double *host_state, int nx, int ny);
 
-/* Tile shape of the fused stage kernels (0: 8x32 / 9x32 cells, 1: 16x16 /
-   18x16).  rmhd2d_autotune times trial_steps steps with each shape (the
-   state is restored afterwards) and keeps the fastest.  No counterpart in the
-   reference (its launches are fixed 16x16 thread blocks). */
+/* Tile shape of the fused stage kernels (stage 1 / stage 2 cells per CTA):
+   0: 8x32 / 9x32 and 1: 16x16 / 18x16 with 320 threads, 2 CTAs per SM;
+   2: 16x32 / 18x32 with 640 threads, 1 CTA per SM (fewer redundant ring
+   fluxes per cell).  Each stage has its own shape: rmhd2d_set_tile_shape
+   sets both, rmhd2d_set_stage_shapes each, rmhd2d_get_tile_shape returns
+   stage 1's.  rmhd2d_autotune times trial_steps steps with each shape (CUDA
+   events around each stage's launch; the state is restored afterwards),
+   keeps the fastest shape of each stage, and returns stage 1's;
+   rmhd2d_get_tuning returns the median ms of each stage with each shape (up
+   to max entries; *n = the number of shapes tried, 0 before any autotune).
+   Results do not depend on the shapes.  No counterpart in the reference
+   (its launches are fixed 16x16 thread blocks). */
 int rmhd2d_set_tile_shape(rmhd2d_solver *s, int shape);
+int rmhd2d_set_stage_shapes(rmhd2d_solver *s, int shape1, int shape2);
 int rmhd2d_get_tile_shape(const rmhd2d_solver *s, int *shape);
+int rmhd2d_get_stage_shapes(const rmhd2d_solver *s, int *shape1, int *shape2);
 int rmhd2d_autotune(rmhd2d_solver *s, int trial_steps, int *best_shape);
+int rmhd2d_get_tuning(const rmhd2d_solver *s, int max, int *n, int *shapes, float *ms_stage1, float *ms_stage2);
 
 /* Batches of independent runs (grid size, eta, boundary kinds per run; one
    precision and device per batch), stepped together: every RK2 stage of all
@@ -223,12 +234,16 @@ int rmhd2d_batch_size(const rmhd2d_batch *b, int *nruns);
 int rmhd2d_batch_member(rmhd2d_batch *b, int run, rmhd2d_solver **member);
 int rmhd2d_batch_run(rmhd2d_batch *b, int nsteps);
 int rmhd2d_batch_run_timed(rmhd2d_batch *b, int nsteps, float *ms);
-/* Launch configuration: tile shape (0..1) and persistent CTAs per SM (1..2);
-   rmhd2d_batch_autotune times each (state restored afterwards) and keeps the
-   fastest. */
+/* Launch configuration: tile shape (0..2, as above) and persistent CTAs per
+   SM (1..2; 1 for shape 2); rmhd2d_batch_autotune times every valid pair
+   (state restored afterwards) and keeps the fastest; rmhd2d_batch_get_tuning
+   returns each pair tried with its ms per step (up to max entries, *n =
+   the number tried). */
 int rmhd2d_batch_set_launch(rmhd2d_batch *b, int shape, int ctas_per_sm);
 int rmhd2d_batch_get_launch(const rmhd2d_batch *b, int *shape, int *ctas_per_sm);
 int rmhd2d_batch_autotune(rmhd2d_batch *b, int trial_steps, int *best_shape, int *best_ctas_per_sm);
+int rmhd2d_batch_get_tuning(const rmhd2d_batch *b, int max, int *n, int *shapes, int *ctas_per_sm,
+                            float *ms_per_step);
 const char *rmhd2d_batch_last_error(const rmhd2d_batch *b);
 
 /* Discrete adjoint of the step (no counterpart in the reference).

@@ -60,6 +60,10 @@ SIGNATURES = [
     ("rmhd2d_set_tile_shape", ctypes.c_int, [_S, ctypes.c_int]),
     ("rmhd2d_get_tile_shape", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_int)]),
     ("rmhd2d_autotune", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("rmhd2d_get_tuning", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    ("rmhd2d_set_stage_shapes", ctypes.c_int, [_S, ctypes.c_int, ctypes.c_int]),
+    ("rmhd2d_get_stage_shapes", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("rmhd2d_batch_create", ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     ("rmhd2d_batch_destroy", ctypes.c_int, [_S]),
     ("rmhd2d_batch_size", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_int)]),
@@ -70,6 +74,9 @@ SIGNATURES = [
     ("rmhd2d_batch_get_launch", ctypes.c_int, [_S, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("rmhd2d_batch_autotune", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int)]),
+    ("rmhd2d_batch_get_tuning", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_float)]),
     ("rmhd2d_batch_last_error", ctypes.c_char_p, [_S]),
     ("rmhd2d_run_fixed_dt", ctypes.c_int, [_S, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     ("rmhd2d_adjoint_forward", ctypes.c_int, [_S, ctypes.c_int, ctypes.c_int]),

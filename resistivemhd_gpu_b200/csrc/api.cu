@@ -50,7 +50,8 @@ struct rmhd2d_solver {
     // per tile shape: stage-1 source A, stage-2 source B, eta plane with the
     // stage-1 and stage-2 boxes
     CUtensorMap mapA[NSHAPE]{}, mapB[NSHAPE]{}, mapE1[NSHAPE]{}, mapE2[NSHAPE]{};
-    int shape = 0;
+    int shape = 0;                       // tile shape of stage 1
+    int shape2 = 0;                      // tile shape of stage 2
     void *batch = nullptr;               // owning batch, if any
     int parity = 0;
     bool has_state = false;
@@ -60,6 +61,7 @@ struct rmhd2d_solver {
     AdjointWork *adj = nullptr;          // recorded trajectory and workspace of the discrete adjoint
     double *contact = nullptr;           // CT-Contact workspace: C, F1, G1, F2, G2 (8 planes each), R1, R2, E
     int slab = 0;                        // RMHD2D_SLAB_* flags of a slab of a decomposed domain (rmhd2d_create_slab)
+    std::vector<float> tuning_ms;        // per tile shape: median ms of stage 1 and of stage 2 in the last autotune
     std::string err;
 };
 
@@ -241,7 +243,7 @@ void enqueue_step_between(rmhd2d_solver *s, int parity, const double *un, const 
     a.src = ustar;
     a.un = un;
     a.dst = dst;
-    launch(2, s->shape, map_ustar, &s->mapE2[s->shape], a, s->stream);
+    launch(2, s->shape2, map_ustar, &s->mapE2[s->shape2], a, s->stream);
     launch_boundary(s->g, dst, s->row2, s->ctl, parity ^ 1, s->stream);
 }
 
@@ -285,7 +287,7 @@ void enqueue_step(rmhd2d_solver *s, int parity)
     a.src = s->B;
     a.un = s->A;
     a.dst = s->A;
-    launch(2, s->shape, &s->mapB[s->shape], &s->mapE2[s->shape], a, s->stream);
+    launch(2, s->shape2, &s->mapB[s->shape2], &s->mapE2[s->shape2], a, s->stream);
     launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
 }
 
@@ -741,7 +743,7 @@ int rmhd2d_profile_step(rmhd2d_solver *s, float *ms4)
     launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
     CK(cudaEventRecord(ev[2], s->stream));
     a.src = s->B; a.un = s->A; a.dst = s->A;
-    launch(2, s->shape, &s->mapB[s->shape], &s->mapE2[s->shape], a, s->stream);
+    launch(2, s->shape2, &s->mapB[s->shape2], &s->mapE2[s->shape2], a, s->stream);
     CK(cudaEventRecord(ev[3], s->stream));
     launch_boundary(s->g, s->A, s->row2, s->ctl, parity ^ 1, s->stream);
     CK(cudaEventRecord(ev[4], s->stream));
@@ -832,14 +834,39 @@ int rmhd2d_load(rmhd2d_solver *s, const char *path)
 // Tile shape and autotuning of one solver
 // ---------------------------------------------------------------------------
 
-int rmhd2d_set_tile_shape(rmhd2d_solver *s, int shape)
+int rmhd2d_set_stage_shapes(rmhd2d_solver *s, int shape1, int shape2)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
-    if (shape < 0 || shape >= NSHAPE) return fail(s, RMHD2D_ERR_INVALID, "unknown tile shape");
+    if (shape1 < 0 || shape1 >= NSHAPE || shape2 < 0 || shape2 >= NSHAPE)
+        return fail(s, RMHD2D_ERR_INVALID, "unknown tile shape");
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->stream));
     destroy_graphs(s);
-    s->shape = shape;
+    s->shape = shape1;
+    s->shape2 = shape2;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_get_stage_shapes(const rmhd2d_solver *s, int *shape1, int *shape2)
+{
+    if (!s || !shape1 || !shape2) return fail(const_cast<rmhd2d_solver *>(s), RMHD2D_ERR_INVALID, "null argument");
+    *shape1 = s->shape;
+    *shape2 = s->shape2;
+    return RMHD2D_OK;
+}
+
+int rmhd2d_set_tile_shape(rmhd2d_solver *s, int shape) { return rmhd2d_set_stage_shapes(s, shape, shape); }
+
+int rmhd2d_get_tuning(const rmhd2d_solver *s, int max, int *n, int *shapes, float *ms_stage1, float *ms_stage2)
+{
+    if (!s || !n) return fail(const_cast<rmhd2d_solver *>(s), RMHD2D_ERR_INVALID, "null argument");
+    const int k = (int)s->tuning_ms.size() / 2;
+    *n = k;
+    for (int q = 0; q < k && q < max; ++q) {
+        if (shapes) shapes[q] = q;
+        if (ms_stage1) ms_stage1[q] = s->tuning_ms[2 * q];
+        if (ms_stage2) ms_stage2[q] = s->tuning_ms[2 * q + 1];
+    }
     return RMHD2D_OK;
 }
 
@@ -894,29 +921,47 @@ int rmhd2d_autotune(rmhd2d_solver *s, int trial_steps, int *best_shape)
     if (s->g.x_halo) return refuse_halo_slab(s, "autotune");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     if (s->batch) return fail(s, RMHD2D_ERR_STATE, "member of a batch: tune the batch");
+    if (s->contact) {   // the CT-Contact pipeline does not run the tiled stage kernels
+        if (best_shape) *best_shape = s->shape;
+        return RMHD2D_OK;
+    }
     if (trial_steps < 2) trial_steps = 2;
     trial_steps += trial_steps & 1;   // even: the step parity comes back
     CK(cudaSetDevice(s->device));
     Snapshot sn;
     int rc = snapshot_take(s, sn);
     if (rc) return rc;
-    float best = 1e30f;
-    int best_sh = s->shape;
+    // Each stage's launch is timed by itself (the two stages read and write
+    // different tiles and buffers), so the fastest shape is picked per stage:
+    // the median over trial steps of each stage's CUDA-event time.
+    s->tuning_ms.assign(2 * NSHAPE, 0.f);
     for (int sh = 0; sh < NSHAPE && rc == RMHD2D_OK; ++sh) {
-        rc = rmhd2d_set_tile_shape(s, sh);
-        float warm = 0.f, ms = 0.f;
-        if (!rc) rc = rmhd2d_run_timed(s, 2, &warm);             // graph capture + warm-up
-        if (!rc) rc = rmhd2d_run_timed(s, trial_steps, &ms);
-        if (!rc && ms < best) {
-            best = ms;
-            best_sh = sh;
+        rc = rmhd2d_set_stage_shapes(s, sh, sh);
+        if (!rc) rc = rmhd2d_run(s, 2);                          // warm-up
+        std::vector<float> t1, t2;
+        for (int k = 0; k < trial_steps && !rc; ++k) {
+            float ms4[4];
+            rc = rmhd2d_profile_step(s, ms4);
+            t1.push_back(ms4[0]);
+            t2.push_back(ms4[2]);
+        }
+        if (!rc) {
+            std::sort(t1.begin(), t1.end());
+            std::sort(t2.begin(), t2.end());
+            s->tuning_ms[2 * sh] = t1[t1.size() / 2];
+            s->tuning_ms[2 * sh + 1] = t2[t2.size() / 2];
         }
     }
     const int rc2 = snapshot_restore(s, sn);
     if (rc) return rc;
     if (rc2) return rc2;
-    rc = rmhd2d_set_tile_shape(s, best_sh);
-    if (best_shape) *best_shape = best_sh;
+    int b1 = 0, b2 = 0;
+    for (int sh = 1; sh < NSHAPE; ++sh) {
+        if (s->tuning_ms[2 * sh] < s->tuning_ms[2 * b1]) b1 = sh;
+        if (s->tuning_ms[2 * sh + 1] < s->tuning_ms[2 * b2 + 1]) b2 = sh;
+    }
+    rc = rmhd2d_set_stage_shapes(s, b1, b2);
+    if (best_shape) *best_shape = b1;
     return rc;
 }
 
@@ -944,6 +989,9 @@ struct rmhd2d_batch {
     int ntiles[2] = {0, 0};
     bool dirty = true;
     cudaGraphExec_t graph2[2] = {nullptr, nullptr};
+    // (tile shape, CTAs per SM, ms per step) of each point of the last rmhd2d_batch_autotune
+    std::vector<int> tune_shape, tune_ctas;
+    std::vector<float> tune_ms;
     std::string err;
 };
 
@@ -1135,8 +1183,8 @@ int rmhd2d_batch_member(rmhd2d_batch *b, int run, rmhd2d_solver **out)
 int rmhd2d_batch_set_launch(rmhd2d_batch *b, int shape, int ctas_per_sm)
 {
     if (!b) return bfail(b, RMHD2D_ERR_INVALID, "null batch");
-    if (shape < 0 || shape >= NSHAPE || ctas_per_sm < 1 || ctas_per_sm > 2)
-        return bfail(b, RMHD2D_ERR_INVALID, "tile shape must be 0..1 and CTAs per SM 1..2");
+    if (shape < 0 || shape >= NSHAPE || ctas_per_sm < 1 || ctas_per_sm > shape_max_ctas(shape))
+        return bfail(b, RMHD2D_ERR_INVALID, "tile shape must be 0..2 and CTAs per SM 1..2 (1 for shape 2)");
     b->shape = shape;
     b->ctas_per_sm = ctas_per_sm;
     b->dirty = true;
@@ -1223,12 +1271,20 @@ int rmhd2d_batch_autotune(rmhd2d_batch *b, int trial_steps, int *best_shape, int
     const long long steps0 = b->steps;
     float best = 1e30f;
     int bs = b->shape, bc = b->ctas_per_sm, rc = RMHD2D_OK;
+    b->tune_shape.clear();
+    b->tune_ctas.clear();
+    b->tune_ms.clear();
     for (int sh = 0; sh < NSHAPE && !rc; ++sh)
-        for (int c = 1; c <= 2 && !rc; ++c) {
+        for (int c = 1; c <= shape_max_ctas(sh) && !rc; ++c) {
             rc = rmhd2d_batch_set_launch(b, sh, c);
             float warm = 0.f, ms = 0.f;
             if (!rc) rc = rmhd2d_batch_run_timed(b, 2, &warm);
             if (!rc) rc = rmhd2d_batch_run_timed(b, trial_steps, &ms);
+            if (!rc) {
+                b->tune_shape.push_back(sh);
+                b->tune_ctas.push_back(c);
+                b->tune_ms.push_back(ms / trial_steps);
+            }
             if (!rc && ms < best) {
                 best = ms;
                 bs = sh;
@@ -1248,6 +1304,19 @@ int rmhd2d_batch_autotune(rmhd2d_batch *b, int trial_steps, int *best_shape, int
     if (best_shape) *best_shape = bs;
     if (best_ctas_per_sm) *best_ctas_per_sm = bc;
     return rc;
+}
+
+int rmhd2d_batch_get_tuning(const rmhd2d_batch *b, int max, int *n, int *shapes, int *ctas_per_sm, float *ms_per_step)
+{
+    if (!b || !n) return bfail(const_cast<rmhd2d_batch *>(b), RMHD2D_ERR_INVALID, "null argument");
+    const int k = (int)b->tune_ms.size();
+    *n = k;
+    for (int q = 0; q < k && q < max; ++q) {
+        if (shapes) shapes[q] = b->tune_shape[q];
+        if (ctas_per_sm) ctas_per_sm[q] = b->tune_ctas[q];
+        if (ms_per_step) ms_per_step[q] = b->tune_ms[q];
+    }
+    return RMHD2D_OK;
 }
 
 const char *rmhd2d_batch_last_error(const rmhd2d_batch *b)
@@ -1406,7 +1475,7 @@ int rmhd2d_slab_stage(rmhd2d_solver *s, int stage)
         a.src = s->B;
         a.un = s->A;
         a.dst = s->A;
-        launch(2, s->shape, &s->mapB[s->shape], &s->mapE2[s->shape], a, s->stream);
+        launch(2, s->shape2, &s->mapB[s->shape2], &s->mapE2[s->shape2], a, s->stream);
     }
     CK(cudaGetLastError());
     return RMHD2D_OK;
@@ -1569,7 +1638,7 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
         w->map1.resize(nsteps);
         for (int k = 0; k < nsteps; ++k)
             if (!encode_state_map(&w->map0[k], g, w->seg0 + (size_t)k * sd, stage_ui(1, s->shape), shape_uj(s->shape)) ||
-                !encode_state_map(&w->map1[k], g, w->seg1 + (size_t)k * sd, stage_ui(2, s->shape), shape_uj(s->shape)))
+                !encode_state_map(&w->map1[k], g, w->seg1 + (size_t)k * sd, stage_ui(2, s->shape2), shape_uj(s->shape2)))
                 return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint's trajectory slots");
         CK(cudaMemcpyAsync(w->seg0, s->A, sd * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
         for (int n = 0; n < nsteps; ++n) {
@@ -1633,7 +1702,7 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
         w->map1.resize(w->interval);
         for (int k = 0; k < w->interval; ++k)
             if (!encode_state_map(&w->map0[k], g, w->seg0 + (size_t)k * sd, stage_ui(1, s->shape), shape_uj(s->shape)) ||
-                !encode_state_map(&w->map1[k], g, w->seg1 + (size_t)k * sd, stage_ui(2, s->shape), shape_uj(s->shape)))
+                !encode_state_map(&w->map1[k], g, w->seg1 + (size_t)k * sd, stage_ui(2, s->shape2), shape_uj(s->shape2)))
                 return fail(s, RMHD2D_ERR_CUDA, "cuTensorMapEncodeTiled failed for the adjoint's segment states");
     }
     int rc = set_fixed_dt_mode(s, 1);

@@ -47,18 +47,30 @@ enum KernelError { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };
 
 // Tiles of the fused stage kernels: TI cells along x (i) by TJ along y (j).
 // Stage 1 also computes the ring of fluxes its corner EMF needs, stage 2
-// only the tile's own interfaces, so their best tile heights differ.  With
-// 320 threads both shapes fill two nearly full rounds of interfaces:
-//   shape 0: stage 1  8 x 32 (636 interfaces), stage 2  9 x 32 (617)
-//   shape 1: stage 1 16 x 16 (612 interfaces), stage 2 18 x 16 (610)
+// only the tile's own interfaces, so their best tile heights differ.
+//   shape 0: stage 1  8 x 32 (636 interfaces), stage 2  9 x 32 (617); 320 threads, 2 CTAs per SM
+//   shape 1: stage 1 16 x 16 (612 interfaces), stage 2 18 x 16 (610); 320 threads, 2 CTAs per SM
+//   shape 2: stage 1 16 x 32 (1172),           stage 2 18 x 32 (1202); 640 threads, 1 CTA per SM
+// Shape 2 forms 2.29 (stage 1) and 2.09 (stage 2) interfaces per cell
+// against 2.48 and 2.14, at the same 20 warps per SM, but one CTA per SM
+// leaves no second CTA to run while the first waits at a barrier; which
+// is faster is the autotuners' question.
 constexpr int HALO = 3;
-constexpr int NSHAPE = 2;
-constexpr int STAGE_THREADS = 320;
-constexpr int shape_tj(int shape) { return shape == 0 ? 32 : 16; }
+constexpr int NSHAPE = 3;
+constexpr int shape_tj(int shape) { return shape == 1 ? 16 : 32; }
 constexpr int stage_ti(int stage, int shape) { return shape == 0 ? (stage == 1 ? 8 : 9) : (stage == 1 ? 16 : 18); }
 constexpr int stage_ui(int stage, int shape) { return stage_ti(stage, shape) + 2 * HALO; }
 constexpr int shape_uj(int shape) { return shape_tj(shape) + 2 * HALO; }  // TMA inner box: UJ * 8 B, a multiple of 16
-static_assert(STAGE_THREADS >= 9 * 32 && STAGE_THREADS >= 18 * 16, "one thread per tile cell in the update phase");
+constexpr int shape_threads(int shape) { return shape == 2 ? 640 : 320; }
+constexpr int shape_max_ctas(int shape) { return shape == 2 ? 1 : 2; }   // CTAs per SM that fit
+constexpr bool shapes_have_a_thread_per_cell()
+{
+    for (int s = 0; s < NSHAPE; ++s)
+        if (shape_threads(s) < stage_ti(2, s) * shape_tj(s) || shape_threads(s) < stage_ti(1, s) * shape_tj(s))
+            return false;
+    return true;
+}
+static_assert(shapes_have_a_thread_per_cell(), "one thread per tile cell in the update phase");
 
 // Per-run record of a batch (device memory), and one entry of a batch's tile
 // table.

@@ -82,9 +82,11 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr size_t SMEM_BYTES = OFF_BAR + 16;
     static constexpr unsigned U_BYTES = (unsigned)U_BYTES_;
     static constexpr unsigned E_BYTES = (unsigned)E_BYTES_;
-    static_assert(STAGE_THREADS / 32 * 8 <= PB_BYTES, "per-warp maxima must fit in the primitive region");
-    // Two CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA).
-    static_assert(SMEM_BYTES <= 113 * 1024, "shared memory for two CTAs per SM");
+    static constexpr int THREADS = shape_threads(SHAPE);
+    static constexpr int CTAS = shape_max_ctas(SHAPE);
+    static_assert(THREADS / 32 * 8 <= PB_BYTES, "per-warp maxima must fit in the primitive region");
+    // CTAS CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA).
+    static_assert(SMEM_BYTES <= (CTAS == 2 ? 113 : 227) * 1024, "shared memory for the CTAs per SM");
 };
 
 // velocity planes (Pv) and B / pressure planes (Pb); rho and bZ are read from
@@ -232,7 +234,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
     // calculate_half_Q.cu:4-38 on the centred state (shift kernels,
     // resistiveMHD_2D.cu:313-337), once for the x sweep and once for the
     // permuted y sweep (hlld.cu:134-152), whose pressure sums in another order.
-    for (int c = tid; c < PF; c += STAGE_THREADS) {
+    for (int c = tid; c < PF; c += T::THREADS) {
         const int pi = c / PJ_, pj = c - pi * PJ_;
         const double *u0 = Ut + (pi + 1) * UJ + (pj + 1);
         const double rho = u0[RHO * UF];
@@ -282,7 +284,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
 #if RMHD_FAST_MATH
         const Real i2dx = (Real)(1.0 / two_dx), i2dy = (Real)(1.0 / two_dy);
 #endif
-        for (int c = tid; c < RF; c += STAGE_THREADS) {
+        for (int c = tid; c < RF; c += T::THREADS) {
             const int ri = c / RJ_, rj = c - ri * RJ_;
             const double *p0 = Pb + (ri + 1) * PJ_ + (rj + 1);
             const double *z0 = Ut + BZF * UF + (ri + 2) * UJ + (rj + 2);
@@ -461,7 +463,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
             if (STAGE == 1) oo[O_EMF * SG] = fov[1] + h * (eZ0 + eZ1);
         }
     };
-    for (int it = tid; it < T::NF + T::NG; it += STAGE_THREADS) {
+    for (int it = tid; it < T::NF + T::NG; it += T::THREADS) {
         if (STAGE == 1 || !RMHD_FAST_MATH)
             flux_at(it, SweepRT{it < T::NF});
         else if (it < T::NF)
@@ -486,7 +488,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
     if (STAGE == 1) {
         // ---- corner EMF (ct.cu:22-41) on (TI+1) x (TJ+1) corners (i, j) =
         // (i0-1+ei, j0-1+ej), i.e. Fs (fi, fj) = (ei, ej) and Gs (gi, gj) = (ei, ej) ----
-        for (int c = tid; c < T::EI_ * EJ_; c += STAGE_THREADS) {
+        for (int c = tid; c < T::EI_ * EJ_; c += T::THREADS) {
             const int ei = c / EJ_, ej = c - ei * EJ_;
             // accumulated in FP64 whatever the flux-side type
             const double eZG1 = (double)Go[O_EMF * SG + ei * G_NJ + ej];
@@ -576,7 +578,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
         const int any_nan = __syncthreads_or(nan_e);
         if (tid == 0) {
             unsigned long long m = 0ull;
-            for (int w = 0; w < STAGE_THREADS / 32; ++w) m = wmax[w] > m ? wmax[w] : m;
+            for (int w = 0; w < T::THREADS / 32; ++w) m = wmax[w] > m ? wmax[w] : m;
             atomicMax(&a.ctl->amax[a.parity ^ 1], m);
             if (any_nan) atomicExch(&a.ctl->crashed, 1);
         }
@@ -592,7 +594,7 @@ __device__ __forceinline__ void init_tile_barrier(uint64_t *bar)
 
 // One CTA per tile of one run.
 template <int STAGE, int SHAPE>
-__global__ void __launch_bounds__(STAGE_THREADS, 2)
+__global__ void __launch_bounds__(shape_threads(SHAPE), shape_max_ctas(SHAPE))
 stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap emap,
              const StageArgs a)
 {
@@ -607,7 +609,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
 // Persistent CTAs over the tile table of a batch of independent runs (each
 // with its own grid, eta, state buffers, tensor maps and control block).
 template <int STAGE, int SHAPE>
-__global__ void __launch_bounds__(STAGE_THREADS, 2)
+__global__ void __launch_bounds__(shape_threads(SHAPE), shape_max_ctas(SHAPE))
 stage_batch_kernel(const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles, int ntiles, int parity)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -641,14 +643,16 @@ template <int STAGE, int SHAPE> constexpr size_t smem_of() { return Tile<STAGE, 
 size_t stage_smem_bytes(int stage, int shape)
 {
     if (shape == 0) return stage == 1 ? smem_of<1, 0>() : smem_of<2, 0>();
-    return stage == 1 ? smem_of<1, 1>() : smem_of<2, 1>();
+    if (shape == 1) return stage == 1 ? smem_of<1, 1>() : smem_of<2, 1>();
+    return stage == 1 ? smem_of<1, 2>() : smem_of<2, 2>();
 }
 
 int stage_regs(int stage, int shape)
 {
     cudaFuncAttributes attr{};
     const void *f = shape == 0 ? (stage == 1 ? (const void *)stage_kernel<1, 0> : (const void *)stage_kernel<2, 0>)
-                               : (stage == 1 ? (const void *)stage_kernel<1, 1> : (const void *)stage_kernel<2, 1>);
+                  : shape == 1 ? (stage == 1 ? (const void *)stage_kernel<1, 1> : (const void *)stage_kernel<2, 1>)
+                               : (stage == 1 ? (const void *)stage_kernel<1, 2> : (const void *)stage_kernel<2, 2>);
     cudaFuncGetAttributes(&attr, f);
     return attr.numRegs;
 }
@@ -659,7 +663,7 @@ static void launch_one(const CUtensorMap *tmap, const CUtensorMap *emap, const S
     using T = Tile<STAGE, SHAPE>;
     cudaFuncSetAttribute(stage_kernel<STAGE, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_BYTES);
     const dim3 grid((args.g.ny - 2 * HALO + T::TJ - 1) / T::TJ, (args.g.nx - 2 * HALO + T::TI - 1) / T::TI);
-    stage_kernel<STAGE, SHAPE><<<grid, STAGE_THREADS, T::SMEM_BYTES, stream>>>(*tmap, *emap, args);
+    stage_kernel<STAGE, SHAPE><<<grid, T::THREADS, T::SMEM_BYTES, stream>>>(*tmap, *emap, args);
 }
 
 void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
@@ -668,9 +672,12 @@ void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorM
     if (shape == 0) {
         if (stage == 1) launch_one<1, 0>(tmap, emap, args, stream);
         else launch_one<2, 0>(tmap, emap, args, stream);
-    } else {
+    } else if (shape == 1) {
         if (stage == 1) launch_one<1, 1>(tmap, emap, args, stream);
         else launch_one<2, 1>(tmap, emap, args, stream);
+    } else {
+        if (stage == 1) launch_one<1, 2>(tmap, emap, args, stream);
+        else launch_one<2, 2>(tmap, emap, args, stream);
     }
 }
 
@@ -681,7 +688,7 @@ static void launch_batch_one(const BatchRun *runs, const CUtensorMap *maps, cons
     using T = Tile<STAGE, SHAPE>;
     cudaFuncSetAttribute(stage_batch_kernel<STAGE, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)T::SMEM_BYTES);
-    stage_batch_kernel<STAGE, SHAPE><<<ctas, STAGE_THREADS, T::SMEM_BYTES, stream>>>(runs, maps, tiles, ntiles, parity);
+    stage_batch_kernel<STAGE, SHAPE><<<ctas, T::THREADS, T::SMEM_BYTES, stream>>>(runs, maps, tiles, ntiles, parity);
 }
 
 void launch_stage_batch(int stage, int shape, const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles,
@@ -690,9 +697,12 @@ void launch_stage_batch(int stage, int shape, const BatchRun *runs, const CUtens
     if (shape == 0) {
         if (stage == 1) launch_batch_one<1, 0>(runs, maps, tiles, ntiles, ctas, parity, stream);
         else launch_batch_one<2, 0>(runs, maps, tiles, ntiles, ctas, parity, stream);
-    } else {
+    } else if (shape == 1) {
         if (stage == 1) launch_batch_one<1, 1>(runs, maps, tiles, ntiles, ctas, parity, stream);
         else launch_batch_one<2, 1>(runs, maps, tiles, ntiles, ctas, parity, stream);
+    } else {
+        if (stage == 1) launch_batch_one<1, 2>(runs, maps, tiles, ntiles, ctas, parity, stream);
+        else launch_batch_one<2, 2>(runs, maps, tiles, ntiles, ctas, parity, stream);
     }
 }
 

@@ -211,6 +211,23 @@ class Solver:
         self._ck(self._lib.rmhd2d_autotune(self._h, int(trial_steps), ctypes.byref(v)))
         return v.value
 
+    def tuning(self) -> dict[int, tuple[float, float]]:
+        """Tile shape -> (stage-1 ms, stage-2 ms) measured by the last autotune."""
+        n = ctypes.c_int()
+        sh = (ctypes.c_int * 8)()
+        m1, m2 = (ctypes.c_float * 8)(), (ctypes.c_float * 8)()
+        self._ck(self._lib.rmhd2d_get_tuning(self._h, 8, ctypes.byref(n), sh, m1, m2))
+        return {int(sh[q]): (float(m1[q]), float(m2[q])) for q in range(min(n.value, 8))}
+
+    @property
+    def stage_shapes(self) -> tuple[int, int]:
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._ck(self._lib.rmhd2d_get_stage_shapes(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def set_stage_shapes(self, shape1: int, shape2: int) -> None:
+        self._ck(self._lib.rmhd2d_set_stage_shapes(self._h, int(shape1), int(shape2)))
+
     def run_timed(self, nsteps: int) -> float:
         """run(nsteps) timed with CUDA events on the solver's stream; ms."""
         ms = ctypes.c_float()
@@ -307,6 +324,14 @@ class Batch:
         a, b = ctypes.c_int(), ctypes.c_int()
         self._ck(self._lib.rmhd2d_batch_autotune(self._h, int(trial_steps), ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def tuning(self) -> list[tuple[int, int, float]]:
+        """(tile shape, CTAs per SM, ms per step) of each point the last autotune tried."""
+        n = ctypes.c_int()
+        sh, ct = (ctypes.c_int * 16)(), (ctypes.c_int * 16)()
+        ms = (ctypes.c_float * 16)()
+        self._ck(self._lib.rmhd2d_batch_get_tuning(self._h, 16, ctypes.byref(n), sh, ct, ms))
+        return [(int(sh[q]), int(ct[q]), float(ms[q])) for q in range(min(n.value, 16))]
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:

@@ -37,7 +37,10 @@ def single(setup, nsteps, precision, shape=0):
     from resistivemhd_gpu_b200 import Solver
 
     with Solver.from_setup(setup, precision=precision) as s:
-        s.set_tile_shape(shape)
+        if isinstance(shape, tuple):
+            s.set_stage_shapes(*shape)        # (stage 1, stage 2)
+        else:
+            s.set_tile_shape(shape)
         dts = []
         for _ in range(nsteps):
             s.step()
@@ -58,19 +61,20 @@ def mixed_setups():
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
-def test_tile_shape_1_equals_shape_0(gpu, precision):
+@pytest.mark.parametrize("shape", [1, 2, (1, 0), (2, 1)])
+def test_tile_shapes_equal_shape_0(gpu, precision, shape):
     from resistivemhd_gpu_b200 import setups
 
     s = setups.random_smooth_state(45, 39, seed=4, bc="symmetric", with_table=True)
     a, da, _ = single(s, 6, precision, shape=0)
-    b, db, _ = single(s, 6, precision, shape=1)
+    b, db, _ = single(s, 6, precision, shape=shape)
     rel = {"fp64_exact": 0.0, "fp64_fast": 1e-12, "fp32_bulk": 1e-6}[precision]
     assert db == pytest.approx(da, rel=rel, abs=0)
-    assert_same(b, a, precision, "shape 1")
+    assert_same(b, a, precision, f"shape {shape}")
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
-@pytest.mark.parametrize("launch", [(0, 2), (1, 1)])
+@pytest.mark.parametrize("launch", [(0, 2), (1, 1), (2, 1)])
 def test_batch_equals_single_runs(gpu, precision, launch):
     from resistivemhd_gpu_b200 import Batch
 
@@ -108,7 +112,10 @@ def test_batch_autotune_restores_state(gpu):
     with Batch(sets, precision="fp64_fast") as b:
         before = [b[r].get_state().copy() for r in range(len(b))]
         shape, ctas = b.autotune(trial_steps=2)
-        assert shape in (0, 1) and ctas in (1, 2)
+        assert shape in (0, 1, 2) and ctas in (1, 2)
+        table = b.tuning()
+        assert [(sh, c) for sh, c, _ in table] == [(0, 1), (0, 2), (1, 1), (1, 2), (2, 1)]
+        assert all(m > 0 for _, _, m in table)
         assert b.launch == (shape, ctas)
         for r in range(len(b)):
             assert np.array_equal(b[r].get_state(), before[r])
@@ -137,5 +144,9 @@ def test_solver_autotune(gpu):
     with Solver.from_setup(s, precision="fp64_fast") as sol:
         before = sol.get_state().copy()
         shape = sol.autotune(trial_steps=2)
-        assert shape in (0, 1) and sol.tile_shape == shape
+        assert shape in (0, 1, 2) and sol.tile_shape == shape
+        t = sol.tuning()
+        assert sorted(t) == [0, 1, 2] and all(a > 0 and b > 0 for a, b in t.values())
+        s1, s2 = sol.stage_shapes
+        assert s1 == shape and t[s2][1] == min(b for _, b in t.values())
         assert np.array_equal(sol.get_state(), before)
