@@ -580,7 +580,11 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
     const float dpT = (float)(pTL64 - pTR64);
     const float pL = (float)s.pL, pR = (float)s.pR;
     const float bYL = (float)s.bYL, bYR = (float)s.bYR, bZL = (float)s.bZL, bZR = (float)s.bZR;
-    const float b2L = (float)b2L64, b2R = (float)b2R64, pTL = (float)pTL64, pTR = (float)pTR64;
+    // the fan's own magnetic and total pressures in single precision (the
+    // FP64 ones above carry the stresses and the pressure difference)
+    const float bt2L = bYL * bYL + bZL * bZL, bt2R = bYR * bYR + bZR * bZR;
+    const float b2L = bx2 + bt2L, b2R = bx2 + bt2R;
+    const float pTL = pL + 0.5f * b2L, pTR = pR + 0.5f * b2R;
     const float rhoL = s.rhoL, rhoR = s.rhoR, uL = s.uL, uR = s.uR, vL = s.vL, vR = s.vR, wL = s.wL, wR = s.wR;
 
     const float iRL = rcp_nr(rhoL), iRR = rcp_nr(rhoR);
@@ -594,7 +598,6 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
     const bool okR = (cs2R >= 0.f) & (ca2R >= 0.f) & (va2R >= 0.f);
     // discriminant without cancellation, as in hlld_flux_fast
     const float dcL = cs2L - ca2L, dcR = cs2R - ca2R;
-    const float bt2L = (float)(s.bYL * s.bYL + s.bZL * s.bZL), bt2R = (float)(s.bYR * s.bYR + s.bZR * s.bZR);
     const float discL = dcL * dcL + 4.f * cs2L * bt2L * iRL, discR = dcR * dcR + 4.f * cs2R * bt2R * iRR;
     const float cfL = okL ? sqrt_t(0.5f * (sL + sqrt_t(discL))) : qnan;
     const float cfR = okR ? sqrt_t(0.5f * (sR + sqrt_t(discR))) : qnan;

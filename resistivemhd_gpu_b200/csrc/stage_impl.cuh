@@ -25,6 +25,12 @@
 namespace rmhd2d {
 namespace RMHD_VARIANT {
 
+// Threads per CTA of a tile shape in this variant: FP32-bulk runs shapes 0
+// and 1 with 384 threads (at 80 registers; its single-precision flux body
+// spills little there, and 24 warps per SM measured 3-6 % faster than 20),
+// the FP64 variants with 320 (their FP64 bodies spill twice as much at 80).
+constexpr int variant_threads(int shape) { return shape == 2 ? shape_threads(2) : (RMHD_BULK ? 384 : shape_threads(shape)); }
+
 // ---- per-stage tile geometry and shared-memory carve-up ----
 // Ut [8][UI][UJ] f64     TMA: U at i0-3..i0+TI+2, j0-3..j0+TJ+2 (kept for the whole CTA)
 // Et [UI][UJ] f64        TMA: eta table on the same cells (when a table is set)
@@ -61,7 +67,8 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr size_t up16(size_t b) { return (b + 15) / 16 * 16; }
     static constexpr size_t U_BYTES_ = (size_t)NFIELD * UF * 8;
     static constexpr size_t E_BYTES_ = (size_t)UF * 8;
-    static constexpr size_t PV_BYTES = up16((size_t)3 * PF * sizeof(Real));
+    static constexpr int NPV = RMHD_BULK ? 4 : 3;            // FP32-bulk also keeps rho in single precision
+    static constexpr size_t PV_BYTES = up16((size_t)NPV * PF * sizeof(Real));
     static constexpr size_t PB_BYTES = up16((size_t)4 * PF * 8);
     static constexpr size_t R_ETA = (size_t)3 * RF * sizeof(Real);
     static constexpr size_t R_EMF = STAGE == 1 ? (size_t)EI_ * EJ_ * 8 : 0;
@@ -82,7 +89,7 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr size_t SMEM_BYTES = OFF_BAR + 16;
     static constexpr unsigned U_BYTES = (unsigned)U_BYTES_;
     static constexpr unsigned E_BYTES = (unsigned)E_BYTES_;
-    static constexpr int THREADS = shape_threads(SHAPE);
+    static constexpr int THREADS = variant_threads(SHAPE);
     static constexpr int CTAS = shape_max_ctas(SHAPE);
     static_assert(THREADS / 32 * 8 <= PB_BYTES, "per-warp maxima must fit in the primitive region");
     // CTAS CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA).
@@ -91,7 +98,7 @@ template <int STAGE, int SHAPE> struct Tile {
 
 // velocity planes (Pv) and B / pressure planes (Pb); rho and bZ are read from
 // the staged tile
-enum { V_U = 0, V_V, V_W };
+enum { V_U = 0, V_V, V_W, V_RHO };
 enum { B_XC = 0, B_YC, B_PX, B_PY };
 // eta*J planes in Rs
 enum { R_JX = 0, R_JY, R_JZ };
@@ -269,6 +276,9 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
         v0[V_U * PF] = (Real)u;
         v0[V_V * PF] = (Real)v;
         v0[V_W * PF] = (Real)w;
+#if RMHD_BULK
+        v0[V_RHO * PF] = (Real)rho;
+#endif
         double *b0 = Pb + c;
         b0[B_XC * PF] = bXc;
         b0[B_YC * PF] = bYc;
@@ -362,11 +372,11 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
             const float EPSF = (float)EPS;
             BulkStates st;
             {
-                const double *q = uc + RHO * UF;
-                double a0d, a1d;
-                muscl_dev(q[-us], q[0], q[us], q[2 * us], EPSF, a0d, a1d);
-                st.rhoL = (float)a0d;
-                st.rhoR = (float)a1d;
+                // density: MUSCL in single precision from the staged copy
+                const Real *q = vc + V_RHO * PF;
+                const float qm = q[-ps], q0 = q[0], qp = q[ps], qpp = q[2 * ps];
+                st.rhoL = q0 + 0.5f * minmod(q0 - qm, qp - q0, EPSF);
+                st.rhoR = qp - 0.5f * minmod(qp - q0, qpp - qp, EPSF);
             }
             {
                 const Real *q = vc + pu * PF;
@@ -594,7 +604,7 @@ __device__ __forceinline__ void init_tile_barrier(uint64_t *bar)
 
 // One CTA per tile of one run.
 template <int STAGE, int SHAPE>
-__global__ void __launch_bounds__(shape_threads(SHAPE), shape_max_ctas(SHAPE))
+__global__ void __launch_bounds__(variant_threads(SHAPE), shape_max_ctas(SHAPE))
 stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap emap,
              const StageArgs a)
 {
@@ -609,7 +619,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
 // Persistent CTAs over the tile table of a batch of independent runs (each
 // with its own grid, eta, state buffers, tensor maps and control block).
 template <int STAGE, int SHAPE>
-__global__ void __launch_bounds__(shape_threads(SHAPE), shape_max_ctas(SHAPE))
+__global__ void __launch_bounds__(variant_threads(SHAPE), shape_max_ctas(SHAPE))
 stage_batch_kernel(const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles, int ntiles, int parity)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
