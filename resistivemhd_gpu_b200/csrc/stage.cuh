@@ -13,7 +13,8 @@
 // cells (TI = 8 in stage 1, 9 in stage 2, TJ = 32) and stages them with a 3-cell halo on every side by one 3-D TMA load
 // (box TJ+6 x TI+6 x 8 fields) into shared memory, plus a 2-D TMA load of the
 // eta table on the same cells; everything after those loads reads shared
-// memory, except stage 2's read of U^n at its own cells.
+// memory, except the update's read of its own cell of the stage's source
+// state (and, in stage 2, of U^n).
 //
 // The kernel is compiled three times: an "exact" variant (-fmad=false, all
 // six HLLD candidate fluxes formed), bit-identical to the reference
@@ -34,7 +35,7 @@ namespace rmhd2d {
 
 struct StageArgs {
     Grid g;
-    const double *src;   // state this stage reads (TMA source); stage 2: U*
+    const double *src;   // state this stage reads (TMA source, and own cells in the update); stage 2: U*
     const double *un;    // stage 2: U^n (hydro fields read at own cells)
     double *dst;         // planes written (stage 1: U*; stage 2: U^n in place)
     const double *eta;   // cell-centred eta plane or nullptr (uniform g.eta)

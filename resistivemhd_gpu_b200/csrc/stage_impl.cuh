@@ -25,23 +25,37 @@
 namespace rmhd2d {
 namespace RMHD_VARIANT {
 
-// Threads per CTA of a tile shape in this variant: FP32-bulk runs shapes 0
-// and 1 with 384 threads (at 80 registers; its single-precision flux body
-// spills little there, and 24 warps per SM measured 3-6 % faster than 20),
-// the FP64 variants with 320 (their FP64 bodies spill twice as much at 80).
-constexpr int variant_threads(int shape) { return shape == 2 ? shape_threads(2) : (RMHD_BULK ? 384 : shape_threads(shape)); }
+// Threads per CTA of a stage and tile shape in this variant.  Shapes 0 and 1
+// run at 384 threads (80 registers, 24 warps per SM) where that measured
+// faster than 320 (96 registers, 20 warps): both stages of FP32-bulk, whose
+// single-precision flux body spills little at 80 registers (3-7 %), and
+// stage 1 of FP64-fast (3 %).  The exact variant and FP64-fast's stage 2
+// keep 320: at 80 registers their FP64 bodies spill 550-590 bytes and were
+// 2-8 % slower.
+constexpr int variant_threads(int stage, int shape)
+{
+    return shape == 2 ? shape_threads(2)
+                      : ((RMHD_BULK || (RMHD_FAST_MATH && stage == 1)) ? 384 : shape_threads(shape));
+}
 
 // ---- per-stage tile geometry and shared-memory carve-up ----
-// Ut [8][UI][UJ] f64     TMA: U at i0-3..i0+TI+2, j0-3..j0+TJ+2 (kept for the whole CTA)
+// Ut [8][UI][UJ] f64     TMA: U at i0-3..i0+TI+2, j0-3..j0+TJ+2
 // Et [UI][UJ] f64        TMA: eta table on the same cells (when a table is set)
-// Pv [3][TI+4][TJ+4]     u, v, w (flux-side type)
-// Pb [4][TI+4][TJ+4] f64 centred bX, centred bY, x- and y-sweep pressures
+// Pv [4][TI+4][TJ+4]     u, v, w, rho (flux-side type)
+// Pb [5][TI+4][TJ+4] f64 centred bX, centred bY, x- and y-sweep pressures, bZ
 // Rs [3][TI+2][TJ+2]     eta*Jx, eta*Jy, eta*Jz (flux-side type); reused for the corner EMF (f64)
 // Fm [3][TI+1][F_NJ] f64 x fluxes of rhoU, rhoV, rhoW at i+1/2
 // Fo [NO][TI+1][F_NJ]    x fluxes of rho, bZ, e (+ bY = EMF part, stage 1), flux-side type
 // Gm, Go                 the same for the y fluxes at j+1/2 (Go slot 3: the bX flux)
 // Stage 1 needs x fluxes on rows j0-1..j0+TJ and y fluxes on columns
 // i0-1..i0+TI for its corner EMF; stage 2 only the tile's own interfaces.
+// Ut is read only by the primitive phase and Et by the eta*J phase, which
+// copy into Pv / Pb what the later phases need (rho, bZ); the update reads
+// its own cell from global memory.  So Rs can overlay Ut, and the flux
+// planes both: about 73 KB per CTA instead of 104-113 KB in shape 0, so
+// that two CTAs take 164 KB of the SM's unified L1 / shared memory and
+// leave 92 KB (instead of 28) to the cache, where the flux phase's register
+// spills go.
 template <int STAGE, int SHAPE> struct Tile {
     using Real = RMHD_REAL;                                  // flux-side arithmetic type
     static constexpr int TI = stage_ti(STAGE, SHAPE);
@@ -67,9 +81,8 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr size_t up16(size_t b) { return (b + 15) / 16 * 16; }
     static constexpr size_t U_BYTES_ = (size_t)NFIELD * UF * 8;
     static constexpr size_t E_BYTES_ = (size_t)UF * 8;
-    static constexpr int NPV = RMHD_BULK ? 4 : 3;            // FP32-bulk also keeps rho in single precision
-    static constexpr size_t PV_BYTES = up16((size_t)NPV * PF * sizeof(Real));
-    static constexpr size_t PB_BYTES = up16((size_t)4 * PF * 8);
+    static constexpr size_t PV_BYTES = up16((size_t)4 * PF * sizeof(Real));
+    static constexpr size_t PB_BYTES = up16((size_t)5 * PF * 8);
     static constexpr size_t R_ETA = (size_t)3 * RF * sizeof(Real);
     static constexpr size_t R_EMF = STAGE == 1 ? (size_t)EI_ * EJ_ * 8 : 0;
     static constexpr size_t R_BYTES = up16(R_ETA > R_EMF ? R_ETA : R_EMF);
@@ -77,29 +90,37 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr size_t FO_BYTES = up16((size_t)NO * SF * sizeof(Real));
     static constexpr size_t GM_BYTES = up16((size_t)3 * SG * 8);
     static constexpr size_t GO_BYTES = up16((size_t)NO * SG * sizeof(Real));
-    static constexpr size_t OFF_E = U_BYTES_;
-    static constexpr size_t OFF_PV = OFF_E + E_BYTES_;
-    static constexpr size_t OFF_PB = OFF_PV + PV_BYTES;
-    static constexpr size_t OFF_R = OFF_PB + PB_BYTES;
-    static constexpr size_t OFF_FM = OFF_R + R_BYTES;
+    static constexpr size_t up128(size_t b) { return (b + 127) / 128 * 128; }
+    // The staged tile (Et, then Ut) and the flux planes share the start of
+    // the block, and Rs follows the flux planes over the rest of Ut: Ut is
+    // dead after the primitive phase, Et after the eta*J phase, and the flux
+    // planes are written only after the eta*J barrier.
+    static constexpr size_t OFF_E = 0;
+    static constexpr size_t OFF_U = up128(E_BYTES_);          // TMA destinations: 128-byte aligned
+    static constexpr size_t STAGED_END = OFF_U + U_BYTES_;
+    static constexpr size_t OFF_FM = 0;
     static constexpr size_t OFF_FO = OFF_FM + FM_BYTES;
     static constexpr size_t OFF_GM = OFF_FO + FO_BYTES;
     static constexpr size_t OFF_GO = OFF_GM + GM_BYTES;
-    static constexpr size_t OFF_BAR = OFF_GO + GO_BYTES;
+    static constexpr size_t OFF_R = OFF_GO + GO_BYTES;
+    static constexpr size_t R_END = OFF_R + R_BYTES;
+    static constexpr size_t OFF_PV = STAGED_END > R_END ? STAGED_END : R_END;
+    static constexpr size_t OFF_PB = OFF_PV + PV_BYTES;
+    static constexpr size_t OFF_BAR = OFF_PB + PB_BYTES;
     static constexpr size_t SMEM_BYTES = OFF_BAR + 16;
     static constexpr unsigned U_BYTES = (unsigned)U_BYTES_;
     static constexpr unsigned E_BYTES = (unsigned)E_BYTES_;
-    static constexpr int THREADS = variant_threads(SHAPE);
+    static constexpr int THREADS = variant_threads(STAGE, SHAPE);
     static constexpr int CTAS = shape_max_ctas(SHAPE);
     static_assert(THREADS / 32 * 8 <= PB_BYTES, "per-warp maxima must fit in the primitive region");
+    static_assert(OFF_R >= OFF_U, "the eta*J planes must not overlay the staged eta table");
     // CTAS CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA).
     static_assert(SMEM_BYTES <= (CTAS == 2 ? 113 : 227) * 1024, "shared memory for the CTAs per SM");
 };
 
-// velocity planes (Pv) and B / pressure planes (Pb); rho and bZ are read from
-// the staged tile
+// velocity and density planes (Pv) and B / pressure planes (Pb)
 enum { V_U = 0, V_V, V_W, V_RHO };
-enum { B_XC = 0, B_YC, B_PX, B_PY };
+enum { B_XC = 0, B_YC, B_PX, B_PY, B_Z };
 // eta*J planes in Rs
 enum { R_JX = 0, R_JY, R_JZ };
 // non-momentum flux slots (Fo / Go): rho, bZ, e, and in stage 1 the EMF
@@ -138,21 +159,50 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase)
     return false;
 }
 
-// One tile of one stage: TMA-stage the tile and its halo, then the primitive,
-// eta*J, flux, EMF and update phases.  (ti, tj) is the tile index of the
-// run, `phase` the parity of the CTA's mbarrier for this tile's load, and
-// ctl_tile marks the tile that updates the run's control block.  Returns
-// false when the bounded wait for the staged tile expired (the CTA must stop).
+// A tile's staging: its run's tensor maps, its tile index, and whether the
+// run has an eta table.
+struct TileLoad {
+    const CUtensorMap *tmap, *emap;
+    int ti, tj;
+    bool eta;
+};
+
+// Stages a tile and its halo (thread 0 only): one 3-D TMA load of all 8
+// field planes and one 2-D load of the eta table, completing the CTA's
+// mbarrier phase.
 template <int STAGE, int SHAPE>
-__device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &a,
-                                           int ti, int tj, bool ctl_tile, unsigned char *smem_raw,
-                                           uint64_t *bar, uint32_t phase)
+__device__ __forceinline__ void issue_tile_load(const TileLoad &n, unsigned char *smem_raw, uint64_t *bar)
+{
+    using T = Tile<STAGE, SHAPE>;
+    // order this CTA's earlier shared-memory accesses before the async copy
+    fence_proxy_async();
+    mbar_expect_tx(bar, T::U_BYTES + (n.eta ? T::E_BYTES : 0u));
+#if !defined(RMHD_TEST_WAIT_EXPIRY)
+    // x coordinate (j) = j0 - 3 = tj * TJ: a multiple of TJ (even), so
+    // 16-byte aligned in the global tensor as TMA requires.
+    const int x = n.tj * T::TJ, y = n.ti * T::TI;
+    tma_load_3d(smem_raw + T::OFF_U, n.tmap, bar, x, y, 0);
+    if (n.eta) tma_load_2d(smem_raw + T::OFF_E, n.emap, bar, x, y);
+#else
+    (void)smem_raw;
+#endif
+}
+
+// One tile of one stage: stage the tile and its halo (`load`), then the
+// primitive, eta*J, flux, EMF and update phases.  (ti, tj) is the tile index
+// of the run, `phase` the parity of the CTA's mbarrier for this tile's load,
+// and ctl_tile marks the tile that updates the run's control block.
+// Returns false when the bounded wait for the staged tile expired (the CTA
+// must stop).
+template <int STAGE, int SHAPE>
+__device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &load, bool ctl_tile,
+                                           unsigned char *smem_raw, uint64_t *bar, uint32_t phase)
 {
     using T = Tile<STAGE, SHAPE>;
     using Real = typename T::Real;
     constexpr int TI = T::TI, TJ = T::TJ, UJ = T::UJ, UF = T::UF, PF = T::PF, RF = T::RF, SF = T::SF, SG = T::SG;
     constexpr int PJ_ = T::PJ_, RJ_ = T::RJ_, F_NJ = T::F_NJ, G_NJ = T::G_NJ, EJ_ = T::EJ_;
-    double *Ut = reinterpret_cast<double *>(smem_raw);
+    double *Ut = reinterpret_cast<double *>(smem_raw + T::OFF_U);
     double *Et = reinterpret_cast<double *>(smem_raw + T::OFF_E);
     Real *Pv = reinterpret_cast<Real *>(smem_raw + T::OFF_PV);
     double *Pb = reinterpret_cast<double *>(smem_raw + T::OFF_PB);
@@ -165,23 +215,11 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
 
     const Grid &g = a.g;
     const int tid = threadIdx.x;
-    const int j0 = HALO + tj * TJ;
-    const int i0 = HALO + ti * TI;
+    const int j0 = HALO + load.tj * TJ;
+    const int i0 = HALO + load.ti * TI;
     const bool has_eta = a.eta != nullptr;
 
-    // ---- stage the tile + halo: one 3-D TMA load of all 8 field planes
-    // (and one 2-D load of the eta table) ----
-    if (tid == 0) {
-        // order this CTA's earlier shared-memory accesses before the async copy
-        fence_proxy_async();
-        mbar_expect_tx(bar, T::U_BYTES + (has_eta ? T::E_BYTES : 0u));
-#if !defined(RMHD_TEST_WAIT_EXPIRY)
-        // x coordinate (j) = j0 - 3 = tj * TJ: a multiple of TJ (even), so
-        // 16-byte aligned in the global tensor as TMA requires.
-        tma_load_3d(Ut, tmap, bar, j0 - HALO, i0 - HALO, 0);
-        if (has_eta) tma_load_2d(Et, emap, bar, j0 - HALO, i0 - HALO);
-#endif
-    }
+    if (tid == 0) issue_tile_load<STAGE, SHAPE>(load, smem_raw, bar);
 
     // own cell of this thread in the update phase
     const int li = tid / TJ, lj = tid - (tid / TJ) * TJ;
@@ -270,20 +308,19 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
                         - 0.5 * (bXc * bXc + bYc * bYc + bZ * bZ));
         const double py = (gm - 1.0) * (e - 0.5 * (rho * (v * v + w * w + u * u))
                         - 0.5 * (bYc * bYc + bZ * bZ + bXc * bXc));
-        // primitives are recovered in FP64; the velocities are stored in the
-        // flux-side type, centred B and pressures in FP64
+        // primitives are recovered in FP64; the velocities and the density
+        // are stored in the flux-side type, B and pressures in FP64
         Real *v0 = Pv + c;
         v0[V_U * PF] = (Real)u;
         v0[V_V * PF] = (Real)v;
         v0[V_W * PF] = (Real)w;
-#if RMHD_BULK
         v0[V_RHO * PF] = (Real)rho;
-#endif
         double *b0 = Pb + c;
         b0[B_XC * PF] = bXc;
         b0[B_YC * PF] = bYc;
         b0[B_PX * PF] = px;
         b0[B_PY * PF] = py;
+        b0[B_Z * PF] = bZ;
     }
     __syncthreads();
 
@@ -297,14 +334,14 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
         for (int c = tid; c < RF; c += T::THREADS) {
             const int ri = c / RJ_, rj = c - ri * RJ_;
             const double *p0 = Pb + (ri + 1) * PJ_ + (rj + 1);
-            const double *z0 = Ut + BZF * UF + (ri + 2) * UJ + (rj + 2);
+            const double *z0 = p0 + B_Z * PF;
 #if RMHD_FAST_MATH
-            const Real jY = -(Real)(z0[UJ] - z0[-UJ]) * i2dx;
+            const Real jY = -(Real)(z0[PJ_] - z0[-PJ_]) * i2dx;
             const Real jX = (Real)(z0[1] - z0[-1]) * i2dy;
             const Real jZ = (Real)(p0[B_YC * PF + PJ_] - p0[B_YC * PF - PJ_]) * i2dx
                           - (Real)(p0[B_XC * PF + 1] - p0[B_XC * PF - 1]) * i2dy;
 #else
-            const double nY = -(z0[UJ] - z0[-UJ]), nX = z0[1] - z0[-1];
+            const double nY = -(z0[PJ_] - z0[-PJ_]), nX = z0[1] - z0[-1];
             const double nZx = p0[B_YC * PF + PJ_] - p0[B_YC * PF - PJ_];
             const double nZy = p0[B_XC * PF + 1] - p0[B_XC * PF - 1];
             MdDiv md;
@@ -351,18 +388,16 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
             ci = a0 + T::G_I0;
             cj = a1 - 1;
         }
-        const double *uc = Ut + (ci + HALO) * UJ + (cj + HALO);
         const Real *vc = Pv + (ci + 2) * PJ_ + (cj + 2);
         const double *bc = Pb + (ci + 2) * PJ_ + (cj + 2);
         const Real *r0 = Rs + (ci + 1) * RJ_ + (cj + 1);
-        const int us = isF ? UJ : 1, ps = isF ? PJ_ : 1;
+        const int ps = isF ? PJ_ : 1;
         // sweep frame: the y sweep runs the x-sweep arithmetic on
         // (rho, v, w, u, bY, bZ, bX, e) (hlld.cu:134-152)
         const int pu = isF ? V_U : V_V, pv = isF ? V_V : V_W, pw = isF ? V_W : V_U;
         const double *pp = bc + (isF ? B_PX : B_PY) * PF;
-        const double *bt1 = isF ? bc + B_YC * PF : uc + BZF * UF;   // tangential B 1
-        const double *bt2 = isF ? uc + BZF * UF : bc + B_XC * PF;   // tangential B 2
-        const int s1 = isF ? ps : us, s2 = isF ? us : ps;
+        const double *bt1 = bc + (isF ? B_YC : B_Z) * PF;   // tangential B 1
+        const double *bt2 = bc + (isF ? B_Z : B_XC) * PF;   // tangential B 2
         const double *nb = bc + (isF ? B_XC : B_YC) * PF;
         const double bn = 0.5 * (nb[0] + nb[ps]);
         double fmv[3];   // momentum fluxes (rhoU, rhoV, rhoW in the sweep frame)
@@ -397,8 +432,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
                 st.wR = qp - 0.5f * minmod(qp - q0, qpp - qp, EPSF);
             }
             muscl_dev(pp[-ps], pp[0], pp[ps], pp[2 * ps], EPSF, st.pL, st.pR);
-            muscl_dev(bt1[-s1], bt1[0], bt1[s1], bt1[2 * s1], EPSF, st.bYL, st.bYR);
-            muscl_dev(bt2[-s2], bt2[0], bt2[s2], bt2[2 * s2], EPSF, st.bZL, st.bZR);
+            muscl_dev(bt1[-ps], bt1[0], bt1[ps], bt1[2 * ps], EPSF, st.bYL, st.bYR);
+            muscl_dev(bt2[-ps], bt2[0], bt2[ps], bt2[2 * ps], EPSF, st.bZL, st.bZR);
             st.bn = bn;
             float fo4[4];
             hlld_flux_bulk(st, gmR, inv_gm1, EPSF, fmv, fo4);
@@ -413,8 +448,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
                 r = qp - Real(0.5) * minmod(qp - q0, qpp - qp, EPSR);
             };
             {
-                const double *q = uc + RHO * UF;
-                rec((Real)q[-us], (Real)q[0], (Real)q[us], (Real)q[2 * us], qL[0], qR[0]);
+                const Real *q = vc + V_RHO * PF;
+                rec(q[-ps], q[0], q[ps], q[2 * ps], qL[0], qR[0]);
             }
             {
                 const Real *q = vc + pu * PF;
@@ -428,8 +463,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
                 const Real *q = vc + pw * PF;
                 rec(q[-ps], q[0], q[ps], q[2 * ps], qL[3], qR[3]);
             }
-            rec((Real)bt1[-s1], (Real)bt1[0], (Real)bt1[s1], (Real)bt1[2 * s1], qL[4], qR[4]);
-            rec((Real)bt2[-s2], (Real)bt2[0], (Real)bt2[s2], (Real)bt2[2 * s2], qL[5], qR[5]);
+            rec((Real)bt1[-ps], (Real)bt1[0], (Real)bt1[ps], (Real)bt1[2 * ps], qL[4], qR[4]);
+            rec((Real)bt2[-ps], (Real)bt2[0], (Real)bt2[ps], (Real)bt2[2 * ps], qL[5], qR[5]);
             rec((Real)pp[-ps], (Real)pp[0], (Real)pp[ps], (Real)pp[2 * ps], qL[6], qR[6]);
             const PrimT<Real> L{qL[0], qL[1], qL[2], qL[3], (Real)bn, qL[4], qL[5], qL[6]};
             const PrimT<Real> R{qR[0], qR[1], qR[2], qR[3], (Real)bn, qR[4], qR[5], qR[6]};
@@ -445,7 +480,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
 #endif
         // eta*J of the two cells sharing the interface and their B
         const int rs = isF ? RJ_ : 1;
-        const Real z0 = (Real)uc[BZF * UF], z1 = (Real)uc[BZF * UF + us];
+        const Real z0 = (Real)bc[B_Z * PF], z1 = (Real)bc[B_Z * PF + ps];
         const Real h = Real(0.5);
         if (isF) {
             const Real eY0 = r0[R_JY * RF], eY1 = r0[R_JY * RF + rs];
@@ -481,14 +516,20 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
         else
             flux_at(it, SweepC<false>{});
     }
-    // Stage 2 reads U^n only in the update: issue those loads now, so their
-    // latency overlaps the barrier wait of the CTA's slower warps.
-    double un_h[6];
-    if (STAGE == 2 && own) {
+    // The update reads its own cell of the stage's source state (the staged
+    // copy is the next tile's by now), and stage 2 that of U^n, from global
+    // memory: issue those loads here, so that their latency overlaps the
+    // barrier wait of the CTA's slower warps.
+    double uo[NFIELD], un_h[6];
+    if (own) {
 #pragma unroll
-        for (int n = 0; n < 6; ++n) {
-            const int f = n == 0 ? RHO : n == 1 ? MX : n == 2 ? MY : n == 3 ? MZ : n == 4 ? BZF : EN;
-            un_h[n] = a.un[f * PL + k];
+        for (int f = 0; f < NFIELD; ++f) uo[f] = a.src[f * PL + k];
+        if (STAGE == 2) {
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                const int f = n == 0 ? RHO : n == 1 ? MX : n == 2 ? MY : n == 3 ? MZ : n == 4 ? BZF : EN;
+                un_h[n] = a.un[f * PL + k];
+            }
         }
     }
     __syncthreads();
@@ -513,7 +554,6 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
     // ---- update of the tile's own cells ----
     const int fo_ = (li + 1) * F_NJ + (lj - T::F_J0);             // F(i); F(i-1) is F_NJ before
     const int go_ = (li - T::G_I0) * G_NJ + (lj + 1);             // G(j); G(j-1) is 1 before
-    const double *uo = Ut + (li + HALO) * UJ + (lj + HALO);        // own cell in the staged tile
     const int fld[6] = {RHO, MX, MY, MZ, BZF, EN};
     // flux difference of hydro field n (0..5), in FP64
     auto dF = [&](int n) -> double {
@@ -532,16 +572,16 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
             // oneStepFirstFunctor (resistiveMHD_2D.cu:53-86)
 #pragma unroll
             for (int n = 0; n < 6; ++n)
-                a.dst[fld[n] * PL + k] = uo[fld[n] * UF] - dtdx * dF(n) - dtdy * dG(n);
+                a.dst[fld[n] * PL + k] = uo[fld[n]] - dtdx * dF(n) - dtdy * dG(n);
             // CT_kernel (ct.cu:44-59) with the EMF of this stage
             const double *ez = Ez + (li + 1) * EJ_ + (lj + 1);
-            a.dst[BXF * PL + k] = uo[BXF * UF] - dtdy * (ez[0] - ez[-1]);
-            a.dst[BYF * PL + k] = uo[BYF * UF] + dtdx * (ez[0] - ez[-EJ_]);
+            a.dst[BXF * PL + k] = uo[BXF] - dtdy * (ez[0] - ez[-1]);
+            a.dst[BYF * PL + k] = uo[BYF] + dtdx * (ez[0] - ez[-EJ_]);
             // Symmetric boundaries read the CT'd face bY at j = 2 (the lower
             // wall face) before replacing it (TS boundary.cu:57-88).
             if (a.row2 && j0 == HALO && lj == 0) {
                 const double *e2 = Ez + (li + 1) * EJ_;
-                a.row2[i] = uo[BYF * UF - 1] + dtdx * (e2[0] - e2[-EJ_]);
+                a.row2[i] = a.src[BYF * PL + k - 1] + dtdx * (e2[0] - e2[-EJ_]);
             }
         }
     } else {
@@ -552,11 +592,11 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap *tmap, const CUtens
 #pragma unroll
             for (int n = 0; n < 6; ++n) {
                 const double u = un_h[n];
-                const double ub = uo[fld[n] * UF];
+                const double ub = uo[fld[n]];
                 nv[fld[n]] = 0.5 * (u + ub - dtdx * dF(n) - dtdy * dG(n));
             }
-            nv[BXF] = uo[BXF * UF];
-            nv[BYF] = uo[BYF * UF];
+            nv[BXF] = uo[BXF];
+            nv[BYF] = uo[BYF];
 #pragma unroll
             for (int n = 0; n < 8; ++n) a.dst[n * PL + k] = nv[n];
         }
@@ -604,7 +644,7 @@ __device__ __forceinline__ void init_tile_barrier(uint64_t *bar)
 
 // One CTA per tile of one run.
 template <int STAGE, int SHAPE>
-__global__ void __launch_bounds__(variant_threads(SHAPE), shape_max_ctas(SHAPE))
+__global__ void __launch_bounds__(variant_threads(STAGE, SHAPE), shape_max_ctas(SHAPE))
 stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap emap,
              const StageArgs a)
 {
@@ -612,14 +652,30 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
     using T = Tile<STAGE, SHAPE>;
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::OFF_BAR);
     init_tile_barrier(bar);
-    stage_tile<STAGE, SHAPE>(&tmap, &emap, a, blockIdx.y, blockIdx.x, blockIdx.x == 0 && blockIdx.y == 0, smem_raw,
-                             bar, 0);
+    const TileLoad load{&tmap, &emap, (int)blockIdx.y, (int)blockIdx.x, a.eta != nullptr};
+    stage_tile<STAGE, SHAPE>(a, load, blockIdx.x == 0 && blockIdx.y == 0, smem_raw, bar, 0);
+}
+
+// The stage arguments of one run of a batch.
+template <int STAGE>
+__device__ __forceinline__ StageArgs batch_args(const BatchRun &r, int parity)
+{
+    StageArgs a;
+    a.g = r.g;
+    a.src = STAGE == 1 ? r.A : r.B;
+    a.un = r.A;
+    a.dst = STAGE == 1 ? r.B : r.A;
+    a.eta = r.eta;
+    a.row2 = r.g.bc_x == BC_SYMMETRIC ? r.row2 : nullptr;
+    a.ctl = r.ctl;
+    a.parity = parity;
+    return a;
 }
 
 // Persistent CTAs over the tile table of a batch of independent runs (each
 // with its own grid, eta, state buffers, tensor maps and control block).
 template <int STAGE, int SHAPE>
-__global__ void __launch_bounds__(variant_threads(SHAPE), shape_max_ctas(SHAPE))
+__global__ void __launch_bounds__(variant_threads(STAGE, SHAPE), shape_max_ctas(SHAPE))
 stage_batch_kernel(const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles, int ntiles, int parity)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -630,21 +686,16 @@ stage_batch_kernel(const BatchRun *runs, const CUtensorMap *maps, const TileRef 
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const TileRef tr = tiles[t];
         const BatchRun &r = runs[tr.run];
-        StageArgs a;
-        a.g = r.g;
-        a.src = STAGE == 1 ? r.A : r.B;
-        a.un = r.A;
-        a.dst = STAGE == 1 ? r.B : r.A;
-        a.eta = r.eta;
-        a.row2 = r.g.bc_x == BC_SYMMETRIC ? r.row2 : nullptr;
-        a.ctl = r.ctl;
-        a.parity = parity;
         const CUtensorMap *m = maps + (size_t)tr.run * MAPS_PER_RUN;
-        if (!stage_tile<STAGE, SHAPE>(m + (STAGE - 1), m + 2 + (STAGE - 1), a, tr.ti, tr.tj,
-                                      tr.ti == 0 && tr.tj == 0, smem_raw, bar, phase))
+        const TileLoad load{m + (STAGE - 1), m + 2 + (STAGE - 1), tr.ti, tr.tj, r.eta != nullptr};
+        if (!stage_tile<STAGE, SHAPE>(batch_args<STAGE>(r, parity), load, tr.ti == 0 && tr.tj == 0, smem_raw, bar,
+                                      phase))
             return;
         phase ^= 1;
-        __syncthreads();   // every thread is done with this tile's shared memory
+        // every thread is done with this tile's shared memory, whose flux
+        // planes the next tile's staging overwrites through the async proxy
+        fence_proxy_async();
+        __syncthreads();
     }
 }
 
@@ -667,11 +718,22 @@ int stage_regs(int stage, int shape)
     return attr.numRegs;
 }
 
+// Opts a stage kernel into its dynamic shared memory and asks for the
+// smallest shared-memory carve-out that holds `ctas` of its CTAs per SM,
+// leaving the rest of the SM's unified L1 to the cache.
+template <class K> static void set_smem_attributes(K kernel, size_t smem, int ctas)
+{
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t need = (size_t)ctas * (smem + 1024), most = 228 * 1024;
+    const int pct = (int)((need * 100 + most - 1) / most);
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct > 100 ? 100 : pct);
+}
+
 template <int STAGE, int SHAPE>
 static void launch_one(const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args, cudaStream_t stream)
 {
     using T = Tile<STAGE, SHAPE>;
-    cudaFuncSetAttribute(stage_kernel<STAGE, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_BYTES);
+    set_smem_attributes(stage_kernel<STAGE, SHAPE>, T::SMEM_BYTES, T::CTAS);
     const dim3 grid((args.g.ny - 2 * HALO + T::TJ - 1) / T::TJ, (args.g.nx - 2 * HALO + T::TI - 1) / T::TI);
     stage_kernel<STAGE, SHAPE><<<grid, T::THREADS, T::SMEM_BYTES, stream>>>(*tmap, *emap, args);
 }
@@ -696,8 +758,7 @@ static void launch_batch_one(const BatchRun *runs, const CUtensorMap *maps, cons
                              int ctas, int parity, cudaStream_t stream)
 {
     using T = Tile<STAGE, SHAPE>;
-    cudaFuncSetAttribute(stage_batch_kernel<STAGE, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)T::SMEM_BYTES);
+    set_smem_attributes(stage_batch_kernel<STAGE, SHAPE>, T::SMEM_BYTES, T::CTAS);
     stage_batch_kernel<STAGE, SHAPE><<<ctas, T::THREADS, T::SMEM_BYTES, stream>>>(runs, maps, tiles, ntiles, parity);
 }
 

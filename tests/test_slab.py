@@ -208,6 +208,34 @@ def test_slab_group_equals_whole_domain_on_gpu(gpu, bcx, bcy, table, shape, part
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("bcx,bcy", [("symmetric", None), ("periodic", "symmetric")])
+def test_slab_group_full_size_harris_on_gpu(gpu, bcx, bcy):
+    """The headline workload, the Harris sheet on 2048x1024 cells with its eta
+    table (its symmetric walls, and periodic in x), in 4 slabs of 512
+    columns: 10 steps bit for bit those of one solver on the whole domain."""
+    from resistivemhd_gpu_b200 import Solver, setups
+    from resistivemhd_gpu_b200.slab import SlabGroup
+
+    s = dataclasses.replace(setups.harris_sheet(2048, 1024), bc=bcx, bc_y=bcy)
+    steps = 10
+    with Solver.from_setup(s, precision="fp64_exact") as whole:
+        dts = []
+        for _ in range(steps):
+            whole.step()
+            dts.append(whole.dt)
+        want = whole.get_state()
+    with SlabGroup(s, 4) as g:
+        assert [sl.n for sl in g.slabs] == [512] * 4
+        got_dts = []
+        for _ in range(steps):
+            g.step()
+            got_dts.append(g.dt)
+        assert _bits(np.array(got_dts)).tolist() == _bits(np.array(dts)).tolist()
+        assert np.array_equal(_bits(g.get_state()), _bits(want))
+        assert not g.check_crashed()
+
+
+@pytest.mark.gpu
 def test_slab_domain_one_nccl_rank_on_gpu(gpu, oracle):
     """SlabDomain over an NCCL process group of one rank (periodic x: the
     slab's halos are its own far edges; the words' all-reduce runs)."""
