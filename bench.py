@@ -251,10 +251,15 @@ def ours_arm(args, rank: int, world: int, local_rank: int) -> None:
 
     sol = Solver.from_setup(setup, precision=args.precision, device=local_rank)
     # the stage kernels' tile shape, picked by the library's autotuner on this
-    # workload (the state is restored afterwards; results do not depend on it)
-    sol.autotune(6)
+    # workload (the state is restored afterwards; results do not depend on
+    # it), unless given (a profiler run that must launch what the timed run did)
+    if args.tile_shapes:
+        sol.set_stage_shapes(*args.tile_shapes)
+        tuning = {}
+    else:
+        sol.autotune(6)
+        tuning = sol.tuning()
     shape = list(sol.stage_shapes)
-    tuning = sol.tuning()
     sol.run(args.warmup)
     sol.dt  # synchronise
 
@@ -1058,6 +1063,8 @@ def main() -> None:
     ap.add_argument("--no-contact", dest="contact_block", action="store_false")
     ap.add_argument("--no-ensemble", dest="ensemble_block", action="store_false")
     ap.add_argument("--quick", action="store_true", help="headline only (no extra blocks, baselines or e2e)")
+    ap.add_argument("--tile-shapes", type=int, nargs=2, metavar=("STAGE1", "STAGE2"), default=None,
+                    help="the stage kernels' tile shapes instead of the autotuner's pick")
     ap.add_argument("--study", choices=sorted(STUDIES), default=None,
                     help="instead of the benchmark: the long FP32-bulk / FP64 error study of one workload")
     ap.add_argument("--study-steps", type=int, default=0, help="override the study's step count")

@@ -18,6 +18,15 @@
 #define RMHD_REAL double
 #endif
 
+// Whether the flux planes overlay the staged tile (and the update reads its
+// own cell from global memory).  The FP64 variants spill registers in the
+// flux phase and gain from the L1 the smaller block leaves; FP32-bulk does
+// not spill, and its persistent batch kernel measured 4 % faster reading
+// the own cell from the staged tile.
+#ifndef RMHD_OVERLAY
+#define RMHD_OVERLAY (!RMHD_BULK)
+#endif
+
 #ifndef RMHD_VARIANT
 #error "define RMHD_VARIANT (exact or fast) before including stage_impl.cuh"
 #endif
@@ -49,13 +58,13 @@ constexpr int variant_threads(int stage, int shape)
 // Gm, Go                 the same for the y fluxes at j+1/2 (Go slot 3: the bX flux)
 // Stage 1 needs x fluxes on rows j0-1..j0+TJ and y fluxes on columns
 // i0-1..i0+TI for its corner EMF; stage 2 only the tile's own interfaces.
-// Ut is read only by the primitive phase and Et by the eta*J phase, which
-// copy into Pv / Pb what the later phases need (rho, bZ); the update reads
-// its own cell from global memory.  So Rs can overlay Ut, and the flux
-// planes both: about 73 KB per CTA instead of 104-113 KB in shape 0, so
-// that two CTAs take 164 KB of the SM's unified L1 / shared memory and
-// leave 92 KB (instead of 28) to the cache, where the flux phase's register
-// spills go.
+// Ut is read only by the primitive phase (and, without RMHD_OVERLAY, the
+// update) and Et by the eta*J phase, which copy into Pv / Pb what the later
+// phases need (rho, bZ).  With RMHD_OVERLAY the update reads its own cell
+// from global memory, Rs overlays Ut and the flux planes overlay both:
+// about 73 KB per CTA instead of 104-113 KB in shape 0, so that two CTAs
+// take 164 KB of the SM's unified L1 / shared memory and leave 92 KB
+// (instead of 28) to the cache, where the flux phase's register spills go.
 template <int STAGE, int SHAPE> struct Tile {
     using Real = RMHD_REAL;                                  // flux-side arithmetic type
     static constexpr int TI = stage_ti(STAGE, SHAPE);
@@ -91,14 +100,15 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr size_t GM_BYTES = up16((size_t)3 * SG * 8);
     static constexpr size_t GO_BYTES = up16((size_t)NO * SG * sizeof(Real));
     static constexpr size_t up128(size_t b) { return (b + 127) / 128 * 128; }
-    // The staged tile (Et, then Ut) and the flux planes share the start of
-    // the block, and Rs follows the flux planes over the rest of Ut: Ut is
-    // dead after the primitive phase, Et after the eta*J phase, and the flux
-    // planes are written only after the eta*J barrier.
+    // With RMHD_OVERLAY the staged tile (Et, then Ut) and the flux planes
+    // share the start of the block, and Rs follows the flux planes over the
+    // rest of Ut: Ut is dead after the primitive phase, Et after the eta*J
+    // phase, and the flux planes are written only after the eta*J barrier.
+    // Without it they follow the staged tile.
     static constexpr size_t OFF_E = 0;
     static constexpr size_t OFF_U = up128(E_BYTES_);          // TMA destinations: 128-byte aligned
     static constexpr size_t STAGED_END = OFF_U + U_BYTES_;
-    static constexpr size_t OFF_FM = 0;
+    static constexpr size_t OFF_FM = RMHD_OVERLAY ? 0 : STAGED_END;
     static constexpr size_t OFF_FO = OFF_FM + FM_BYTES;
     static constexpr size_t OFF_GM = OFF_FO + FO_BYTES;
     static constexpr size_t OFF_GO = OFF_GM + GM_BYTES;
@@ -516,14 +526,15 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
         else
             flux_at(it, SweepC<false>{});
     }
-    // The update reads its own cell of the stage's source state (the staged
-    // copy is the next tile's by now), and stage 2 that of U^n, from global
-    // memory: issue those loads here, so that their latency overlaps the
+    // The update's own cell of the stage's source state (from global memory
+    // when the flux planes overlay the staged tile), and in stage 2 that of
+    // U^n: issue those loads here, so that their latency overlaps the
     // barrier wait of the CTA's slower warps.
     double uo[NFIELD], un_h[6];
     if (own) {
 #pragma unroll
-        for (int f = 0; f < NFIELD; ++f) uo[f] = a.src[f * PL + k];
+        for (int f = 0; f < NFIELD; ++f)
+            uo[f] = RMHD_OVERLAY ? a.src[f * PL + k] : Ut[f * UF + (li + HALO) * UJ + (lj + HALO)];
         if (STAGE == 2) {
 #pragma unroll
             for (int n = 0; n < 6; ++n) {
@@ -581,7 +592,9 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
             // wall face) before replacing it (TS boundary.cu:57-88).
             if (a.row2 && j0 == HALO && lj == 0) {
                 const double *e2 = Ez + (li + 1) * EJ_;
-                a.row2[i] = a.src[BYF * PL + k - 1] + dtdx * (e2[0] - e2[-EJ_]);
+                const double b2 = RMHD_OVERLAY ? a.src[BYF * PL + k - 1]
+                                               : Ut[BYF * UF + (li + HALO) * UJ + (lj + HALO) - 1];
+                a.row2[i] = b2 + dtdx * (e2[0] - e2[-EJ_]);
             }
         }
     } else {
