@@ -21,8 +21,9 @@
 // Whether the flux planes overlay the staged tile (and the update reads its
 // own cell from global memory).  The FP64 variants spill registers in the
 // flux phase and gain from the L1 the smaller block leaves; FP32-bulk does
-// not spill, and its persistent batch kernel measured 4 % faster reading
-// the own cell from the staged tile.
+// not spill, and its persistent batch kernel measured 1.3 % faster reading
+// the own cell from the staged tile.  Shapes of 3 CTAs per SM overlay in
+// every variant, to fit.
 #ifndef RMHD_OVERLAY
 #define RMHD_OVERLAY (!RMHD_BULK)
 #endif
@@ -43,7 +44,7 @@ namespace RMHD_VARIANT {
 // 2-8 % slower.
 constexpr int variant_threads(int stage, int shape)
 {
-    return shape == 2 ? shape_threads(2)
+    return shape >= 2 ? shape_threads(shape)
                       : ((RMHD_BULK || (RMHD_FAST_MATH && stage == 1)) ? 384 : shape_threads(shape));
 }
 
@@ -108,7 +109,8 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr size_t OFF_E = 0;
     static constexpr size_t OFF_U = up128(E_BYTES_);          // TMA destinations: 128-byte aligned
     static constexpr size_t STAGED_END = OFF_U + U_BYTES_;
-    static constexpr size_t OFF_FM = RMHD_OVERLAY ? 0 : STAGED_END;
+    static constexpr bool OVERLAY = RMHD_OVERLAY || shape_max_ctas(SHAPE) >= 3;
+    static constexpr size_t OFF_FM = OVERLAY ? 0 : STAGED_END;
     static constexpr size_t OFF_FO = OFF_FM + FM_BYTES;
     static constexpr size_t OFF_GM = OFF_FO + FO_BYTES;
     static constexpr size_t OFF_GO = OFF_GM + GM_BYTES;
@@ -125,7 +127,7 @@ template <int STAGE, int SHAPE> struct Tile {
     static_assert(THREADS / 32 * 8 <= PB_BYTES, "per-warp maxima must fit in the primitive region");
     static_assert(OFF_R >= OFF_U, "the eta*J planes must not overlay the staged eta table");
     // CTAS CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA).
-    static_assert(SMEM_BYTES <= (CTAS == 2 ? 113 : 227) * 1024, "shared memory for the CTAs per SM");
+    static_assert(SMEM_BYTES <= (228 / CTAS - 1) * 1024, "shared memory for the CTAs per SM");
 };
 
 // velocity and density planes (Pv) and B / pressure planes (Pb)
@@ -534,7 +536,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
     if (own) {
 #pragma unroll
         for (int f = 0; f < NFIELD; ++f)
-            uo[f] = RMHD_OVERLAY ? a.src[f * PL + k] : Ut[f * UF + (li + HALO) * UJ + (lj + HALO)];
+            uo[f] = T::OVERLAY ? a.src[f * PL + k] : Ut[f * UF + (li + HALO) * UJ + (lj + HALO)];
         if (STAGE == 2) {
 #pragma unroll
             for (int n = 0; n < 6; ++n) {
@@ -592,7 +594,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
             // wall face) before replacing it (TS boundary.cu:57-88).
             if (a.row2 && j0 == HALO && lj == 0) {
                 const double *e2 = Ez + (li + 1) * EJ_;
-                const double b2 = RMHD_OVERLAY ? a.src[BYF * PL + k - 1]
+                const double b2 = T::OVERLAY ? a.src[BYF * PL + k - 1]
                                                : Ut[BYF * UF + (li + HALO) * UJ + (lj + HALO) - 1];
                 a.row2[i] = b2 + dtdx * (e2[0] - e2[-EJ_]);
             }
@@ -714,20 +716,49 @@ stage_batch_kernel(const BatchRun *runs, const CUtensorMap *maps, const TileRef 
 
 template <int STAGE, int SHAPE> constexpr size_t smem_of() { return Tile<STAGE, SHAPE>::SMEM_BYTES; }
 
+// Calls f.template operator()<STAGE, SHAPE>() for the run-time stage and shape.
+template <class F> static void with_stage_shape(int stage, int shape, const F &f)
+{
+#define RMHD_SHAPE_CASE(SH)                                                                            \
+    case SH:                                                                                           \
+        if (stage == 1) f.template operator()<1, SH>();                                                \
+        else f.template operator()<2, SH>();                                                           \
+        break;
+    switch (shape) {
+    RMHD_SHAPE_CASE(0)
+    RMHD_SHAPE_CASE(1)
+    RMHD_SHAPE_CASE(2)
+    RMHD_SHAPE_CASE(3)
+    default: RMHD_SHAPE_CASE(4)
+    }
+#undef RMHD_SHAPE_CASE
+}
+static_assert(NSHAPE == 5, "one case per tile shape in with_stage_shape");
+
+struct SmemOf {
+    size_t &n;
+    template <int ST, int SH> void operator()() const { n = smem_of<ST, SH>(); }
+};
+
 size_t stage_smem_bytes(int stage, int shape)
 {
-    if (shape == 0) return stage == 1 ? smem_of<1, 0>() : smem_of<2, 0>();
-    if (shape == 1) return stage == 1 ? smem_of<1, 1>() : smem_of<2, 1>();
-    return stage == 1 ? smem_of<1, 2>() : smem_of<2, 2>();
+    size_t n = 0;
+    with_stage_shape(stage, shape, SmemOf{n});
+    return n;
 }
+
+struct RegsOf {
+    cudaFuncAttributes &attr;
+    template <int ST, int SH> void operator()() const
+    {
+        cudaFuncGetAttributes(&attr, (const void *)stage_kernel<ST, SH>);
+    }
+};
 
 int stage_regs(int stage, int shape)
 {
     cudaFuncAttributes attr{};
-    const void *f = shape == 0 ? (stage == 1 ? (const void *)stage_kernel<1, 0> : (const void *)stage_kernel<2, 0>)
-                  : shape == 1 ? (stage == 1 ? (const void *)stage_kernel<1, 1> : (const void *)stage_kernel<2, 1>)
-                               : (stage == 1 ? (const void *)stage_kernel<1, 2> : (const void *)stage_kernel<2, 2>);
-    cudaFuncGetAttributes(&attr, f);
+    with_stage_shape(stage, shape, RegsOf{attr});
     return attr.numRegs;
 }
 
@@ -742,52 +773,43 @@ template <class K> static void set_smem_attributes(K kernel, size_t smem, int ct
     cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct > 100 ? 100 : pct);
 }
 
-template <int STAGE, int SHAPE>
-static void launch_one(const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args, cudaStream_t stream)
-{
-    using T = Tile<STAGE, SHAPE>;
-    set_smem_attributes(stage_kernel<STAGE, SHAPE>, T::SMEM_BYTES, T::CTAS);
-    const dim3 grid((args.g.ny - 2 * HALO + T::TJ - 1) / T::TJ, (args.g.nx - 2 * HALO + T::TI - 1) / T::TI);
-    stage_kernel<STAGE, SHAPE><<<grid, T::THREADS, T::SMEM_BYTES, stream>>>(*tmap, *emap, args);
-}
+struct LaunchOne {
+    const CUtensorMap *tmap, *emap;
+    const StageArgs &args;
+    cudaStream_t stream;
+    template <int ST, int SH> void operator()() const
+    {
+        using T = Tile<ST, SH>;
+        set_smem_attributes(stage_kernel<ST, SH>, T::SMEM_BYTES, T::CTAS);
+        const dim3 grid((args.g.ny - 2 * HALO + T::TJ - 1) / T::TJ, (args.g.nx - 2 * HALO + T::TI - 1) / T::TI);
+        stage_kernel<ST, SH><<<grid, T::THREADS, T::SMEM_BYTES, stream>>>(*tmap, *emap, args);
+    }
+};
 
 void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,
                   cudaStream_t stream)
 {
-    if (shape == 0) {
-        if (stage == 1) launch_one<1, 0>(tmap, emap, args, stream);
-        else launch_one<2, 0>(tmap, emap, args, stream);
-    } else if (shape == 1) {
-        if (stage == 1) launch_one<1, 1>(tmap, emap, args, stream);
-        else launch_one<2, 1>(tmap, emap, args, stream);
-    } else {
-        if (stage == 1) launch_one<1, 2>(tmap, emap, args, stream);
-        else launch_one<2, 2>(tmap, emap, args, stream);
-    }
+    with_stage_shape(stage, shape, LaunchOne{tmap, emap, args, stream});
 }
 
-template <int STAGE, int SHAPE>
-static void launch_batch_one(const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles, int ntiles,
-                             int ctas, int parity, cudaStream_t stream)
-{
-    using T = Tile<STAGE, SHAPE>;
-    set_smem_attributes(stage_batch_kernel<STAGE, SHAPE>, T::SMEM_BYTES, T::CTAS);
-    stage_batch_kernel<STAGE, SHAPE><<<ctas, T::THREADS, T::SMEM_BYTES, stream>>>(runs, maps, tiles, ntiles, parity);
-}
+struct LaunchBatch {
+    const BatchRun *runs;
+    const CUtensorMap *maps;
+    const TileRef *tiles;
+    int ntiles, ctas, parity;
+    cudaStream_t stream;
+    template <int ST, int SH> void operator()() const
+    {
+        using T = Tile<ST, SH>;
+        set_smem_attributes(stage_batch_kernel<ST, SH>, T::SMEM_BYTES, T::CTAS);
+        stage_batch_kernel<ST, SH><<<ctas, T::THREADS, T::SMEM_BYTES, stream>>>(runs, maps, tiles, ntiles, parity);
+    }
+};
 
 void launch_stage_batch(int stage, int shape, const BatchRun *runs, const CUtensorMap *maps, const TileRef *tiles,
                         int ntiles, int ctas, int parity, cudaStream_t stream)
 {
-    if (shape == 0) {
-        if (stage == 1) launch_batch_one<1, 0>(runs, maps, tiles, ntiles, ctas, parity, stream);
-        else launch_batch_one<2, 0>(runs, maps, tiles, ntiles, ctas, parity, stream);
-    } else if (shape == 1) {
-        if (stage == 1) launch_batch_one<1, 1>(runs, maps, tiles, ntiles, ctas, parity, stream);
-        else launch_batch_one<2, 1>(runs, maps, tiles, ntiles, ctas, parity, stream);
-    } else {
-        if (stage == 1) launch_batch_one<1, 2>(runs, maps, tiles, ntiles, ctas, parity, stream);
-        else launch_batch_one<2, 2>(runs, maps, tiles, ntiles, ctas, parity, stream);
-    }
+    with_stage_shape(stage, shape, LaunchBatch{runs, maps, tiles, ntiles, ctas, parity, stream});
 }
 
 }  // namespace RMHD_VARIANT
