@@ -82,42 +82,90 @@ __device__ __forceinline__ void sweep_cell(const Grid &g, const double *U, int i
 // current values in), NaN elsewhere.  One CTA stages the primitives of
 // (CT_TI + 3) x (CT_TJ + 3) cells in shared memory once -- the x and y
 // sweeps' pressures sum their squares in different orders, so both are
-// kept -- and forms the x and y interfaces (i, j) of its CT_TI x CT_TJ
-// cells from there, in the reference's order of operations.
+// kept -- then the hook's eta*J of the (CT_TI + 1) x (CT_TJ + 1) cells its
+// interfaces read, once per cell, and forms the x and y interfaces (i, j)
+// of its CT_TI x CT_TJ cells from there, in the reference's order of
+// operations.  Divisions go through shared correctly rounded reciprocals
+// (MdDiv, with IEEE division where its guard fails), which give the
+// reference's quotients bit for bit.
 constexpr int CT_TI = 16, CT_TJ = 32, CT_THREADS = 256;
 constexpr int CT_SI = CT_TI + 3, CT_SJ = CT_TJ + 3, CT_SC = CT_SI * CT_SJ;
+constexpr int CT_JI = CT_TI + 1, CT_JJ = CT_TJ + 1, CT_JC = CT_JI * CT_JJ;
 enum { S_RHO = 0, S_U, S_V, S_W, S_BXC, S_BYC, S_BZ, S_PX, S_PY, S_NF };
+enum { J_X = 0, J_Y, J_Z, J_NF };   // eta*Jx, eta*Jy, eta*Jz
+constexpr size_t CT_SMEM = (size_t)(S_NF * CT_SC + J_NF * CT_JC) * sizeof(double);
 
 __global__ void __launch_bounds__(CT_THREADS, 2) contact_flux_tiled_kernel(Grid g, const double *U, const double *eta,
                                                                          double *F, double *G)
 {
-    __shared__ double S[S_NF][CT_SC];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    double (*S)[CT_SC] = reinterpret_cast<double (*)[CT_SC]>(smem_raw);
+    double (*J)[CT_JC] = reinterpret_cast<double (*)[CT_JC]>(smem_raw + S_NF * CT_SC * sizeof(double));
     const int i0 = blockIdx.y * CT_TI, j0 = blockIdx.x * CT_TJ;
     const long long P = g.plane;
+    const double gm1 = g.gamma - 1.0;
     // staged cell (si, sj) is cell (i0 - 1 + si, j0 - 1 + sj)
     for (int c = threadIdx.x; c < CT_SC; c += CT_THREADS) {
         const int si = c / CT_SJ, sj = c - si * CT_SJ;
         const int i = i0 - 1 + si, j = j0 - 1 + sj;
         if (i < 0 || j < 0 || i >= g.nx || j >= g.ny) continue;   // read by no defined interface
-        double cx[8], cy[8], qx[8], qy[8];
-        sweep_cell<0>(g, U, i, j, cx);
-        sweep_cell<1>(g, U, i, j, cy);
-        adj::basic_param(cx, 0.0, g.gamma, qx);
-        adj::basic_param(cy, 0.0, g.gamma, qy);
-        S[S_RHO][c] = qx[adj::QR];
-        S[S_U][c] = qx[adj::QU];
-        S[S_V][c] = qx[adj::QV];
-        S[S_W][c] = qx[adj::QW];
-        S[S_BXC][c] = cx[4];
-        S[S_BYC][c] = cx[5];
-        S[S_BZ][c] = cx[6];
-        S[S_PX][c] = qx[adj::QP];
-        S[S_PY][c] = qy[adj::QP];
+        const long long k = at(g, i, j);
+        const double rho = U[RHO * P + k], mx = U[MX * P + k], my = U[MY * P + k], mz = U[MZ * P + k];
+        // calculate_half_Q.cu:4-38 in both sweeps' orders
+        MdDiv md;
+        const double yr = md.recip(rho);
+        double u = md.div(mx, rho, yr), v = md.div(my, rho, yr), w = md.div(mz, rho, yr);
+        if (!md.ok) {
+            u = mx / rho;
+            v = my / rho;
+            w = mz / rho;
+        }
+        const double bxc = bx_c(g, U, i, j), byc = by_c(g, U, i, j), bz = U[BZF * P + k], e = U[EN * P + k];
+        S[S_RHO][c] = rho;
+        S[S_U][c] = u;
+        S[S_V][c] = v;
+        S[S_W][c] = w;
+        S[S_BXC][c] = bxc;
+        S[S_BYC][c] = byc;
+        S[S_BZ][c] = bz;
+        S[S_PX][c] = gm1 * ((e - 0.5 * (rho * (u * u + v * v + w * w))) - 0.5 * (bxc * bxc + byc * byc + bz * bz));
+        S[S_PY][c] = gm1 * ((e - 0.5 * (rho * (v * v + w * w + u * u))) - 0.5 * (byc * byc + bz * bz + bxc * bxc));
     }
     __syncthreads();
 
     auto at_s = [](int si, int sj) { return si * CT_SJ + sj; };
+    auto bz = [&](int a, int b) { return S[S_BZ][at_s(a, b)]; };
+    auto byc = [&](int a, int b) { return S[S_BYC][at_s(a, b)]; };
+    auto bxc = [&](int a, int b) { return S[S_BXC][at_s(a, b)]; };
     const double two_dx = 2.0 * g.dx, two_dy = 2.0 * g.dy;
+    MdDiv cd;
+    const double y2dx = cd.recip(two_dx), y2dy = cd.recip(two_dy);
+    // eta*J of cell (i0 + ci, j0 + cj), staged at (ci + 1, cj + 1), where
+    // all its neighbours exist (the hook reads it only there)
+    for (int c = threadIdx.x; c < CT_JC; c += CT_THREADS) {
+        const int ci = c / CT_JJ, cj = c - ci * CT_JJ;
+        const int i = i0 + ci, j = j0 + cj;
+        if (i < 1 || j < 1 || i > g.nx - 2 || j > g.ny - 2) continue;
+        const int si = ci + 1, sj = cj + 1;
+        const double nX = bz(si, sj + 1) - bz(si, sj - 1);
+        const double nY = -(bz(si + 1, sj) - bz(si - 1, sj));
+        const double nZx = byc(si + 1, sj) - byc(si - 1, sj), nZy = bxc(si, sj + 1) - bxc(si, sj - 1);
+        MdDiv md;
+        md.ok = cd.ok;
+        double jX = md.div(nX, two_dy, y2dy), jY = md.div(nY, two_dx, y2dx);
+        double jZ = md.div(nZx, two_dx, y2dx) - md.div(nZy, two_dy, y2dy);
+        if (!md.ok) {
+            jX = nX / two_dy;
+            jY = nY / two_dx;
+            jZ = nZx / two_dx - nZy / two_dy;
+        }
+        const double e = eta ? eta[at(g, i, j)] : g.eta;
+        J[J_X][c] = e * jX;
+        J[J_Y][c] = e * jY;
+        J[J_Z][c] = e * jZ;
+    }
+    __syncthreads();
+
     for (int t = threadIdx.x; t < 2 * CT_TI * CT_TJ; t += CT_THREADS) {
         const int dir = t >= CT_TI * CT_TJ;
         const int r = t - dir * CT_TI * CT_TJ;
@@ -165,37 +213,21 @@ __global__ void __launch_bounds__(CT_THREADS, 2) contact_flux_tiled_kernel(Grid 
             }
             // the resistive hook (the reference's 0 < i < nx-2, 0 < j < ny-2)
             if (i >= 1 && i <= g.nx - 3 && j >= 1 && j <= g.ny - 3) {
-                auto bz = [&](int a, int b) { return S[S_BZ][at_s(a, b)]; };
-                auto byc = [&](int a, int b) { return S[S_BYC][at_s(a, b)]; };
-                auto bxc = [&](int a, int b) { return S[S_BXC][at_s(a, b)]; };
+                const int c0 = li * CT_JJ + lj;                         // eta*J of cell (i, j)
                 if (dir == 0) {
-                    double jY, jZ, e;
-                    jY = -(bz(si + 1, sj) - bz(si - 1, sj)) / two_dx;
-                    jZ = (byc(si + 1, sj) - byc(si - 1, sj)) / two_dx - (bxc(si, sj + 1) - bxc(si, sj - 1)) / two_dy;
-                    e = eta ? eta[at(g, i, j)] : g.eta;
-                    const double etaJY = e * jY, etaJZ = e * jZ;
+                    const int c1 = c0 + CT_JJ;                          // (i + 1, j)
+                    const double etaJY = J[J_Y][c0], etaJZ = J[J_Z][c0];
                     const double etaJYBZ = etaJY * bz(si, sj), etaJZBY = etaJZ * byc(si, sj);
-                    jY = -(bz(si + 2, sj) - bz(si, sj)) / two_dx;
-                    jZ = (byc(si + 2, sj) - byc(si, sj)) / two_dx
-                       - (bxc(si + 1, sj + 1) - bxc(si + 1, sj - 1)) / two_dy;
-                    e = eta ? eta[at(g, i + 1, j)] : g.eta;
-                    const double etaJYPlus1 = e * jY, etaJZPlus1 = e * jZ;
+                    const double etaJYPlus1 = J[J_Y][c1], etaJZPlus1 = J[J_Z][c1];
                     const double etaJYBZPlus1 = etaJYPlus1 * bz(si + 1, sj), etaJZBYPlus1 = etaJZPlus1 * byc(si + 1, sj);
                     out[5] -= 0.5 * (etaJZ + etaJZPlus1);
                     out[6] += 0.5 * (etaJY + etaJYPlus1);
                     out[7] += 0.5 * (etaJYBZ + etaJYBZPlus1) - 0.5 * (etaJZBY + etaJZBYPlus1);
                 } else {
-                    double jX, jZ, e;
-                    jX = (bz(si, sj + 1) - bz(si, sj - 1)) / two_dy;
-                    jZ = (byc(si + 1, sj) - byc(si - 1, sj)) / two_dx - (bxc(si, sj + 1) - bxc(si, sj - 1)) / two_dy;
-                    e = eta ? eta[at(g, i, j)] : g.eta;
-                    const double etaJX = e * jX, etaJZ = e * jZ;
+                    const int c1 = c0 + 1;                              // (i, j + 1)
+                    const double etaJX = J[J_X][c0], etaJZ = J[J_Z][c0];
                     const double etaJXBZ = etaJX * bz(si, sj), etaJZBX = etaJZ * bxc(si, sj);
-                    jX = (bz(si, sj + 2) - bz(si, sj)) / two_dy;
-                    jZ = (byc(si + 1, sj + 1) - byc(si - 1, sj + 1)) / two_dx
-                       - (bxc(si, sj + 2) - bxc(si, sj)) / two_dy;
-                    e = eta ? eta[at(g, i, j + 1)] : g.eta;
-                    const double etaJXPlus1 = e * jX, etaJZPlus1 = e * jZ;
+                    const double etaJXPlus1 = J[J_X][c1], etaJZPlus1 = J[J_Z][c1];
                     const double etaJXBZPlus1 = etaJXPlus1 * bz(si, sj + 1), etaJZBXPlus1 = etaJZPlus1 * bxc(si, sj + 1);
                     out[4] += 0.5 * (etaJZ + etaJZPlus1);
                     out[6] -= 0.5 * (etaJX + etaJXPlus1);
@@ -239,18 +271,33 @@ __global__ void contact_ref_kernel(Grid g, const double *U, const double *eta, d
     auto BX = [&](int ii, int jj) { return SMOOTHED ? bx_s(g, U, ii, jj) : U[BXF * P + at(g, ii, jj)]; };
     auto BY = [&](int ii, int jj) { return SMOOTHED ? by_s(g, U, ii, jj) : U[BYF * P + at(g, ii, jj)]; };
     const double dx = g.dx, dy = g.dy;
-    const double rho = U[RHO * P + k];
-    const double u = U[MX * P + k] / rho;
-    const double v = U[MY * P + k] / rho;
+    const double rho = U[RHO * P + k], mx = U[MX * P + k], my = U[MY * P + k];
     const double bX = 0.5 * (BX(i, j) + BX(i - 1, j));
     const double bY = 0.5 * (BY(i, j) + BY(i, j - 1));
-    const double jZ = 0.25 * (
-        (BY(i + 1, j) - BY(i, j)) / dx - (BX(i, j + 1) - BX(i, j)) / dy
-      + (BY(i + 1, j - 1) - BY(i, j - 1)) / dx - (BX(i, j) - BX(i, j - 1)) / dy
-      + (BY(i, j - 1) - BY(i - 1, j - 1)) / dx - (BX(i - 1, j) - BX(i - 1, j - 1)) / dy
-      + (BY(i, j) - BY(i - 1, j)) / dx - (BX(i - 1, j + 1) - BX(i - 1, j)) / dy);
+    // the differences of the current's eight terms, in the reference's order
+    const double nb[8] = {BY(i + 1, j) - BY(i, j),         BX(i, j + 1) - BX(i, j),
+                          BY(i + 1, j - 1) - BY(i, j - 1), BX(i, j) - BX(i, j - 1),
+                          BY(i, j - 1) - BY(i - 1, j - 1), BX(i - 1, j) - BX(i - 1, j - 1),
+                          BY(i, j) - BY(i - 1, j),         BX(i - 1, j + 1) - BX(i - 1, j)};
     const double e = eta ? eta[k] : g.eta;
-    ref[k] = u * bY - v * bX - e * jZ;
+    // divisions through shared correctly rounded reciprocals (MdDiv), or
+    // IEEE division where its guard fails: the same quotients
+    auto ref_of = [&](auto &dv) {
+        const double yr = dv.recip(rho), ydx = dv.recip(dx), ydy = dv.recip(dy);
+        const double u = dv.div(mx, rho, yr), v = dv.div(my, rho, yr);
+        const double jZ = 0.25 * (dv.div(nb[0], dx, ydx) - dv.div(nb[1], dy, ydy)
+                                + dv.div(nb[2], dx, ydx) - dv.div(nb[3], dy, ydy)
+                                + dv.div(nb[4], dx, ydx) - dv.div(nb[5], dy, ydy)
+                                + dv.div(nb[6], dx, ydx) - dv.div(nb[7], dy, ydy));
+        return u * bY - v * bX - e * jZ;
+    };
+    MdDiv md;
+    double r = ref_of(md);
+    if (!md.ok) {
+        IeeeDiv id;
+        r = ref_of(id);
+    }
+    ref[k] = r;
 }
 
 // The stage updates (resistiveMHD_2D.cu:53-130 functors, over k >= ny), all
@@ -405,14 +452,15 @@ void enqueue_contact_step(const ContactStep &c, cudaStream_t st)
         if (g.bc_x == BC_SYMMETRIC) launch_snapshot_row2(g, state, c.row2, st);
         launch_boundary(g, state, c.row2, nullptr, 0, st);
     };
+    cudaFuncSetAttribute(contact_flux_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CT_SMEM);
     contact_begin_kernel<<<1, 32, 0, st>>>(g, c.ctl, c.parity);
     // stage 1
-    contact_flux_tiled_kernel<<<flux_grid, CT_THREADS, 0, st>>>(g, c.A, c.eta, c.F1, c.G1);
+    contact_flux_tiled_kernel<<<flux_grid, CT_THREADS, CT_SMEM, st>>>(g, c.A, c.eta, c.F1, c.G1);
     contact_ref_kernel<true><<<b256, 256, 0, st>>>(g, c.A, c.eta, c.R1);
     contact_update_kernel<1><<<b256, 256, 0, st>>>(g, c.A, nullptr, c.F1, c.G1, c.ctl, c.B);
     boundary(c.B);
     // stage 2
-    contact_flux_tiled_kernel<<<flux_grid, CT_THREADS, 0, st>>>(g, c.B, c.eta, c.F2, c.G2);
+    contact_flux_tiled_kernel<<<flux_grid, CT_THREADS, CT_SMEM, st>>>(g, c.B, c.eta, c.F2, c.G2);
     contact_update_kernel<2><<<b256, 256, 0, st>>>(g, c.A, c.B, c.F2, c.G2, c.ctl, c.C);
     boundary(c.C);
     contact_ref_kernel<false><<<b256, 256, 0, st>>>(g, c.C, c.eta, c.R2);

@@ -773,6 +773,8 @@ template <class K> static void set_smem_attributes(K kernel, size_t smem, int ct
     cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct > 100 ? 100 : pct);
 }
 
+// The launchers pass the kernels local copies of their arguments, which a
+// launch captures by value.
 struct LaunchOne {
     const CUtensorMap *tmap, *emap;
     const StageArgs &args;
@@ -781,8 +783,10 @@ struct LaunchOne {
     {
         using T = Tile<ST, SH>;
         set_smem_attributes(stage_kernel<ST, SH>, T::SMEM_BYTES, T::CTAS);
-        const dim3 grid((args.g.ny - 2 * HALO + T::TJ - 1) / T::TJ, (args.g.nx - 2 * HALO + T::TI - 1) / T::TI);
-        stage_kernel<ST, SH><<<grid, T::THREADS, T::SMEM_BYTES, stream>>>(*tmap, *emap, args);
+        const CUtensorMap tm = *tmap, em = *emap;
+        const StageArgs a = args;
+        const dim3 grid((a.g.ny - 2 * HALO + T::TJ - 1) / T::TJ, (a.g.nx - 2 * HALO + T::TI - 1) / T::TI);
+        stage_kernel<ST, SH><<<grid, T::THREADS, T::SMEM_BYTES, stream>>>(tm, em, a);
     }
 };
 
@@ -802,7 +806,11 @@ struct LaunchBatch {
     {
         using T = Tile<ST, SH>;
         set_smem_attributes(stage_batch_kernel<ST, SH>, T::SMEM_BYTES, T::CTAS);
-        stage_batch_kernel<ST, SH><<<ctas, T::THREADS, T::SMEM_BYTES, stream>>>(runs, maps, tiles, ntiles, parity);
+        const BatchRun *r = runs;
+        const CUtensorMap *m = maps;
+        const TileRef *t = tiles;
+        const int n = ntiles, c = ctas, par = parity;
+        stage_batch_kernel<ST, SH><<<c, T::THREADS, T::SMEM_BYTES, stream>>>(r, m, t, n, par);
     }
 };
 
