@@ -264,19 +264,72 @@ __device__ __forceinline__ void reduce_ghost_rates(Control *ctl, int slot, unsig
     }
 }
 
-// Every ghost cell of one run.  With `ctl` set it also folds the ghost
-// cells' CFL rate and NaN-energy test into the reductions of the stage-2
-// kernel (slot = the next step's parity).
+// Field f of ghost cell (i, j): fill_ghost's value of that field alone.
 template <int BX, int BY>
-__global__ void boundary_kernel(Grid g, double *s, const double *row2, Control *ctl, int slot)
+__device__ __forceinline__ double ghost_field(const Grid &g, const double *s, const double *row2, int i, int j, int f)
 {
+    if (j >= 3 && j < g.ny - 3) return after_x_field<BX>(g, s, row2, f, i, j);
+    switch (BY >= 0 ? BY : g.bc_y) {
+    case BC_PERIODIC:
+        return after_x_field<BX>(g, s, row2, f, i, wrap(j, g.ny));
+    case BC_SYMMETRIC:
+        return f == BYF ? bY_yghost<BX>(g, s, row2, i, j) : after_x_field<BX>(g, s, row2, f, i, mirror(j, g.ny));
+    case BC_WALL: {
+        const int r = j < 3 ? 3 : g.ny - 4;
+        if (f == RHO || f == BXF || f == BZF) return after_x_field<BX>(g, s, row2, f, i, r);
+        if (f != EN) return f == BYF ? 0.0 : after_x_field<BX>(g, s, row2, RHO, i, r) * 0.0;
+        double c[NFIELD], v[NFIELD];
+        after_x_cell<BX>(g, s, row2, i, r, c);
+        mc_wall_state<false>(c, g.gamma, v);
+        return v[EN];
+    }
+    default:   // BC_ZERO_GRADIENT
+        return after_x_field<BX>(g, s, row2, f, i, j < 3 ? 3 : g.ny - 4);
+    }
+}
+
+// Every ghost cell of one run, one thread per (ghost cell, field): a block
+// of GHOST_CELLS x 8 threads holds GHOST_CELLS consecutive ghost cells, warp
+// f their field f, so that each thread follows only its own field's
+// dependences (a copy, or one wall-normal B integration chain) and the
+// launch spreads over every SM.  With `ctl` set the block's first warp also
+// folds the ghost cells' CFL rate and NaN-energy test into the reductions of
+// the stage-2 kernel (slot = the next step's parity), from the 8 values the
+// block staged in shared memory.  The values are fill_ghost's, bit for bit.
+constexpr int GHOST_CELLS = 32;
+template <int BX, int BY>
+__global__ void __launch_bounds__(GHOST_CELLS * NFIELD)
+boundary_kernel(Grid g, double *s, const double *row2, Control *ctl, int slot)
+{
+    __shared__ double sv[NFIELD][GHOST_CELLS];
     const long long nghost = 6LL * g.ny + 6LL * (g.nx - 6);
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, f = threadIdx.x >> 5;
+    const long long t = (long long)blockIdx.x * GHOST_CELLS + lane;
+    int i = 0, j = 0;
+    bool live = false;
+    if (t < nghost) {
+        ghost_cell(g, t, i, j);
+        live = !halo_col(g, i);   // a slab's halo comes from its neighbour
+    }
+    if (live) {
+        const double v = ghost_field<BX, BY>(g, s, row2, i, j, f);
+        s[f * g.plane + at(g, i, j)] = v;
+        if (ctl) sv[f][lane] = v;
+    }
+    if (!ctl) return;
+    __syncthreads();
+    if (f != 0) return;
     unsigned long long bits = 0ull;
     int nan_e = 0;
     bool c0 = false;
-    if (t < nghost) fill_ghost<BX, BY>(g, s, row2, t, ctl != nullptr, bits, nan_e, c0);
-    if (ctl) reduce_ghost_rates(ctl, slot, bits, nan_e, c0);
+    if (live) {
+        const double r = cfl_rate(sv[RHO][lane], sv[MX][lane], sv[MY][lane], sv[MZ][lane], sv[BXF][lane],
+                                  sv[BYF][lane], sv[BZF][lane], sv[EN][lane], g.gamma, g.dx, g.dy);
+        bits = rate_bits(r);
+        nan_e = sv[EN][lane] != sv[EN][lane];
+        c0 = (i == 0 && j == 0 && r != r);
+    }
+    reduce_ghost_rates(ctl, slot, bits, nan_e, c0);
 }
 
 // Every ghost cell of every run of a batch (blockIdx.y = run); `which`
@@ -434,8 +487,8 @@ int grid_for(long long n, int threads)
 void launch_boundary(const Grid &g, double *s, const double *row2, Control *ctl, int slot, cudaStream_t st)
 {
     const long long nghost = 6LL * g.ny + 6LL * (g.nx - 6);
-    const int threads = 256;
-    const int blocks = (int)((nghost + threads - 1) / threads);
+    const int threads = GHOST_CELLS * NFIELD;
+    const int blocks = (int)((nghost + GHOST_CELLS - 1) / GHOST_CELLS);
     // one instantiation per (x, y) wall pair; the y kind is a template
     // argument under each x kind
     auto launch = [&](auto kernel) { kernel<<<blocks, threads, 0, st>>>(g, s, row2, ctl, slot); };
