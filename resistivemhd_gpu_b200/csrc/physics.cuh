@@ -429,6 +429,162 @@ __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double g
     hlld_flux<ALL_CANDIDATES>(L, R, gm, EPS, ygm1, g1.ok, f);
 }
 
+// The reference's arithmetic in full (IEEE division, all six candidates
+// weighted), out of line: the rare path of hlld_flux_sel, kept from shaping
+// the register allocation of the common one.
+#if defined(__CUDACC__)
+#define RMHD_NOINLINE __noinline__
+#else
+#define RMHD_NOINLINE __attribute__((noinline))   // host builds of the kernels (CPU tests)
+#endif
+static __device__ RMHD_NOINLINE void hlld_flux_full(const Prim &L, const Prim &R, double gm, double EPS, double f[8])
+{
+    IeeeDiv id;
+    hlld_body<true>(L, R, gm, EPS, gm - 1.0, id, f);
+}
+
+// The exact HLLD flux with the candidate picked as the fan is built.  Every
+// value is the same expression as in hlld_body, so the bits are those of
+// hlld_flux<true>; only what stays live differs.  hlld_body keeps all six
+// candidate states (38 values) live until the region flags are known and
+// then selects; here each candidate is taken into the nine `c*` values as
+// soon as its own flag is known, so the left and right input states die
+// after the star states, and the magnitude guard is summed as the values
+// appear.  Where the shortcut's conditions fail -- a guard of the shared
+// reciprocals, more or fewer than one region selected, a value of 1e75 or
+// more (or non-finite) -- the interface is formed again by hlld_flux_full.
+__device__ __forceinline__ void hlld_flux_sel(const Prim &L, const Prim &R, double gm, double EPS, double ygm1,
+                                              bool gm1_ok, double f[8])
+{
+    MdDiv dv;
+    dv.ok = gm1_ok;
+    const double rhoL = L.rho, uL = L.u, vL = L.v, wL = L.w, bXL = L.bX, bYL = L.bY, bZL = L.bZ, pL = L.p;
+    const double rhoR = R.rho, uR = R.u, vR = R.v, wR = R.w, bXR = R.bX, bYR = R.bY, bZR = R.bZ, pR = R.p;
+    const double gm1 = gm - 1.0;
+
+    const double eL = dv.div(pL, gm1, ygm1)
+                    + 0.5 * rhoL * (uL * uL + vL * vL + wL * wL)
+                    + 0.5 * (bXL * bXL + bYL * bYL + bZL * bZL);
+    const double pTL = pL + 0.5 * (bXL * bXL + bYL * bYL + bZL * bZL);
+    const double eR = dv.div(pR, gm1, ygm1)
+                    + 0.5 * rhoR * (uR * uR + vR * vR + wR * wR)
+                    + 0.5 * (bXR * bXR + bYR * bYR + bZR * bZR);
+    const double pTR = pR + 0.5 * (bXR * bXR + bYR * bYR + bZR * bZR);
+    // magnitude guard of the shortcut (any order of summation will do: the
+    // guard only chooses between two evaluations with the same bits)
+    double mag = fabs(rhoL) + fabs(uL) + fabs(vL) + fabs(wL) + fabs(bXL) + fabs(bYL) + fabs(bZL) + fabs(eL)
+               + fabs(pTL) + fabs(rhoR) + fabs(uR) + fabs(vR) + fabs(wR) + fabs(bXR) + fabs(bYR) + fabs(bZR)
+               + fabs(eR) + fabs(pTR);
+
+    const double yrL = dv.recip(rhoL), yrR = dv.recip(rhoR);
+    const double csL = sqrt(dv.div(gm * pL, rhoL, yrL));
+    const double caL = sqrt(dv.div(bXL * bXL + bYL * bYL + bZL * bZL, rhoL, yrL));
+    const double vaL = sqrt(dv.div(bXL * bXL, rhoL, yrL));
+    const double cfL = sqrt(0.5 * (csL * csL + caL * caL
+                     + sqrt((csL * csL + caL * caL) * (csL * csL + caL * caL)
+                     - 4.0 * csL * csL * vaL * vaL)));
+    const double csR = sqrt(dv.div(gm * pR, rhoR, yrR));
+    const double caR = sqrt(dv.div(bXR * bXR + bYR * bYR + bZR * bZR, rhoR, yrR));
+    const double vaR = sqrt(dv.div(bXR * bXR, rhoR, yrR));
+    const double cfR = sqrt(0.5 * (csR * csR + caR * caR
+                     + sqrt((csR * csR + caR * caR) * (csR * csR + caR * caR)
+                     - 4.0 * csR * csR * vaR * vaR)));
+
+    double SL = tmin(uL, uR) - tmax(cfL, cfR);
+    double SR = tmax(uL, uR) + tmax(cfL, cfR);
+    SL = tmin(SL, 0.0);
+    SR = tmax(SR, 0.0);
+
+    // the outer states: candidates of their own
+    const bool bOL = SL > 0.0;
+    const bool bOR = SR <= 0.0;
+    double cr = bOL ? rhoL : rhoR, cu = bOL ? uL : uR, cv = bOL ? vL : vR, cw = bOL ? wL : wR;
+    double cbx = bOL ? bXL : bXR, cby = bOL ? bYL : bYR, cbz = bOL ? bZL : bZR;
+    double ce = bOL ? eL : eR, cpt = bOL ? pTL : pTR;
+    int nsel = (int)bOL + (int)bOR;
+
+    const double den = (SR - uR) * rhoR - (SL - uL) * rhoL + EPS;
+    const double yden = dv.recip(den);
+    const double SM = dv.div((SR - uR) * rhoR * uR - (SL - uL) * rhoL * uL - pTR + pTL, den, yden);
+    const double pT1 = dv.div((SR - uR) * rhoR * pTL - (SL - uL) * rhoL * pTR
+                              + rhoL * rhoR * (SR - uR) * (SL - uL) * (uR - uL), den, yden);
+    mag += fabs(SM) + fabs(pT1);
+
+    // left star state (u1L = SM, bX1L = bXL)
+    const double dLM = SL - SM + EPS;
+    const double yLM = dv.recip(dLM);
+    const double DL = rhoL * (SL - uL) * (SL - SM) - bXL * bXL + EPS;
+    const double yDL = dv.recip(DL);
+    const double NL = rhoL * (SL - uL) * (SL - uL) - bXL * bXL;
+    const double rho1L = dv.div(rhoL * (SL - uL), dLM, yLM);
+    const double v1L = vL - dv.div(bXL * bYL * (SM - uL), DL, yDL);
+    const double w1L = wL - dv.div(bXL * bZL * (SM - uL), DL, yDL);
+    const double bY1L = dv.div(bYL * NL, DL, yDL);
+    const double bZ1L = dv.div(bZL * NL, DL, yDL);
+    const double vb1L = SM * bXL + v1L * bY1L + w1L * bZ1L;
+    const double e1L = dv.div((SL - uL) * eL - pTL * uL + pT1 * SM
+                              + bXL * ((uL * bXL + vL * bYL + wL * bZL) - vb1L),
+                              dLM, yLM);
+    mag += fabs(rho1L) + fabs(v1L) + fabs(w1L) + fabs(bY1L) + fabs(bZ1L) + fabs(e1L);
+    const double yr1L = dv.recip(rho1L);
+    const double S1L = SM - sqrt(dv.div(bXL * bXL, rho1L, yr1L));
+    const bool bML = (SL <= 0.0) && (0.0 < S1L);
+    const bool bIL = (S1L <= 0.0) && (0.0 < SM);
+    if (bML) {
+        cr = rho1L; cu = SM; cv = v1L; cw = w1L; cbx = bXL; cby = bY1L; cbz = bZ1L; ce = e1L; cpt = pT1;
+    }
+
+    // right star state
+    const double dRM = SR - SM + EPS;
+    const double yRM = dv.recip(dRM);
+    const double DR = rhoR * (SR - uR) * (SR - SM) - bXR * bXR + EPS;
+    const double yDR = dv.recip(DR);
+    const double NR = rhoR * (SR - uR) * (SR - uR) - bXR * bXR;
+    const double rho1R = dv.div(rhoR * (SR - uR), dRM, yRM);
+    const double v1R = vR - dv.div(bXR * bYR * (SM - uR), DR, yDR);
+    const double w1R = wR - dv.div(bXR * bZR * (SM - uR), DR, yDR);
+    const double bY1R = dv.div(bYR * NR, DR, yDR);
+    const double bZ1R = dv.div(bZR * NR, DR, yDR);
+    const double vb1R = SM * bXR + v1R * bY1R + w1R * bZ1R;
+    const double e1R = dv.div((SR - uR) * eR - pTR * uR + pT1 * SM
+                              + bXR * ((uR * bXR + vR * bYR + wR * bZR) - vb1R),
+                              dRM, yRM);
+    mag += fabs(rho1R) + fabs(v1R) + fabs(w1R) + fabs(bY1R) + fabs(bZ1R) + fabs(e1R);
+    const double yr1R = dv.recip(rho1R);
+    const double S1R = SM + sqrt(dv.div(bXR * bXR, rho1R, yr1R));
+    const bool bMR = (S1R <= 0.0) && (0.0 < SR);
+    const bool bIR = (SM <= 0.0) && (0.0 < S1R);
+    if (bMR) {
+        cr = rho1R; cu = SM; cv = v1R; cw = w1R; cbx = bXR; cby = bY1R; cbz = bZ1R; ce = e1R; cpt = pT1;
+    }
+    nsel += (int)bML + (int)bIL + (int)bMR + (int)bIR;
+
+    // double-star states (u2 = SM)
+    const double sqL = sqrt(rho1L), sqR = sqrt(rho1R), sqLR = sqrt(rho1L * rho1R);
+    const double sbX = sgn(bXL);
+    const double dsq = sqL + sqR + EPS;
+    const double ysq = dv.recip(dsq);
+    const double v2 = dv.div(sqL * v1L + sqR * v1R + (bY1R - bY1L) * sbX, dsq, ysq);
+    const double w2 = dv.div(sqL * w1L + sqR * w1R + (bZ1R - bZ1L) * sbX, dsq, ysq);
+    const double bY2 = dv.div(sqL * bY1R + sqR * bY1L + sqLR * (v1R - v1L) * sbX, dsq, ysq);
+    const double bZ2 = dv.div(sqL * bZ1R + sqR * bZ1L + sqLR * (w1R - w1L) * sbX, dsq, ysq);
+    const double e2L = e1L - sqL * (vb1L - (SM * bXL + v2 * bY2 + w2 * bZ2)) * sgn(bXL);
+    const double e2R = e1R + sqR * (vb1R - (SM * bXR + v2 * bY2 + w2 * bZ2)) * sgn(bXR);
+    mag += fabs(v2) + fabs(w2) + fabs(bY2) + fabs(bZ2) + fabs(e2L) + fabs(e2R);
+    if (bIL | bIR) {
+        cr = bIL ? rho1L : rho1R; cu = SM; cv = v2; cw = w2; cbx = bIL ? bXL : bXR;
+        cby = bY2; cbz = bZ2; ce = bIL ? e2L : e2R; cpt = pT1;
+    }
+
+    if (!dv.ok || nsel != 1 || !(mag < 1e75)) {
+        hlld_flux_full(L, R, gm, EPS, f);
+        return;
+    }
+#pragma unroll
+    for (int n = 0; n < 8; ++n) f[n] = 0.0;
+    add_one_flux(cr, cu, cv, cw, cbx, cby, cbz, ce, cpt, f);
+}
+
 // HLLD flux of the fast variant: the same wave-speed estimates, star and
 // double-star states and candidate selection as hlld_flux (hlld.cu:256-565),
 // rearranged for the FP64 pipe.  It differs from the exact form by rounding

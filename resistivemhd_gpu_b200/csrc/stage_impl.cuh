@@ -484,7 +484,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
 #if RMHD_FAST_MATH
             hlld_flux_fast(L, R, gmR, inv_gm1, EPSR, f);
 #else
-            hlld_flux<RMHD_ALL_CANDIDATES>(L, R, gm, EPS, ygm1, gm1_ok, f);
+            hlld_flux_sel(L, R, gm, EPS, ygm1, gm1_ok, f);
 #endif
             fmv[0] = f[1]; fmv[1] = f[2]; fmv[2] = f[3];
             fov[0] = f[0]; fov[1] = f[6]; fov[2] = f[7]; fov[3] = f[5];
