@@ -205,7 +205,8 @@ int rmhd2d_write_snapshot(const char *path, const double *host_state, int nx, in
    0: 8x32 / 9x32 and 1: 16x16 / 18x16 with 320 threads, 2 CTAs per SM;
    2: 16x32 / 18x32 with 640 threads, 1 CTA per SM (fewer redundant ring
    fluxes per cell); 3: 8x64 / 8x64 with 512 threads, 1 CTA per SM (128
-   registers per thread); 4: 8x32 / 8x32 with 256 threads, 3 CTAs per SM.
+   registers per thread); 4: 8x32 / 8x32 and 5: 6x32 / 7x32 with 256
+   threads, 3 CTAs per SM.
    Each stage has its own shape: rmhd2d_set_tile_shape
    sets both, rmhd2d_set_stage_shapes each, rmhd2d_get_tile_shape returns
    stage 1's.  rmhd2d_autotune times trial_steps steps with each shape (CUDA
@@ -236,9 +237,9 @@ int rmhd2d_batch_size(const rmhd2d_batch *b, int *nruns);
 int rmhd2d_batch_member(rmhd2d_batch *b, int run, rmhd2d_solver **member);
 int rmhd2d_batch_run(rmhd2d_batch *b, int nsteps);
 int rmhd2d_batch_run_timed(rmhd2d_batch *b, int nsteps, float *ms);
-/* Launch configuration: tile shape (0..4, as above) and persistent CTAs per
+/* Launch configuration: tile shape (0..5, as above) and persistent CTAs per
    SM (1 up to the shape's CTAs per SM: 2 for shapes 0 and 1, 1 for 2 and 3,
-   3 for 4); rmhd2d_batch_autotune times every valid pair
+   3 for 4 and 5); rmhd2d_batch_autotune times every valid pair
    (state restored afterwards) and keeps the fastest; rmhd2d_batch_get_tuning
    returns each pair tried with its ms per step (up to max entries, *n =
    the number tried). */

@@ -429,15 +429,9 @@ __device__ __forceinline__ void hlld_flux(const Prim &L, const Prim &R, double g
     hlld_flux<ALL_CANDIDATES>(L, R, gm, EPS, ygm1, g1.ok, f);
 }
 
-// The reference's arithmetic in full (IEEE division, all six candidates
-// weighted), out of line: the rare path of hlld_flux_sel, kept from shaping
-// the register allocation of the common one.
-#if defined(__CUDACC__)
-#define RMHD_NOINLINE __noinline__
-#else
-#define RMHD_NOINLINE __attribute__((noinline))   // host builds of the kernels (CPU tests)
-#endif
-static __device__ RMHD_NOINLINE void hlld_flux_full(const Prim &L, const Prim &R, double gm, double EPS, double f[8])
+// The reference's arithmetic in full: IEEE division and all six candidates
+// weighted, for every input.  The rare path of hlld_flux_sel.
+__device__ __forceinline__ void hlld_flux_ieee(const Prim &L, const Prim &R, double gm, double EPS, double f[8])
 {
     IeeeDiv id;
     hlld_body<true>(L, R, gm, EPS, gm - 1.0, id, f);
@@ -452,8 +446,11 @@ static __device__ RMHD_NOINLINE void hlld_flux_full(const Prim &L, const Prim &R
 // after the star states, and the magnitude guard is summed as the values
 // appear.  Where the shortcut's conditions fail -- a guard of the shared
 // reciprocals, more or fewer than one region selected, a value of 1e75 or
-// more (or non-finite) -- the interface is formed again by hlld_flux_full.
-__device__ __forceinline__ void hlld_flux_sel(const Prim &L, const Prim &R, double gm, double EPS, double ygm1,
+// more (or non-finite) -- it returns false with f unwritten, and the caller
+// forms the interface with hlld_flux_ieee, away from its common path (the
+// stage kernel's flux phase does that after its loop, for the interfaces
+// that asked, so the rare path does not shape the common path's registers).
+__device__ __forceinline__ bool hlld_flux_sel(const Prim &L, const Prim &R, double gm, double EPS, double ygm1,
                                               bool gm1_ok, double f[8])
 {
     MdDiv dv;
@@ -576,13 +573,11 @@ __device__ __forceinline__ void hlld_flux_sel(const Prim &L, const Prim &R, doub
         cby = bY2; cbz = bZ2; ce = bIL ? e2L : e2R; cpt = pT1;
     }
 
-    if (!dv.ok || nsel != 1 || !(mag < 1e75)) {
-        hlld_flux_full(L, R, gm, EPS, f);
-        return;
-    }
+    if (!dv.ok || nsel != 1 || !(mag < 1e75)) return false;
 #pragma unroll
     for (int n = 0; n < 8; ++n) f[n] = 0.0;
     add_one_flux(cr, cu, cv, cw, cbx, cby, cbz, ce, cpt, f);
+    return true;
 }
 
 // HLLD flux of the fast variant: the same wave-speed estimates, star and
@@ -592,8 +587,14 @@ __device__ __forceinline__ void hlld_flux_sel(const Prim &L, const Prim &R, doub
 // of 28 divisions), squared sound/Alfven speeds used directly (the reference
 // squares their square roots), sqrt(rho*) and |bX|/sqrt(rho*) from one rsqrt,
 // and bX taken once (left and right states share the interface-normal B).
-template <typename T>
-__device__ __forceinline__ void hlld_flux_fast(const PrimT<T> &L, const PrimT<T> &R, T gm, T inv_gm1, T EPS, T f[8])
+//
+// ONE = true forms the common case only: exactly one region selected and
+// finite wave speeds.  That region's state is taken into the `c*` values as
+// soon as its flag is known, so the input states need not stay live until
+// the end; it returns false (f unwritten) when the case does not apply.
+// ONE = false forms every case.
+template <bool ONE, typename T>
+__device__ __forceinline__ bool hlld_fast_body(const PrimT<T> &L, const PrimT<T> &R, T gm, T inv_gm1, T EPS, T f[8])
 {
     const T bX = L.bX;
     const T bx2 = bX * bX;
@@ -628,6 +629,14 @@ __device__ __forceinline__ void hlld_flux_fast(const PrimT<T> &L, const PrimT<T>
     SL = tmin(SL, T(0));
     SR = tmax(SR, T(0));
 
+    const bool bOL = SL > T(0);
+    const bool bOR = SR <= T(0);
+    T cr, cu, cv, cw, cby, cbz, ce, cpt;   // the selected candidate (ONE)
+    if (ONE) {
+        cr = bOL ? L.rho : R.rho; cu = bOL ? L.u : R.u; cv = bOL ? L.v : R.v; cw = bOL ? L.w : R.w;
+        cby = bOL ? L.bY : R.bY; cbz = bOL ? L.bZ : R.bZ; ce = bOL ? eL : eR; cpt = bOL ? pTL : pTR;
+    }
+
     const T dSL = SL - uL, dSR = SR - uR;
     const T rdSL = L.rho * dSL, rdSR = R.rho * dSR;
     const T iden = rcp_nr(rdSR - rdSL + EPS);
@@ -653,6 +662,14 @@ __device__ __forceinline__ void hlld_flux_fast(const PrimT<T> &L, const PrimT<T>
     const T sqL = rho1L * rsL, sqR = rho1R * rsR;
     const T abx = fabs(bX);
     const T S1L = SM - abx * rsL, S1R = SM + abx * rsR;
+    const bool bML = (SL <= T(0)) && (T(0) < S1L);
+    const bool bIL = (S1L <= T(0)) && (T(0) < SM);
+    const bool bMR = (S1R <= T(0)) && (T(0) < SR);
+    const bool bIR = (SM <= T(0)) && (T(0) < S1R);
+    if (ONE && (bML | bMR)) {
+        cr = bML ? rho1L : rho1R; cu = SM; cv = bML ? v1L : v1R; cw = bML ? w1L : w1R;
+        cby = bML ? bY1L : bY1R; cbz = bML ? bZ1L : bZ1R; ce = bML ? e1L : e1R; cpt = pT1;
+    }
     const T sb = sgn(bX);
     const T id2 = rcp_nr(sqL + sqR + EPS);
     const T sqLR = sqL * sqR;
@@ -664,15 +681,21 @@ __device__ __forceinline__ void hlld_flux_fast(const PrimT<T> &L, const PrimT<T>
     const T e2L = e1L - sqL * (vb1L - vb2) * sb;
     const T e2R = e1R + sqR * (vb1R - vb2) * sb;
 
-    const bool bOL = SL > T(0);
-    const bool bML = (SL <= T(0)) && (T(0) < S1L);
-    const bool bIL = (S1L <= T(0)) && (T(0) < SM);
-    const bool bOR = SR <= T(0);
-    const bool bMR = (S1R <= T(0)) && (T(0) < SR);
-    const bool bIR = (SM <= T(0)) && (T(0) < S1R);
+    const int nsel = (int)bOL + (int)bML + (int)bIL + (int)bOR + (int)bMR + (int)bIR;
+    const bool nan_speed = (SL != SL) | (SR != SR) | (SM != SM) | (S1L != S1L) | (S1R != S1R);
+    if (ONE) {
+        if (nsel != 1 || nan_speed) return false;
+        if (bIL | bIR) {
+            cr = bIL ? rho1L : rho1R; cu = SM; cv = v2; cw = w2; cby = bY2; cbz = bZ2; ce = bIL ? e2L : e2R;
+            cpt = pT1;
+        }
+#pragma unroll
+        for (int n = 0; n < 8; ++n) f[n] = T(0);
+        add_one_flux(cr, cu, cv, cw, bX, cby, cbz, ce, cpt, f);
+        return true;
+    }
 #pragma unroll
     for (int n = 0; n < 8; ++n) f[n] = T(0);
-    const int nsel = (int)bOL + (int)bML + (int)bIL + (int)bOR + (int)bMR + (int)bIR;
     if (nsel == 1) {
         // The usual case: one region is selected; pick its state with
         // selects and form one flux (no per-candidate divergence in a warp).
@@ -697,10 +720,28 @@ __device__ __forceinline__ void hlld_flux_fast(const PrimT<T> &L, const PrimT<T>
     }
     // NaN wave speeds select no candidate here, while the reference's
     // weighted sum turns them into a NaN flux: do the same.
-    if ((SL != SL) | (SR != SR) | (SM != SM) | (S1L != S1L) | (S1R != S1R)) {
+    if (nan_speed) {
 #pragma unroll
         for (int n = 0; n < 8; ++n) f[n] = qnan;
     }
+    return true;
+}
+
+// Every case of the fast HLLD flux.
+template <typename T>
+__device__ __forceinline__ void hlld_flux_fast(const PrimT<T> &L, const PrimT<T> &R, T gm, T inv_gm1, T EPS, T f[8])
+{
+    hlld_fast_body<false>(L, R, gm, inv_gm1, EPS, f);
+}
+
+// The common case of the fast HLLD flux (one region, finite wave speeds);
+// false, with f unwritten, where it does not apply: the caller then forms
+// the interface with hlld_flux_fast away from its common path.
+template <typename T>
+__device__ __forceinline__ bool hlld_flux_fast_sel(const PrimT<T> &L, const PrimT<T> &R, T gm, T inv_gm1, T EPS,
+                                                   T f[8])
+{
+    return hlld_fast_body<true>(L, R, gm, inv_gm1, EPS, f);
 }
 
 // Inputs of the FP32-bulk HLLD flux at one interface: the reconstructed

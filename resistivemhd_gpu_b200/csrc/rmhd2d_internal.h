@@ -53,23 +53,28 @@ enum KernelError { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };
 //   shape 2: stage 1 16 x 32 (1172),           stage 2 18 x 32 (1202); 640 threads, 1 CTA per SM
 //   shape 3: stage 1  8 x 64 (1244),           stage 2  8 x 64 (1096); 512 threads, 1 CTA per SM
 //   shape 4: stage 1  8 x 32 (636),            stage 2  8 x 32 (552);  256 threads, 3 CTAs per SM
+//   shape 5: stage 1  6 x 32 (502),            stage 2  7 x 32 (487);  256 threads, 3 CTAs per SM
 // Shape 2 forms 2.29 (stage 1) and 2.09 (stage 2) interfaces per cell
 // against 2.48 and 2.14, at the same 20 warps per SM, but one CTA per SM
 // leaves no second CTA to run while the first waits at a barrier.  Shape 3
 // gives each thread 128 registers (16 warps per SM), shape 4 80 (24 warps
-// in three CTAs).  Which is fastest for a variant and grid is the
-// autotuners' question.
+// in three CTAs).  Shape 5 is shape 4 with fewer rows: each stage's
+// interfaces fit two passes of its 256 threads, where shape 4 needs a
+// third pass that leaves most of its threads idle (stage 2: 40 of 256).
+// Which is fastest for a variant and grid is the autotuners' question.
 constexpr int HALO = 3;
-constexpr int NSHAPE = 5;
+constexpr int NSHAPE = 6;
 constexpr int shape_tj(int shape) { return shape == 1 ? 16 : shape == 3 ? 64 : 32; }
 constexpr int stage_ti(int stage, int shape)
 {
-    return shape == 0 ? (stage == 1 ? 8 : 9) : shape >= 3 ? 8 : (stage == 1 ? 16 : 18);
+    return shape == 0 ? (stage == 1 ? 8 : 9)
+         : shape == 5 ? (stage == 1 ? 6 : 7)
+         : shape >= 3 ? 8 : (stage == 1 ? 16 : 18);
 }
 constexpr int stage_ui(int stage, int shape) { return stage_ti(stage, shape) + 2 * HALO; }
 constexpr int shape_uj(int shape) { return shape_tj(shape) + 2 * HALO; }  // TMA inner box: UJ * 8 B, a multiple of 16
-constexpr int shape_threads(int shape) { return shape == 2 ? 640 : shape == 3 ? 512 : shape == 4 ? 256 : 320; }
-constexpr int shape_max_ctas(int shape) { return shape == 2 || shape == 3 ? 1 : shape == 4 ? 3 : 2; }   // CTAs per SM that fit
+constexpr int shape_threads(int shape) { return shape == 2 ? 640 : shape == 3 ? 512 : shape >= 4 ? 256 : 320; }
+constexpr int shape_max_ctas(int shape) { return shape == 2 || shape == 3 ? 1 : shape >= 4 ? 3 : 2; }   // CTAs per SM that fit
 constexpr bool shapes_have_a_thread_per_cell()
 {
     for (int s = 0; s < NSHAPE; ++s)

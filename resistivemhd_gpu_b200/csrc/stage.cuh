@@ -53,6 +53,10 @@ template <bool F> struct SweepC {
 struct SweepRT {
     bool value;
 };
+// Whether an interface takes the exact variant's rare path (see flux_at).
+template <bool B> struct FullC {
+    static constexpr bool value = B;
+};
 
 namespace exact {
 void launch_stage(int stage, int shape, const CUtensorMap *tmap, const CUtensorMap *emap, const StageArgs &args,

@@ -384,7 +384,13 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
     // copies, and the exact variant, which measured slower with them, pass
     // it at run time.  Both sweeps share one index space, so the threads
     // stay balanced.
-    auto flux_at = [&](const int it, const auto sweep) {
+    // `full` (a FullC tag) selects the FP64 variants' rare path for an
+    // interface whose common-case flux declined (hlld_flux_sel or
+    // hlld_flux_fast_sel returned false; flux_at then stores nothing and
+    // returns false): every case of the fast flux, or in the exact variant
+    // the reference's arithmetic in full (hlld_flux_ieee).
+    auto flux_at = [&](const int it, const auto sweep, const auto full) -> bool {
+        (void)full;
         const bool isF = sweep.value;
         int a0, a1;   // (fi, fj) or (gi, gj)
         int ci, cj;   // the cell left of / below the interface, relative to (i0, j0)
@@ -482,9 +488,15 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
             const PrimT<Real> R{qR[0], qR[1], qR[2], qR[3], (Real)bn, qR[4], qR[5], qR[6]};
             Real f[8];
 #if RMHD_FAST_MATH
-            hlld_flux_fast(L, R, gmR, inv_gm1, EPSR, f);
+            if (full.value)
+                hlld_flux_fast(L, R, gmR, inv_gm1, EPSR, f);
+            else if (!hlld_flux_fast_sel(L, R, gmR, inv_gm1, EPSR, f))
+                return false;
 #else
-            hlld_flux_sel(L, R, gm, EPS, ygm1, gm1_ok, f);
+            if (full.value)
+                hlld_flux_ieee(L, R, gm, EPS, f);
+            else if (!hlld_flux_sel(L, R, gm, EPS, ygm1, gm1_ok, f))
+                return false;
 #endif
             fmv[0] = f[1]; fmv[1] = f[2]; fmv[2] = f[3];
             fov[0] = f[0]; fov[1] = f[6]; fov[2] = f[7]; fov[3] = f[5];
@@ -519,15 +531,29 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
             oo[O_EN * SG] = fov[2] + (h * (eZ0 * x0 + eZ1 * x1) - h * (eX0 * z0 + eX1 * z1));
             if (STAGE == 1) oo[O_EMF * SG] = fov[1] + h * (eZ0 + eZ1);
         }
+        return true;
     };
-    for (int it = tid; it < T::NF + T::NG; it += T::THREADS) {
+    // bit r of `redo`: this thread's interface of pass r asked for the full path
+    unsigned redo = 0u;
+    static_assert((T::NF + T::NG + T::THREADS - 1) / T::THREADS <= 32, "passes of the flux phase");
+    for (int it = tid, r = 0; it < T::NF + T::NG; it += T::THREADS, ++r) {
+        bool done;
         if (STAGE == 1 || !RMHD_FAST_MATH)
-            flux_at(it, SweepRT{it < T::NF});
+            done = flux_at(it, SweepRT{it < T::NF}, FullC<false>{});
         else if (it < T::NF)
-            flux_at(it, SweepC<true>{});
+            done = flux_at(it, SweepC<true>{}, FullC<false>{});
         else
-            flux_at(it, SweepC<false>{});
+            done = flux_at(it, SweepC<false>{}, FullC<false>{});
+        redo |= done ? 0u : 1u << r;
     }
+#if !RMHD_BULK
+    // The FP64 variants' rare path, after the loop, so that its registers
+    // do not weigh on the loop's.
+    if (redo) {
+        for (int it = tid, r = 0; it < T::NF + T::NG; it += T::THREADS, ++r)
+            if ((redo >> r) & 1u) flux_at(it, SweepRT{it < T::NF}, FullC<true>{});
+    }
+#endif
     // The update's own cell of the stage's source state (from global memory
     // when the flux planes overlay the staged tile), and in stage 2 that of
     // U^n: issue those loads here, so that their latency overlaps the
@@ -729,11 +755,12 @@ template <class F> static void with_stage_shape(int stage, int shape, const F &f
     RMHD_SHAPE_CASE(1)
     RMHD_SHAPE_CASE(2)
     RMHD_SHAPE_CASE(3)
-    default: RMHD_SHAPE_CASE(4)
+    RMHD_SHAPE_CASE(4)
+    default: RMHD_SHAPE_CASE(5)
     }
 #undef RMHD_SHAPE_CASE
 }
-static_assert(NSHAPE == 5, "one case per tile shape in with_stage_shape");
+static_assert(NSHAPE == 6, "one case per tile shape in with_stage_shape");
 
 struct SmemOf {
     size_t &n;

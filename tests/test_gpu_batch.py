@@ -61,7 +61,7 @@ def mixed_setups():
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
-@pytest.mark.parametrize("shape", [1, 2, 3, 4, (1, 0), (2, 1), (3, 4), (4, 3)])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5, (1, 0), (2, 1), (3, 4), (4, 3), (5, 4), (0, 5)])
 def test_tile_shapes_equal_shape_0(gpu, precision, shape):
     from resistivemhd_gpu_b200 import setups
 
@@ -112,10 +112,10 @@ def test_batch_autotune_restores_state(gpu):
     with Batch(sets, precision="fp64_fast") as b:
         before = [b[r].get_state().copy() for r in range(len(b))]
         shape, ctas = b.autotune(trial_steps=2)
-        assert shape in range(5) and ctas in (1, 2, 3)
+        assert shape in range(6) and ctas in (1, 2, 3)
         table = b.tuning()
         assert [(sh, c) for sh, c, _ in table] == [(0, 1), (0, 2), (1, 1), (1, 2), (2, 1), (3, 1), (4, 1), (4, 2),
-                                                   (4, 3)]
+                                                   (4, 3), (5, 1), (5, 2), (5, 3)]
         assert all(m > 0 for _, _, m in table)
         assert b.launch == (shape, ctas)
         for r in range(len(b)):
@@ -145,9 +145,9 @@ def test_solver_autotune(gpu):
     with Solver.from_setup(s, precision="fp64_fast") as sol:
         before = sol.get_state().copy()
         shape = sol.autotune(trial_steps=2)
-        assert shape in range(5) and sol.tile_shape == shape
+        assert shape in range(6) and sol.tile_shape == shape
         t = sol.tuning()
-        assert sorted(t) == [0, 1, 2, 3, 4] and all(a > 0 and b > 0 for a, b in t.values())
+        assert sorted(t) == [0, 1, 2, 3, 4, 5] and all(a > 0 and b > 0 for a, b in t.values())
         s1, s2 = sol.stage_shapes
         assert s1 == shape and t[s2][1] == min(b for _, b in t.values())
         assert np.array_equal(sol.get_state(), before)

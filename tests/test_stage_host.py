@@ -65,7 +65,7 @@ def run_host(lib, s, nsteps, shape, apply_boundary=True, fixed_dts=None):
     return state, dts[:nsteps], rc - 1 if rc > 0 else -1
 
 
-@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("dims,nsteps,bc,bc_y,with_table", [
     ((20, 18), 3, "periodic", None, False),
     ((37, 29), 2, "periodic", None, True),
@@ -85,7 +85,7 @@ def test_host_stage_step_equals_oracle(host_stage, oracle, shape, dims, nsteps, 
     assert np.array_equal(got, want, equal_nan=True)
 
 
-@pytest.mark.parametrize("shape,ctas", [(0, 1), (0, 3), (1, 2), (2, 1), (3, 1), (4, 2)])
+@pytest.mark.parametrize("shape,ctas", [(0, 1), (0, 3), (1, 2), (2, 1), (3, 1), (4, 2), (5, 3)])
 def test_host_batch_equals_single_oracle_runs(host_stage, oracle, shape, ctas):
     """The persistent batch kernel over runs of uneven size and walls: a few
     CTAs walk the tile table (flipping the mbarrier's phase tile by tile),
@@ -131,7 +131,7 @@ def host_stage_contracted(request, tmp_path_factory):
 HOST_REL_L1 = {"fast": 1e-12, "bulk32": 1e-5}
 
 
-@pytest.mark.parametrize("shape", [0, 1, 3, 4])
+@pytest.mark.parametrize("shape", [0, 1, 3, 4, 5])
 @pytest.mark.parametrize("dims,bc,bc_y,with_table", [
     ((37, 29), "periodic", None, True),
     ((26, 40), "symmetric", None, True),
