@@ -53,7 +53,7 @@ constexpr int variant_threads(int stage, int shape)
 // Et [UI][UJ] f64        TMA: eta table on the same cells (when a table is set)
 // Pv [4][TI+4][TJ+4]     u, v, w, rho (flux-side type)
 // Pb [5][TI+4][TJ+4] f64 centred bX, centred bY, x- and y-sweep pressures, bZ
-// Rs [3][TI+2][TJ+2]     eta*Jx, eta*Jy, eta*Jz (flux-side type); reused for the corner EMF (f64)
+// Rs [3][TI+2][TJ+2]     eta*Jx, eta*Jy, eta*Jz (flux-side type)
 // Fm [3][TI+1][F_NJ] f64 x fluxes of rhoU, rhoV, rhoW at i+1/2
 // Fo [NO][TI+1][F_NJ]    x fluxes of rho, bZ, e (+ bY = EMF part, stage 1), flux-side type
 // Gm, Go                 the same for the y fluxes at j+1/2 (Go slot 3: the bX flux)
@@ -81,7 +81,6 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr int G_I0 = STAGE == 1 ? -1 : 0;         // column of gi = 0, relative to i0
     static constexpr int G_NI = STAGE == 1 ? TI + 2 : TI;
     static constexpr int G_NJ = TJ + 1;
-    static constexpr int EI_ = TI + 1, EJ_ = TJ + 1;
     static constexpr int UF = UI * UJ;                       // doubles per staged field
     static constexpr int PF = PI_ * PJ_;
     static constexpr int RF = RI_ * RJ_;
@@ -94,8 +93,7 @@ template <int STAGE, int SHAPE> struct Tile {
     static constexpr size_t PV_BYTES = up16((size_t)4 * PF * sizeof(Real));
     static constexpr size_t PB_BYTES = up16((size_t)5 * PF * 8);
     static constexpr size_t R_ETA = (size_t)3 * RF * sizeof(Real);
-    static constexpr size_t R_EMF = STAGE == 1 ? (size_t)EI_ * EJ_ * 8 : 0;
-    static constexpr size_t R_BYTES = up16(R_ETA > R_EMF ? R_ETA : R_EMF);
+    static constexpr size_t R_BYTES = up16(R_ETA);
     static constexpr size_t FM_BYTES = up16((size_t)3 * SF * 8);
     static constexpr size_t FO_BYTES = up16((size_t)NO * SF * sizeof(Real));
     static constexpr size_t GM_BYTES = up16((size_t)3 * SG * 8);
@@ -213,13 +211,12 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
     using T = Tile<STAGE, SHAPE>;
     using Real = typename T::Real;
     constexpr int TI = T::TI, TJ = T::TJ, UJ = T::UJ, UF = T::UF, PF = T::PF, RF = T::RF, SF = T::SF, SG = T::SG;
-    constexpr int PJ_ = T::PJ_, RJ_ = T::RJ_, F_NJ = T::F_NJ, G_NJ = T::G_NJ, EJ_ = T::EJ_;
+    constexpr int PJ_ = T::PJ_, RJ_ = T::RJ_, F_NJ = T::F_NJ, G_NJ = T::G_NJ;
     double *Ut = reinterpret_cast<double *>(smem_raw + T::OFF_U);
     double *Et = reinterpret_cast<double *>(smem_raw + T::OFF_E);
     Real *Pv = reinterpret_cast<Real *>(smem_raw + T::OFF_PV);
     double *Pb = reinterpret_cast<double *>(smem_raw + T::OFF_PB);
     Real *Rs = reinterpret_cast<Real *>(smem_raw + T::OFF_R);
-    double *Ez = reinterpret_cast<double *>(smem_raw + T::OFF_R);
     double *Fm = reinterpret_cast<double *>(smem_raw + T::OFF_FM);
     Real *Fo = reinterpret_cast<Real *>(smem_raw + T::OFF_FO);
     double *Gm = reinterpret_cast<double *>(smem_raw + T::OFF_GM);
@@ -575,20 +572,17 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
 
     const double dtdx = dt / g.dx, dtdy = dt / g.dy;
 
-    if (STAGE == 1) {
-        // ---- corner EMF (ct.cu:22-41) on (TI+1) x (TJ+1) corners (i, j) =
-        // (i0-1+ei, j0-1+ej), i.e. Fs (fi, fj) = (ei, ej) and Gs (gi, gj) = (ei, ej) ----
-        for (int c = tid; c < T::EI_ * EJ_; c += T::THREADS) {
-            const int ei = c / EJ_, ej = c - ei * EJ_;
-            // accumulated in FP64 whatever the flux-side type
-            const double eZG1 = (double)Go[O_EMF * SG + ei * G_NJ + ej];
-            const double eZG2 = (double)Go[O_EMF * SG + (ei + 1) * G_NJ + ej];
-            const double eZF1 = -1.0 * (double)Fo[O_EMF * SF + ei * F_NJ + ej];
-            const double eZF2 = -1.0 * (double)Fo[O_EMF * SF + ei * F_NJ + ej + 1];
-            Ez[c] = 0.25 * (eZG1 + eZG2 + eZF1 + eZF2);
-        }
-        __syncthreads();
-    }
+    // ---- corner EMF (ct.cu:22-41) at corner (i, j) = (i0-1+ei, j0-1+ej),
+    // i.e. Fs (fi, fj) = (ei, ej) and Gs (gi, gj) = (ei, ej); formed by each
+    // update cell for the corners it reads (no phase and barrier of its own) ----
+    auto corner_ez = [&](const int ei, const int ej) -> double {
+        // accumulated in FP64 whatever the flux-side type
+        const double eZG1 = (double)Go[O_EMF * SG + ei * G_NJ + ej];
+        const double eZG2 = (double)Go[O_EMF * SG + (ei + 1) * G_NJ + ej];
+        const double eZF1 = -1.0 * (double)Fo[O_EMF * SF + ei * F_NJ + ej];
+        const double eZF2 = -1.0 * (double)Fo[O_EMF * SF + ei * F_NJ + ej + 1];
+        return 0.25 * (eZG1 + eZG2 + eZF1 + eZF2);
+    };
 
     // ---- update of the tile's own cells ----
     const int fo_ = (li + 1) * F_NJ + (lj - T::F_J0);             // F(i); F(i-1) is F_NJ before
@@ -613,16 +607,16 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
             for (int n = 0; n < 6; ++n)
                 a.dst[fld[n] * PL + k] = uo[fld[n]] - dtdx * dF(n) - dtdy * dG(n);
             // CT_kernel (ct.cu:44-59) with the EMF of this stage
-            const double *ez = Ez + (li + 1) * EJ_ + (lj + 1);
-            a.dst[BXF * PL + k] = uo[BXF] - dtdy * (ez[0] - ez[-1]);
-            a.dst[BYF * PL + k] = uo[BYF] + dtdx * (ez[0] - ez[-EJ_]);
+            const double ez_c = corner_ez(li + 1, lj + 1), ez_w = corner_ez(li + 1, lj);
+            const double ez_s = corner_ez(li, lj + 1);
+            a.dst[BXF * PL + k] = uo[BXF] - dtdy * (ez_c - ez_w);
+            a.dst[BYF * PL + k] = uo[BYF] + dtdx * (ez_c - ez_s);
             // Symmetric boundaries read the CT'd face bY at j = 2 (the lower
             // wall face) before replacing it (TS boundary.cu:57-88).
             if (a.row2 && j0 == HALO && lj == 0) {
-                const double *e2 = Ez + (li + 1) * EJ_;
                 const double b2 = T::OVERLAY ? a.src[BYF * PL + k - 1]
                                                : Ut[BYF * UF + (li + HALO) * UJ + (lj + HALO) - 1];
-                a.row2[i] = b2 + dtdx * (e2[0] - e2[-EJ_]);
+                a.row2[i] = b2 + dtdx * (ez_w - corner_ez(li, lj));
             }
         }
     } else {
