@@ -546,9 +546,11 @@ def precision_block(args, setup, label, local_rank):
         ref_diag = _diagnostics(ref.get_state(), setup.dx, setup.dy, setup.gamma)
     for prec in ("fp64_exact", "fp64_fast", "fp32_bulk"):
         with Solver.from_setup(setup, precision=prec, device=local_rank) as sol:
+            sol.autotune(4)
             sol.run(args.warmup)
             ms = sol.run_timed(args.steps)
-            entry = {"value": setup.interior_cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps}
+            entry = {"value": setup.interior_cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                     "tile_shapes": list(sol.stage_shapes)}
             if prec != "fp64_exact":
                 sol.set_state(setup.state, apply_boundary=True)
                 sol.run_fixed_dt(dts)
@@ -700,6 +702,7 @@ def adjoint_block(args, local_rank, n=512, nsteps=2000, ndirs=32, h=1e-6):
     grads = {}
     for prec in ("fp32_bulk", "fp64_exact"):
         with Solver.from_setup(s, precision=prec, device=local_rank) as sol:
+            sol.autotune(4)
             sol.run(3)
             sol.set_state(s.state, apply_boundary=True)
             ms_fwd = sol.run_timed(nsteps)
@@ -966,6 +969,8 @@ def contact_block(args, setup, label, local_rank):
     for ct in ("stage1", "contact"):
         s = dataclasses.replace(setup, ct=ct)
         with Solver.from_setup(s, precision="fp64_exact", device=local_rank) as sol:
+            if ct == "stage1":
+                sol.autotune(4)
             sol.run(args.warmup)
             ms = sol.run_timed(args.steps)
             out[ct] = {"value": setup.interior_cells * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
