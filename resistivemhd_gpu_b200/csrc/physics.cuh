@@ -766,7 +766,13 @@ struct BulkStates {
 // other flux components (mass, induction, energy) stay single precision.
 // fm[0..2]: the three momentum components (f1, f2, f3) in FP64;
 // fo[0]: f0, fo[1]: f5, fo[2]: f6, fo[3]: f7 in FP32.
-__device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, float inv_gm1, float EPS,
+//
+// ONE = true forms the common case only (exactly one region, finite wave
+// speeds), taking that region's state as soon as its flag is known; it
+// returns false (fm, fo unwritten) where the case does not apply.  ONE =
+// false forms every case.
+template <bool ONE>
+__device__ __forceinline__ bool hlld_bulk_body(const BulkStates &s, float gm, float inv_gm1, float EPS,
                                                double fm[3], float fo[4])
 {
     const double bn64 = s.bn;
@@ -804,6 +810,16 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
     SL = tmin(SL, 0.f);
     SR = tmax(SR, 0.f);
 
+    // the selected candidate (ONE): single-precision state, FP64 total
+    // pressure and tangential B
+    const bool bOL = SL > 0.f, bOR = SR <= 0.f;
+    float cr, cu, cv, cw, ce;
+    double cpt, cby, cbz;
+    if (ONE) {
+        cr = bOL ? rhoL : rhoR; cu = bOL ? uL : uR; cv = bOL ? vL : vR; cw = bOL ? wL : wR; ce = 0.f;
+        cpt = bOL ? pTL64 : pTR64; cby = bOL ? s.bYL : s.bYR; cbz = bOL ? s.bZL : s.bZR;
+    }
+
     const float dSL = SL - uL, dSR = SR - uR;
     const float rdSL = rhoL * dSL, rdSR = rhoR * dSR;
     const float iden = rcp_nr(rdSR - rdSL + EPS);
@@ -837,6 +853,17 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
     const float sqL = rho1L * rsL, sqR = rho1R * rsR;
     const float abx = fabsf(bX);
     const float S1L = SM - abx * rsL, S1R = SM + abx * rsR;
+    const bool bML = (SL <= 0.f) && (0.f < S1L), bIL = (S1L <= 0.f) && (0.f < SM);
+    const bool bMR = (S1R <= 0.f) && (0.f < SR), bIR = (SM <= 0.f) && (0.f < S1R);
+    if (ONE) {
+        ce = bOL ? eL : eR;
+        if (bML | bMR) {
+            cr = bML ? rho1L : rho1R; cu = SM; cv = bML ? v1L : v1R; cw = bML ? w1L : w1R; ce = bML ? e1L : e1R;
+            cpt = pT1_64;
+            cby = bML ? s.bYL + (double)cYL : s.bYR + (double)cYR;
+            cbz = bML ? s.bZL + (double)cZL : s.bZR + (double)cZR;
+        }
+    }
     const float sb = sgn(bX);
     const float id2 = rcp_nr(sqL + sqR + EPS);
     const float sqLR = sqL * sqR;
@@ -851,10 +878,34 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
     const float e2L = e1L - sqL * (vb1L - vb2) * sb;
     const float e2R = e1R + sqR * (vb1R - vb2) * sb;
 
-    const bool ind[6] = {SL > 0.f, (SL <= 0.f) && (0.f < S1L), (S1L <= 0.f) && (0.f < SM), SR <= 0.f,
-                         (S1R <= 0.f) && (0.f < SR), (SM <= 0.f) && (0.f < S1R)};
+    const bool ind[6] = {bOL, bML, bIL, bOR, bMR, bIR};
+    const int nsel = (int)bOL + (int)bML + (int)bIL + (int)bOR + (int)bMR + (int)bIR;
+    const bool nan_speed = (SL != SL) | (SR != SR) | (SM != SM) | (S1L != S1L) | (S1R != S1R);
     fm[0] = fm[1] = fm[2] = 0.0;
     fo[0] = fo[1] = fo[2] = fo[3] = 0.f;
+    // FP64 momentum stresses and single-precision mass, induction and energy
+    // fluxes of one candidate state
+    auto add_state = [&](float rho, float u, float v, float w, float e, double pT, double by, double bz) {
+        const float by32 = (float)by, bz32 = (float)bz, pT32 = (float)pT;
+        const float ru = rho * u;
+        fm[0] += (double)(ru * u) + pT - bn64 * bn64;
+        fm[1] += (double)(ru * v) - bn64 * by;
+        fm[2] += (double)(ru * w) - bn64 * bz;
+        fo[0] += ru;
+        fo[1] += u * by32 - v * bX;
+        fo[2] += u * bz32 - w * bX;
+        fo[3] += (e + pT32) * u - bX * (bX * u + by32 * v + bz32 * w);
+    };
+    if (ONE) {
+        if (nsel != 1 || nan_speed) return false;
+        if (bIL | bIR) {
+            cr = bIL ? rho1L : rho1R; cu = SM; cv = v2; cw = w2; ce = bIL ? e2L : e2R; cpt = pT1_64;
+            cby = s.bYL + (double)(cYL + c2Y);   // the double-star B is shared by both sides
+            cbz = s.bZL + (double)(cZL + c2Z);
+        }
+        add_state(cr, cu, cv, cw, ce, cpt, cby, cbz);
+        return true;
+    }
     // candidate r: 0 outer L, 1 middle L, 2 inner L, 3 outer R, 4 middle R, 5 inner R
     auto add = [&](int r) {
         const bool lft = r < 3;
@@ -869,17 +920,8 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
                         : r == 4 ? s.bYR + (double)cYR : s.bYL + (double)(cYL + c2Y);
         const double bz = r == 0 ? s.bZL : r == 3 ? s.bZR : r == 1 ? s.bZL + (double)cZL
                         : r == 4 ? s.bZR + (double)cZR : s.bZL + (double)(cZL + c2Z);
-        const float by32 = (float)by, bz32 = (float)bz, pT32 = (float)pT;
-        const float ru = rho * u;
-        fm[0] += (double)(ru * u) + pT - bn64 * bn64;
-        fm[1] += (double)(ru * v) - bn64 * by;
-        fm[2] += (double)(ru * w) - bn64 * bz;
-        fo[0] += ru;
-        fo[1] += u * by32 - v * bX;
-        fo[2] += u * bz32 - w * bX;
-        fo[3] += (e + pT32) * u - bX * (bX * u + by32 * v + bz32 * w);
+        add_state(rho, u, v, w, e, pT, by, bz);
     };
-    const int nsel = (int)ind[0] + (int)ind[1] + (int)ind[2] + (int)ind[3] + (int)ind[4] + (int)ind[5];
     if (nsel == 1) {
         const int r = ind[0] ? 0 : ind[1] ? 1 : ind[2] ? 2 : ind[3] ? 3 : ind[4] ? 4 : 5;
         add(r);
@@ -887,11 +929,27 @@ __device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, fl
         for (int r = 0; r < 6; ++r)
             if (ind[r]) add(r);
     }
-    if ((SL != SL) | (SR != SR) | (SM != SM) | (S1L != S1L) | (S1R != S1R)) {
+    if (nan_speed) {
         const double dn = bits_to_double(0x7FF8000000000000ull);
         fm[0] = fm[1] = fm[2] = dn;
         fo[0] = fo[1] = fo[2] = fo[3] = qnan;
     }
+    return true;
+}
+
+// Every case of the FP32-bulk HLLD flux.
+__device__ __forceinline__ void hlld_flux_bulk(const BulkStates &s, float gm, float inv_gm1, float EPS, double fm[3],
+                                               float fo[4])
+{
+    hlld_bulk_body<false>(s, gm, inv_gm1, EPS, fm, fo);
+}
+
+// Its common case; false, with fm and fo unwritten, where that does not
+// apply (the caller then forms the interface with hlld_flux_bulk).
+__device__ __forceinline__ bool hlld_flux_bulk_sel(const BulkStates &s, float gm, float inv_gm1, float EPS,
+                                                   double fm[3], float fo[4])
+{
+    return hlld_bulk_body<true>(s, gm, inv_gm1, EPS, fm, fo);
 }
 
 // calculateDtFunctor arithmetic with reciprocals (fast variant); a negative

@@ -381,11 +381,11 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
     // copies, and the exact variant, which measured slower with them, pass
     // it at run time.  Both sweeps share one index space, so the threads
     // stay balanced.
-    // `full` (a FullC tag) selects the FP64 variants' rare path for an
-    // interface whose common-case flux declined (hlld_flux_sel or
-    // hlld_flux_fast_sel returned false; flux_at then stores nothing and
-    // returns false): every case of the fast flux, or in the exact variant
-    // the reference's arithmetic in full (hlld_flux_ieee).
+    // `full` (a FullC tag) selects the rare path for an interface whose
+    // common-case flux declined (hlld_flux_sel, hlld_flux_fast_sel or
+    // hlld_flux_bulk_sel returned false; flux_at then stores nothing and
+    // returns false): every case of the fast or FP32-bulk flux, or in the
+    // exact variant the reference's arithmetic in full (hlld_flux_ieee).
     auto flux_at = [&](const int it, const auto sweep, const auto full) -> bool {
         (void)full;
         const bool isF = sweep.value;
@@ -451,7 +451,10 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
             muscl_dev(bt2[-ps], bt2[0], bt2[ps], bt2[2 * ps], EPSF, st.bZL, st.bZR);
             st.bn = bn;
             float fo4[4];
-            hlld_flux_bulk(st, gmR, inv_gm1, EPSF, fmv, fo4);
+            if (full.value)
+                hlld_flux_bulk(st, gmR, inv_gm1, EPSF, fmv, fo4);
+            else if (!hlld_flux_bulk_sel(st, gmR, inv_gm1, EPSF, fmv, fo4))
+                return false;
             // fo4: f0, f5 (tangential-1 induction), f6 (tangential-2), f7
             fov[0] = fo4[0]; fov[1] = fo4[2]; fov[2] = fo4[3]; fov[3] = fo4[1];
         }
@@ -543,14 +546,12 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
             done = flux_at(it, SweepC<false>{}, FullC<false>{});
         redo |= done ? 0u : 1u << r;
     }
-#if !RMHD_BULK
-    // The FP64 variants' rare path, after the loop, so that its registers
-    // do not weigh on the loop's.
+    // The rare path, after the loop, so that its registers do not weigh on
+    // the loop's.
     if (redo) {
         for (int it = tid, r = 0; it < T::NF + T::NG; it += T::THREADS, ++r)
             if ((redo >> r) & 1u) flux_at(it, SweepRT{it < T::NF}, FullC<true>{});
     }
-#endif
     // The update's own cell of the stage's source state (from global memory
     // when the flux planes overlay the staged tile), and in stage 2 that of
     // U^n: issue those loads here, so that their latency overlaps the
