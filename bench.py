@@ -725,6 +725,7 @@ def adjoint_block(args, local_rank, n=512, nsteps=2000, ndirs=32, h=1e-6):
     for prec in ("fp32_bulk", "fp64_exact"):
         try:
             with Solver.from_setup(s, precision=prec, device=local_rank) as sol:
+                sol.autotune(4)
                 sol.adjoint_forward(nsteps, -1)                        # allocates the trajectory
                 sol.set_state(s.state, apply_boundary=True)
                 t0 = time.perf_counter()

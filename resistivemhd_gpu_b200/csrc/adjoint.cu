@@ -130,7 +130,7 @@ __device__ __forceinline__ void gather_sweep(const AdjStageArgs &a, int dir, int
     for (int s = 0; s < 8; ++s) nat_bar[sweep_field(dir, s)] += cb[s];
 }
 
-__global__ void __launch_bounds__(ADJ_THREADS) adj_gather_kernel(AdjStageArgs a)
+__global__ void __launch_bounds__(ADJ_THREADS, 6) adj_gather_kernel(AdjStageArgs a)
 {
     const Grid &g = a.g;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

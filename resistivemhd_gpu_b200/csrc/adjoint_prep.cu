@@ -65,7 +65,7 @@ __device__ void resistive_reverse(const AdjStageArgs &a, int i, int j)
     rj[5 * g.plane] = dbZ;
 }
 
-__global__ void __launch_bounds__(128) adj_prep_kernel(AdjStageArgs a)
+__global__ void __launch_bounds__(128, 8) adj_prep_kernel(AdjStageArgs a)
 {
     const Grid &g = a.g;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
