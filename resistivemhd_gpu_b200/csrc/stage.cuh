@@ -10,14 +10,15 @@
 //
 // Data layout: 8 field planes of nx x pitch doubles (index i*pitch + j,
 // y contiguous), one allocation per state.  Each CTA owns TI x TJ interior
-// cells (TI = 8 in stage 1, 9 in stage 2, TJ = 32) and stages them with a 3-cell halo on every side by one 3-D TMA load
+// cells (one of the tile shapes of rmhd2d_internal.h, e.g. 8 x 32) and
+// stages them with a 3-cell halo on every side by one 3-D TMA load
 // (box TJ+6 x TI+6 x 8 fields) into shared memory, plus a 2-D TMA load of the
 // eta table on the same cells; everything after those loads reads shared
 // memory, except the update's read of its own cell of the stage's source
 // state (and, in stage 2, of U^n).
 //
-// The kernel is compiled three times: an "exact" variant (-fmad=false, all
-// six HLLD candidate fluxes formed), bit-identical to the reference
+// The kernel is compiled three times: an "exact" variant (-fmad=false, the
+// bits of the reference's sum of six HLLD candidate fluxes), bit-identical to the reference
 // evaluated in IEEE binary64; a "fast" FP64 variant (FMA contraction, shared
 // reciprocals, only the selected HLLD candidate); and an "FP32-bulk" variant
 // (reconstruction and fluxes in single precision, pressure recovery, EMF,

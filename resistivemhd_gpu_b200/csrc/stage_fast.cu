@@ -4,6 +4,5 @@
 // the current density and the CFL rate.  Differs from the exact variant by
 // rounding only.
 #define RMHD_VARIANT fast
-#define RMHD_ALL_CANDIDATES false
 #define RMHD_FAST_MATH 1
 #include "stage_impl.cuh"

@@ -1,6 +1,7 @@
 // stage_impl.cuh -- body of the fused stage kernel (see stage.cuh).  Included
-// once per variant by stage_exact.cu and stage_fast.cu, which define
-// RMHD_VARIANT, RMHD_ALL_CANDIDATES and RMHD_FAST_MATH.
+// once per variant by stage_exact.cu, stage_fast.cu and stage_bulk32.cu,
+// which define RMHD_VARIANT and, as they need them, RMHD_FAST_MATH,
+// RMHD_REAL and RMHD_BULK.
 #pragma once
 
 #include "stage.cuh"

@@ -107,6 +107,25 @@ def test_exact_bitwise_vs_oracle_on_extreme_values(gpu, oracle, case):
     assert np.array_equal(out, ref, equal_nan=True)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64_fast", "fp32_bulk"])
+def test_contracted_variants_propagate_a_nan_energy(gpu, oracle, precision):
+    """The contracted variants form an interface with NaN wave speeds after
+    their flux loop (the common-case flux declines it) as a NaN flux, as the
+    reference's weighted sum does: after one step the same cells are
+    non-finite as in the oracle's run, and the crash flag is raised."""
+    from resistivemhd_gpu_b200 import setups
+
+    s = setups.random_smooth_state(40, 36, seed=11, bc="periodic")
+    st = s.state.copy()
+    st[18, 15, 7] = np.nan
+    s.state = st
+    ref, _, crashed_at = oracle.run(s, st, 1)
+    out, _, _, crashed = run_cuda(s, 1, precision=precision)
+    assert crashed_at == 0 and crashed
+    assert np.array_equal(~np.isfinite(out), ~np.isfinite(ref))
+
+
 @pytest.mark.parametrize("bc,bc_y,table,shape", [
     ("periodic", "symmetric", False, (40, 33)),   # oneStepRK2PeriodicXSymmetricY
     ("periodic", "symmetric", True, (17, 70)),

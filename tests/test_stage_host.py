@@ -195,3 +195,22 @@ def test_host_contracted_variants_survive_the_degenerate_face(host_stage_contrac
     assert crashed == -1 and np.isfinite(c).all(), variant
     rel = np.abs(c[..., 7] - s.state[F.CENTRE][..., 7]) / np.abs(s.state[F.CENTRE][..., 7])
     assert rel.max() < 1e-2, (variant, rel.max())
+
+
+def test_host_contracted_variants_take_the_nan_path(host_stage_contracted, oracle):
+    """A NaN energy makes the wave speeds of the interfaces around it NaN.
+    The contracted variants' common-case flux declines those interfaces, and
+    the pass after the flux loop forms them as NaN fluxes, as the reference's
+    weighted sum does: after one step the same cells are non-finite as in
+    the oracle's run, and the crash flag is raised."""
+    from resistivemhd_gpu_b200 import setups
+
+    variant, lib = host_stage_contracted
+    s = setups.random_smooth_state(40, 36, seed=11, bc="periodic")
+    st = s.state.copy()
+    st[18, 15, 7] = np.nan
+    s.state = st
+    want, _, crashed_at = oracle.run(s, st, 1)
+    got, _, crashed = run_host(lib, s, 1, 4)
+    assert crashed_at == 0 and crashed == 0, variant
+    assert np.array_equal(~np.isfinite(got), ~np.isfinite(want)), variant
