@@ -376,12 +376,12 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
 
     // ---- HLLD fluxes (hlld.cu:110-233, muscl.cu:6-126, flux_solver.cu:10-33)
     // with the resistive terms ----
-    // One interface per call.  Stage 2 of the contracted variants passes the
-    // sweep as a compile-time tag (a copy of the body per sweep, with
-    // constant plane strides); stage 1, whose larger tile spills with two
-    // copies, and the exact variant, which measured slower with them, pass
-    // it at run time.  Both sweeps share one index space, so the threads
-    // stay balanced.
+    // One interface per call.  Stage 2 of the contracted variants and both
+    // stages of FP32-bulk pass the sweep as a compile-time tag (a copy of the
+    // body per sweep, with constant plane strides); FP64-fast's stage 1 and
+    // the exact variant, which measured slower with two copies (8 % and
+    // 10-25 % at 256-thread tiles), pass it at run time.  Both sweeps share
+    // one index space, so the threads stay balanced.
     // `full` (a FullC tag) selects the rare path for an interface whose
     // common-case flux declined (hlld_flux_sel, hlld_flux_fast_sel or
     // hlld_flux_bulk_sel returned false; flux_at then stores nothing and
@@ -539,7 +539,7 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
     static_assert((T::NF + T::NG + T::THREADS - 1) / T::THREADS <= 32, "passes of the flux phase");
     for (int it = tid, r = 0; it < T::NF + T::NG; it += T::THREADS, ++r) {
         bool done;
-        if (STAGE == 1 || !RMHD_FAST_MATH)
+        if ((STAGE == 1 && !RMHD_BULK) || !RMHD_FAST_MATH)
             done = flux_at(it, SweepRT{it < T::NF}, FullC<false>{});
         else if (it < T::NF)
             done = flux_at(it, SweepC<true>{}, FullC<false>{});
