@@ -627,6 +627,39 @@ int rmhd2d_calculate_dt(rmhd2d_solver *s, double *dt)
     return RMHD2D_OK;
 }
 
+// Captures `nsteps` consecutive steps starting at step parity `parity` into
+// *ge and uploads the graph, so that its first launch costs no more than
+// the later ones.
+static int capture_steps(rmhd2d_solver *s, int parity, int nsteps, cudaGraphExec_t *ge)
+{
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    for (int n = 0; n < nsteps; ++n) enqueue_step(s, parity ^ (n & 1));
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (e != cudaSuccess) return fail(s, RMHD2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(ge, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        *ge = nullptr;
+        return fail(s, RMHD2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    CK(cudaGraphUpload(*ge, s->stream));
+    return RMHD2D_OK;
+}
+
+// The one-step (k = 1) or two-step (k = 2) graphs of both step parities,
+// captured together on first use: a run's step count then never meets an
+// uncaptured parity, so no capture falls inside a later (timed) run.
+static int ensure_step_graphs(rmhd2d_solver *s, cudaGraphExec_t g[2], int k)
+{
+    for (int p = 0; p < 2; ++p)
+        if (!g[p]) {
+            const int rc = capture_steps(s, p, k, &g[p]);
+            if (rc) return rc;
+        }
+    return RMHD2D_OK;
+}
+
 int rmhd2d_step_rk2(rmhd2d_solver *s)
 {
     if (!s) return fail(s, RMHD2D_ERR_INVALID, "null solver");
@@ -644,21 +677,9 @@ int rmhd2d_step_rk2(rmhd2d_solver *s)
         enqueue_step(s, s->parity);
         CK(cudaGetLastError());
     } else {
-        cudaGraphExec_t &ge = s->graph1[s->parity];
-        if (!ge) {
-            cudaGraph_t graph = nullptr;
-            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            enqueue_step(s, s->parity);
-            cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
-            if (e != cudaSuccess) return fail(s, RMHD2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&ge, graph, 0);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) {
-                ge = nullptr;
-                return fail(s, RMHD2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            }
-        }
-        CK(cudaGraphLaunch(ge, s->stream));
+        const int rc = ensure_step_graphs(s, s->graph1, 1);
+        if (rc) return rc;
+        CK(cudaGraphLaunch(s->graph1[s->parity], s->stream));
     }
     s->parity ^= 1;
     s->steps += 1;
@@ -673,23 +694,12 @@ int rmhd2d_run(rmhd2d_solver *s, int nsteps)
     if (nsteps < 0) return fail(s, RMHD2D_ERR_INVALID, "nsteps < 0");
     if (!s->has_state) return fail(s, RMHD2D_ERR_STATE, "no state set");
     CK(cudaSetDevice(s->device));
+    if (nsteps >= 2) {
+        const int rc = ensure_step_graphs(s, s->graph2, 2);
+        if (rc) return rc;
+    }
     while (nsteps >= 2) {
-        cudaGraphExec_t &ge = s->graph2[s->parity];
-        if (!ge) {
-            cudaGraph_t graph = nullptr;
-            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            enqueue_step(s, s->parity);
-            enqueue_step(s, s->parity ^ 1);
-            cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
-            if (e != cudaSuccess) return fail(s, RMHD2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&ge, graph, 0);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) {
-                ge = nullptr;
-                return fail(s, RMHD2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            }
-        }
-        CK(cudaGraphLaunch(ge, s->stream));
+        CK(cudaGraphLaunch(s->graph2[s->parity], s->stream));
         s->steps += 2;
         nsteps -= 2;
     }
@@ -1206,23 +1216,27 @@ int rmhd2d_batch_run(rmhd2d_batch *b, int nsteps)
     BCK(cudaSetDevice(b->device));
     int rc = batch_build(b);
     if (rc) return rc;
-    while (nsteps >= 2) {
-        cudaGraphExec_t &ge = b->graph2[b->parity];
-        if (!ge) {
-            cudaGraph_t graph = nullptr;
-            BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            batch_enqueue_step(b, b->parity);
-            batch_enqueue_step(b, b->parity ^ 1);
-            cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
-            if (e != cudaSuccess) return bfail(b, RMHD2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&ge, graph, 0);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) {
-                ge = nullptr;
-                return bfail(b, RMHD2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            }
+    // the two-step graphs of both step parities, captured together on first
+    // use (as for a single solver, rmhd2d_run) and uploaded
+    for (int p = 0; p < 2 && nsteps >= 2; ++p) {
+        cudaGraphExec_t &ge = b->graph2[p];
+        if (ge) continue;
+        cudaGraph_t graph = nullptr;
+        BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        batch_enqueue_step(b, p);
+        batch_enqueue_step(b, p ^ 1);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+        if (e != cudaSuccess) return bfail(b, RMHD2D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&ge, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            ge = nullptr;
+            return bfail(b, RMHD2D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
         }
-        BCK(cudaGraphLaunch(ge, b->stream));
+        BCK(cudaGraphUpload(ge, b->stream));
+    }
+    while (nsteps >= 2) {
+        BCK(cudaGraphLaunch(b->graph2[b->parity], b->stream));
         batch_advance(b, 2);
         nsteps -= 2;
     }

@@ -142,6 +142,7 @@ inline cudaError_t cudaGraphExecDestroy(cudaGraphExec_t e)
     delete reinterpret_cast<ShimGraph *>(e);
     return cudaSuccess;
 }
+inline cudaError_t cudaGraphUpload(cudaGraphExec_t, cudaStream_t) { return cudaSuccess; }
 inline cudaError_t cudaGraphLaunch(cudaGraphExec_t e, cudaStream_t)
 {
     for (auto &op : reinterpret_cast<ShimGraph *>(e)->ops) op();
