@@ -226,9 +226,10 @@ BatchLauncher batch_launcher(int precision)
 // in `ustar` (read through map_ustar); the same launches as enqueue_step
 // without A and B.  dst may not be un.
 void enqueue_step_between(rmhd2d_solver *s, int parity, const double *un, const CUtensorMap *map_un, double *ustar,
-                          const CUtensorMap *map_ustar, double *dst)
+                          const CUtensorMap *map_ustar, double *dst, double *dt_log, const double *dt_in)
 {
     StageArgs a{};
+    a.dt_in = dt_in;
     a.g = s->g;
     a.eta = s->eta;
     a.row2 = s->g.bc_x == BC_SYMMETRIC ? s->row2 : nullptr;
@@ -238,7 +239,9 @@ void enqueue_step_between(rmhd2d_solver *s, int parity, const double *un, const 
     a.src = un;
     a.un = un;
     a.dst = ustar;
+    a.dt_log = dt_log;
     launch(1, s->shape, map_un, &s->mapE1[s->shape], a, s->stream);
+    a.dt_log = nullptr;
     launch_boundary(s->g, ustar, s->row2, nullptr, 0, s->stream);
     a.src = ustar;
     a.un = un;
@@ -247,7 +250,10 @@ void enqueue_step_between(rmhd2d_solver *s, int parity, const double *un, const 
     launch_boundary(s->g, dst, s->row2, s->ctl, parity ^ 1, s->stream);
 }
 
-void enqueue_step(rmhd2d_solver *s, int parity)
+// dt_log: stage 1 also writes the step's dt there (a recorded run); dt_in:
+// the step reads its dt from there (a replayed run).  Not for CT-Contact,
+// whose pipeline takes its dt from the control block.
+void enqueue_step(rmhd2d_solver *s, int parity, double *dt_log = nullptr, const double *dt_in = nullptr)
 {
     if (s->contact) {
         const size_t P = (size_t)s->g.plane;
@@ -276,12 +282,15 @@ void enqueue_step(rmhd2d_solver *s, int parity)
     a.row2 = s->g.bc_x == BC_SYMMETRIC ? s->row2 : nullptr;
     a.ctl = s->ctl;
     a.parity = parity;
+    a.dt_in = dt_in;
     auto launch = stage_launcher(s->cfg.precision);
     // stage 1: U^n (A) -> U* (B)
     a.src = s->A;
     a.un = s->A;
     a.dst = s->B;
+    a.dt_log = dt_log;
     launch(1, s->shape, &s->mapA[s->shape], &s->mapE1[s->shape], a, s->stream);
+    a.dt_log = nullptr;
     launch_boundary(s->g, s->B, s->row2, nullptr, 0, s->stream);
     // stage 2: (U*, U^n) -> U^{n+1} in A
     a.src = s->B;
@@ -1567,8 +1576,14 @@ extern "C" int rmhd2d_run_fixed_dt(rmhd2d_solver *s, int nsteps, const double *h
     if (rc) return rc;
     FixedDtScope fixed{s, true};
     for (int n = 0; n < nsteps; ++n) {
-        CK(cudaMemcpyAsync(&s->ctl->dt_fixed, d.p + n, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-        enqueue_step(s, s->parity);
+        // the stage kernels read the step's dt from d.p + n; CT-Contact's
+        // pipeline reads the control block's dt_fixed
+        if (s->contact) {
+            CK(cudaMemcpyAsync(&s->ctl->dt_fixed, d.p + n, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+            enqueue_step(s, s->parity);
+        } else {
+            enqueue_step(s, s->parity, nullptr, d.p + n);
+        }
         s->parity ^= 1;
         s->steps += 1;
     }
@@ -1658,20 +1673,19 @@ extern "C" int rmhd2d_adjoint_forward(rmhd2d_solver *s, int nsteps, int checkpoi
         for (int n = 0; n < nsteps; ++n) {
             const size_t o = (size_t)n * sd;
             double *next = n + 1 < nsteps ? w->seg0 + o + sd : s->A;
-            enqueue_step_between(s, s->parity, w->seg0 + o, &w->map0[n], w->seg1 + o, &w->map1[n], next);
+            enqueue_step_between(s, s->parity, w->seg0 + o, &w->map0[n], w->seg1 + o, &w->map1[n], next, w->dts + n,
+                                 nullptr);
             s->parity ^= 1;
             s->steps += 1;
-            CK(cudaMemcpyAsync(w->dts + n, &s->ctl->dt, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
         }
     } else {
         for (int n = 0; n < nsteps; ++n) {
             if (n % interval == 0)
                 CK(cudaMemcpyAsync(w->ckpt + (size_t)(n / interval) * sd, s->A, sd * sizeof(double),
                                    cudaMemcpyDeviceToDevice, s->stream));
-            enqueue_step(s, s->parity);
+            enqueue_step(s, s->parity, w->dts + n);
             s->parity ^= 1;
             s->steps += 1;
-            CK(cudaMemcpyAsync(w->dts + n, &s->ctl->dt, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
         }
     }
     CK(cudaMemcpyAsync(w->final_state, s->A, sd * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
@@ -1735,9 +1749,9 @@ extern "C" int rmhd2d_adjoint_backward(rmhd2d_solver *s, const double *host_seed
             for (int n = n0; n < n1; ++n) {
                 const int k = n - n0;
                 const size_t o = (size_t)k * sd;
-                CK(cudaMemcpyAsync(&s->ctl->dt_fixed, w->dts + n, sizeof(double), cudaMemcpyDeviceToDevice, st));
                 double *next = n + 1 < n1 ? w->seg0 + o + sd : s->A;
-                enqueue_step_between(s, 0, w->seg0 + o, &w->map0[k], w->seg1 + o, &w->map1[k], next);
+                enqueue_step_between(s, 0, w->seg0 + o, &w->map0[k], w->seg1 + o, &w->map1[k], next, nullptr,
+                                     w->dts + n);
             }
         }
         // reverse sweep over the segment

@@ -43,6 +43,8 @@ struct StageArgs {
     double *row2;        // symmetric boundaries: CT'd bY at j = 2, indexed by i
     Control *ctl;
     int parity;          // step parity: dt from ctl->amax[parity]
+    double *dt_log;      // stage 1, or nullptr: the step's dt is also written here (a recorded run)
+    const double *dt_in; // or nullptr: the step's dt is read from here (a replayed run), not reduced
 };
 
 // One set of launchers per variant (stage_exact.cu, stage_fast.cu, stage_bulk32.cu).

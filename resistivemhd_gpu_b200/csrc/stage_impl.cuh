@@ -247,12 +247,15 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
 
     // dt of this step from the CFL reduction of the previous state
     // (resistiveMHD_2D.cu:277-291), identical in every thread, unless the
-    // run holds dt fixed (a recorded trajectory being replayed).
-    const double dt = a.ctl->use_fixed_dt
+    // run holds dt fixed (a recorded trajectory being replayed): read from
+    // dt_in, or the control block's dt_fixed.
+    const double dt = a.dt_in ? *a.dt_in
+                    : a.ctl->use_fixed_dt
                           ? a.ctl->dt_fixed
                           : step_dt(a.ctl->amax[a.parity], a.ctl->first_nan[a.parity], g.dx, g.dy, g.eps, g.eta, g.cfl);
     if (STAGE == 1 && ctl_tile && tid == 0) {
         a.ctl->dt = dt;
+        if (a.dt_log) *a.dt_log = dt;
         a.ctl->total_time = a.ctl->total_time + dt;
         a.ctl->amax[a.parity ^ 1] = 0ull;
         a.ctl->first_nan[a.parity ^ 1] = 0;
@@ -697,7 +700,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ C
 template <int STAGE>
 __device__ __forceinline__ StageArgs batch_args(const BatchRun &r, int parity)
 {
-    StageArgs a;
+    StageArgs a{};
     a.g = r.g;
     a.src = STAGE == 1 ? r.A : r.B;
     a.un = r.A;
