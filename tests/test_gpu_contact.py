@@ -90,3 +90,26 @@ def test_contact_refuses_batch_adjoint_and_profile(gpu):
             sol.profile_step()
     with pytest.raises(_lib.RMHDError):
         Batch([s, s])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ct", ["stage1", "contact"])
+def test_fixed_dt_replay_equals_the_run(gpu, ct):
+    """A run replayed with its own recorded dts (rmhd2d_run_fixed_dt) gives
+    the run's states bit for bit, with either CT scheme: the stage kernels
+    read each step's dt from the replay's table, CT-Contact's pipeline from
+    the control block."""
+    from resistivemhd_gpu_b200 import Solver, setups
+
+    s = dataclasses.replace(setups.harris_sheet(64, 32), ct=ct)
+    with Solver.from_setup(s, precision="fp64_exact") as sol:
+        dts = []
+        for _ in range(5):
+            sol.step()
+            dts.append(sol.dt)
+        want = sol.get_state()
+    with Solver.from_setup(s, precision="fp64_exact") as sol:
+        sol.run_fixed_dt(dts)
+        got = sol.get_state()
+        assert sol.dt == dts[-1]
+    assert np.array_equal(got, want)
