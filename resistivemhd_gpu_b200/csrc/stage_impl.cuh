@@ -319,8 +319,12 @@ __device__ __forceinline__ bool stage_tile(const StageArgs &a, const TileLoad &l
         const double e = u0[EN * UF];
         const double px = (gm - 1.0) * (e - 0.5 * (rho * (u * u + v * v + w * w))
                         - 0.5 * (bXc * bXc + bYc * bYc + bZ * bZ));
-        const double py = (gm - 1.0) * (e - 0.5 * (rho * (v * v + w * w + u * u))
-                        - 0.5 * (bYc * bYc + bZ * bZ + bXc * bXc));
+        // The y sweep's pressure sums its squares in the permuted order; the
+        // contracted variants, which differ from the reference by rounding
+        // anyway, take the x sweep's.
+        const double py = RMHD_FAST_MATH ? px
+                        : (gm - 1.0) * (e - 0.5 * (rho * (v * v + w * w + u * u))
+                          - 0.5 * (bYc * bYc + bZ * bZ + bXc * bXc));
         // primitives are recovered in FP64; the velocities and the density
         // are stored in the flux-side type, B and pressures in FP64
         Real *v0 = Pv + c;
